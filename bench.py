@@ -1,0 +1,436 @@
+"""Benchmark: dsposv vs dposv time to an FP64 backward error at n = 32768.
+
+One step = one plasma_dsposv solve (low-precision tile Cholesky + FP64
+iterative refinement) of the mixed-precision configuration: n = 32768,
+nrhs = 1, A = Q diag(lambda) Q^T with Q from Householder QR of an N(0,1)
+matrix (seed 11), lambda log-spaced from 1 to 1/kappa, b = A x_true.  The
+operands are resident in HBM (8.6 GB, larger than L2) and are passed to the
+LAPACK-layout C entry point as device pointers.  Beside it the plain FP64
+plasma_dposv is timed on the same matrix; the ratio is the speed-up.
+
+value      : FP64-equivalent GFLOP/s of dsposv, (n^3/3 + 2 n^2 nrhs) / t.
+e2e        : the same, through plasma_dsposv with HOST buffers (H2D of A and
+             b and D2H of x inside the timed region).
+roofline   : the dominant kernel (trailing update) of the timed region, timed
+             by the library's own CUDA events on its launch stream.
+cpu_baseline / --impl reference : the CPU oracle (a C restatement of the
+             reference's tile algorithms, OpenMP tasks on all host cores) on
+             a bounded sample of the same workload (n = 8192).
+Multi-GPU: the path does not shard (one matrix per GPU); N GPUs run N
+independent replicas, timed as the max over ranks.
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--n", type=int, default=32768)
+    p.add_argument("--nrhs", type=int, default=1)
+    p.add_argument("--kappa", type=float, default=1e5)
+    p.add_argument("--mode", default="fp32", choices=["fp32", "tf32", "bf16", "auto"])
+    p.add_argument("--refine", default="ir", choices=["ir", "gmres", "auto"])
+    p.add_argument("--nb", type=int, default=0, help="0 = autotuned table")
+    p.add_argument("--cpu-n", type=int, default=8192)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-dposv", action="store_true")
+    return p.parse_args()
+
+
+MODES = {"fp32": 0, "tf32": 1, "bf16": 2, "auto": 3}
+REFINE = {"ir": 0, "gmres": 1, "auto": 2}
+
+
+def dist_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def flops_of(n, nrhs):
+    return n ** 3 / 3.0 + 2.0 * n * n * nrhs
+
+
+def make_system(n, nrhs, kappa, device, seed=11):
+    """A = Q diag(lambda) Q^T (symmetric: row-major == column-major), b = A x."""
+    import torch
+    g = torch.Generator(device=device).manual_seed(seed)
+    G = torch.randn(n, n, generator=g, device=device, dtype=torch.float64)
+    Q, _ = torch.linalg.qr(G)
+    del G
+    lam = torch.logspace(0.0, -float(np.log10(kappa)), n, device=device,
+                         dtype=torch.float64)
+    A = (Q * lam) @ Q.T
+    del Q
+    A = 0.5 * (A + A.T)
+    g2 = torch.Generator(device=device).manual_seed(seed + 1)
+    xt = torch.randn(nrhs, n, generator=g2, device=device, dtype=torch.float64)
+    B = (A @ xt.T).T.contiguous()          # nrhs x n row-major = n x nrhs col-major
+    torch.cuda.synchronize()
+    return A.contiguous(), B, xt
+
+
+def measured_peaks(torch):
+    """Roofline denominators.  BF16 and HBM from MEASURED_PEAKS.json; the FP64
+    and FP32/TF32 tensor peaks are not in that file, so they are measured
+    here the same way (cuBLAS GEMM, best of 5, CUDA events)."""
+    peaks = {}
+    try:
+        mp = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peaks["bf16"] = mp.get("bf16_tflops")
+        peaks["bf16_sustained"] = mp.get("bf16_tflops_sustained")
+        peaks["hbm_gbs"] = mp.get("hbm_gbs")
+        peaks["source"] = "MEASURED_PEAKS.json"
+    except Exception:
+        peaks.update({"bf16": 1590.0, "hbm_gbs": 6650.0, "source": "fallback"})
+
+    def gemm_tf(dtype, tf32, n=8192, reps=5):
+        torch.backends.cuda.matmul.allow_tf32 = tf32
+        a = torch.randn(n, n, device="cuda", dtype=dtype)
+        b = torch.randn(n, n, device="cuda", dtype=dtype)
+        for _ in range(2):
+            a @ b
+        torch.cuda.synchronize()
+        best = 1e9
+        for _ in range(reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            a @ b
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        torch.backends.cuda.matmul.allow_tf32 = False
+        return 2.0 * n ** 3 / best / 1e9
+
+    peaks["fp64"] = gemm_tf(torch.float64, False)
+    peaks["fp32"] = gemm_tf(torch.float32, False)
+    peaks["tf32"] = gemm_tf(torch.float32, True)
+    return peaks
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except Exception:
+            self.p.kill()
+            return None
+        mhz, maxmhz, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                mhz.append(float(f[1]))
+                maxmhz = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not mhz:
+            return None
+        return {"sm_mhz": float(np.median(mhz)), "sm_max_mhz": maxmhz,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def cpu_baseline(n, nrhs, kappa, threads=None):
+    """Oracle dsposv on the host cores on a bounded sample (n x n)."""
+    import oracle
+    import torch
+    if threads:
+        oracle.set_threads(threads)
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    A, B, _ = make_system(n, nrhs, kappa, dev) if dev == "cuda" else (None, None, None)
+    if A is None:
+        import gen
+        a = gen.spectrum(n, kappa)
+        b = a @ np.random.default_rng(12).standard_normal((n, nrhs))
+    else:
+        a = np.asfortranarray(A.cpu().numpy())
+        b = np.asfortranarray(B.cpu().numpy().T)
+        del A, B
+    x = np.zeros((n, nrhs), order="F")
+    t0 = time.perf_counter()
+    info, it = oracle.dsposv(oracle.LOWER, a, b, x, 256)
+    dt = time.perf_counter() - t0
+    return {"value": flops_of(n, nrhs) / dt / 1e9, "unit": "GFLOP/s",
+            "cores": oracle.get_threads(), "kind": "port",
+            "sample": f"oracle dsposv n={n} nrhs={nrhs} kappa={kappa:g} nb=256, one solve "
+                      f"({dt:.2f} s, iter {it}, info {info})",
+            "seconds": dt}
+
+
+def run_reference(args):
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return 0
+    import oracle
+    n = args.cpu_n
+    res = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(n, args.nrhs, args.kappa)
+        if i >= args.warmup:
+            res.append(r)
+    value = float(np.median([r["value"] for r in res]))
+    secs = float(np.mean([r["seconds"] for r in res]))
+    line = {
+        "impl": "reference",
+        "metric": "dsposv FP64-equivalent throughput to FP64 backward error",
+        "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": secs * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic",
+        "config": {"workload": f"dsposv n={n} (bounded CPU sample of n={args.n}) nrhs={args.nrhs} "
+                               f"A=Q diag(lambda) Q^T kappa={args.kappa:g}"},
+        "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": oracle.get_threads(),
+                         "kind": "port", "sample": res[-1]["sample"]},
+        "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import plasma_b200 as pb
+
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    L = pb.lib()
+    L.plasma_set(pb.PlasmaDevice, local)
+    assert L.plasma_init() == 0
+    if args.nb > 0:
+        L.plasma_set(pb.PlasmaTuning, pb.PlasmaDisabled)
+        L.plasma_set(pb.PlasmaNb, args.nb)
+    L.plasma_set(pb.PlasmaMixedPrecisionMode, MODES[args.mode])
+    L.plasma_set(pb.PlasmaRefinement, REFINE[args.refine])
+
+    n, nrhs = args.n, args.nrhs
+    peaks = measured_peaks(torch) if rank == 0 else {}
+    A, B, xt = make_system(n, nrhs, args.kappa, "cuda")
+    X = torch.zeros_like(B)
+    it = ctypes.c_int()
+    info = pb.plasma_dsposv_info_t()
+
+    def dsposv():
+        rc = L.plasma_dsposv_ex(pb.PlasmaLower, n, nrhs, A.data_ptr(), n, B.data_ptr(), n,
+                                X.data_ptr(), n, ctypes.byref(it), ctypes.byref(info))
+        assert rc == 0, rc
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        dsposv()
+    barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    pb.profile_enable(True)
+    l0 = pb.launches()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        dsposv()
+    e1.record()
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = pb.launches() - l0
+    prof = {k: pb.profile_query(k) for k in pb.KCLASS}
+    pb.profile_enable(False)
+    clk = clocks.stop()
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = t.item()
+
+    # accuracy of the last solve
+    Xc = X.T
+    R = B.T - A @ Xc
+    anorm = A.abs().sum(1).max().item()
+    berr = (R.abs().max(0).values / (anorm * Xc.abs().max(0).values)).max().item()
+    ferr = ((Xc - xt.T).abs().max(0).values / xt.T.abs().max(0).values).max().item()
+    iters = it.value
+
+    # plain FP64 dposv on the same matrix (A copied: dposv factors in place)
+    dposv = None
+    if not args.no_dposv and rank == 0:
+        Aw = torch.empty_like(A)
+        Bw = torch.empty_like(B)
+        times = []
+        for rep in range(2):
+            Aw.copy_(A)
+            Bw.copy_(B)
+            torch.cuda.synchronize()
+            f0 = torch.cuda.Event(enable_timing=True)
+            f1 = torch.cuda.Event(enable_timing=True)
+            pb.profile_enable(True)
+            f0.record()
+            rc = L.plasma_dposv(pb.PlasmaLower, n, nrhs, Aw.data_ptr(), n, Bw.data_ptr(), n)
+            f1.record()
+            torch.cuda.synchronize()
+            assert rc == 0, rc
+            if rep == 1:
+                times.append(f0.elapsed_time(f1))
+                dprof = pb.profile_query("update")
+            pb.profile_enable(False)
+        Xd = Bw.T
+        Rd = B.T - A @ Xd
+        berr_d = (Rd.abs().max(0).values / (anorm * Xd.abs().max(0).values)).max().item()
+        dms = min(times)
+        upd_tf = dprof["flops"] / dprof["ms"] / 1e9 if dprof["ms"] > 0 else None
+        dposv = {"ms": dms, "gflops": flops_of(n, nrhs) / dms / 1e6,
+                 "frac_fp64_peak": flops_of(n, nrhs) / dms / 1e9 / peaks["fp64"],
+                 "update_kernel_tflops": upd_tf, "backward_error": berr_d}
+        del Aw, Bw
+
+    # end to end through host buffers (pageable numpy arrays)
+    e2e = None
+    if not args.no_e2e and rank == 0:
+        ah = np.ascontiguousarray(A.cpu().numpy())     # symmetric: also column-major
+        bh = np.ascontiguousarray(B.cpu().numpy())     # nrhs x n = column-major n x nrhs
+        xh = np.zeros_like(bh)
+        L.plasma_dsposv_ex(pb.PlasmaLower, n, nrhs, ah.ctypes.data, n, bh.ctypes.data, n,
+                           xh.ctypes.data, n, ctypes.byref(it), None)
+        torch.cuda.synchronize()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record()
+        rc = L.plasma_dsposv_ex(pb.PlasmaLower, n, nrhs, ah.ctypes.data, n, bh.ctypes.data,
+                                n, xh.ctypes.data, n, ctypes.byref(it), None)
+        g1.record()
+        torch.cuda.synchronize()
+        assert rc == 0
+        ems = g0.elapsed_time(g1)
+        nbv = L.plasma_tuning_get_potrf_nb(pb.PlasmaRealFloat, n) if args.nb == 0 else args.nb
+        h2d = sum((n - c0) * min(nbv, n - c0) for c0 in range(0, n, nbv)) * 8 + n * nrhs * 8
+        e2e = {"value": flops_of(n, nrhs) / ems / 1e6, "unit": "GFLOP/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(n * nrhs * 8),
+               "ms_per_step": ems}
+        del ah
+
+    cpu = None
+    if not args.no_cpu and rank == 0:
+        cpu = cpu_baseline(args.cpu_n, nrhs, args.kappa)
+        cpu.pop("seconds", None)
+
+    if rank != 0:
+        L.plasma_finalize()
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return 0
+
+    upd = prof["update"]
+    mode_peak = {"fp32": ("fp32", peaks.get("fp32")), "tf32": ("tf32", peaks.get("tf32")),
+                 "bf16": ("bf16", peaks.get("bf16")), "auto": ("bf16", peaks.get("bf16"))}
+    pk_name, pk = mode_peak[args.mode]
+    achieved = upd["flops"] / upd["ms"] / 1e9 if upd["ms"] > 0 else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "update_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(args.mode)
+        except Exception:
+            traffic = None
+    value = world * flops_of(n, nrhs) / ms / 1e6
+    line = {
+        "metric": "dsposv FP64-equivalent throughput to FP64 backward error "
+                  "(vs dposv) at n=32768 on 1 B200",
+        "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic",
+        "config": {"workload": f"dsposv n={n} nrhs={nrhs} A=Q diag(lambda) Q^T "
+                               f"kappa={args.kappa:g} seed 11, uplo=L",
+                   "factor": args.mode, "refinement": args.refine,
+                   "nb": args.nb or L.plasma_tuning_get_potrf_nb(pb.PlasmaRealFloat, n),
+                   "l2": "inputs larger than L2 (A is 8.6 GB)",
+                   "parallelism": f"replicas x{world}"},
+        "iter": iters, "backward_error": berr, "forward_error": ferr,
+        "backward_error_target": 50 * n * 2.0 ** -53,
+        "dposv": dposv,
+        "speedup_vs_dposv": (dposv["ms"] / ms) if dposv else None,
+        "roofline": {"bound": "tensor" if args.mode != "fp32" else "fp32-simt",
+                     "kernel": "trailing update (SYRK+GEMM)",
+                     "achieved": achieved / 1e3 if achieved else None,
+                     "peak": pk / 1e3 if pk else None, "unit": "TFLOP/s",
+                     "frac": (achieved / pk) if achieved and pk else None,
+                     "peak_source": f"{pk_name} cuBLAS GEMM measured live"
+                     if pk_name != "bf16" else "MEASURED_PEAKS.json bf16_tflops",
+                     "traffic": traffic,
+                     "launches": upd["launches"], "avg_launch_ms": upd["ms"] / max(1, upd["launches"])},
+        "phases_ms_per_step": {k: v["ms"] / args.steps for k, v in prof.items()},
+        "peaks_tflops": {k: (v / 1e3 if isinstance(v, float) and k not in ("hbm_gbs",) else v)
+                         for k, v in peaks.items()},
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "gpu_launches": int(launches),
+    }
+    print(json.dumps(line), flush=True)
+    L.plasma_finalize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,88 @@
+"""ctypes binding of the CPU oracle (test infrastructure only).
+
+Loaded by tests/, __graft_entry__.smoke() and the CPU-baseline leg of
+bench.py to check or time against; the product library never uses it.
+"""
+import ctypes
+import os
+import subprocess
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liboracle.so")
+UPPER, LOWER = 121, 122
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        vp, ci = ctypes.c_void_p, ctypes.c_int
+        for p in ("d", "s"):
+            getattr(L, f"{p}oracle_potrf").argtypes = [ci, ci, vp, ci, ci]
+            getattr(L, f"{p}oracle_potrs").argtypes = [ci, ci, ci, vp, ci, vp, ci, ci]
+            getattr(L, f"{p}oracle_posv").argtypes = [ci, ci, ci, vp, ci, vp, ci, ci]
+            for f in ("potrf", "potrs", "posv"):
+                getattr(L, f"{p}oracle_{f}").restype = ci
+        L.oracle_dsposv.argtypes = [ci, ci, ci, vp, ci, vp, ci, vp, ci,
+                                    ctypes.POINTER(ci), ci]
+        L.oracle_dsposv.restype = ci
+        L.oracle_dlansy_inf.argtypes = [ci, ci, vp, ci]
+        L.oracle_dlansy_inf.restype = ctypes.c_double
+        L.oracle_set_threads.argtypes = [ci]
+        L.oracle_get_threads.restype = ci
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _prefix(a):
+    import numpy as np
+    return "d" if a.dtype == np.float64 else "s"
+
+
+def potrf(uplo, a, nb):
+    """In-place tile Cholesky of the Fortran-ordered array a; returns info."""
+    n = a.shape[0]
+    return getattr(lib(), f"{_prefix(a)}oracle_potrf")(uplo, n, _p(a), a.shape[0], nb)
+
+
+def potrs(uplo, a, b, nb):
+    n, nrhs = b.shape
+    return getattr(lib(), f"{_prefix(a)}oracle_potrs")(uplo, n, nrhs, _p(a),
+                                                       a.shape[0], _p(b), b.shape[0], nb)
+
+
+def posv(uplo, a, b, nb):
+    n, nrhs = b.shape
+    return getattr(lib(), f"{_prefix(a)}oracle_posv")(uplo, n, nrhs, _p(a),
+                                                      a.shape[0], _p(b), b.shape[0], nb)
+
+
+def dsposv(uplo, a, b, x, nb):
+    it = ctypes.c_int(0)
+    n, nrhs = b.shape
+    info = lib().oracle_dsposv(uplo, n, nrhs, _p(a), a.shape[0], _p(b), b.shape[0],
+                               _p(x), x.shape[0], ctypes.byref(it), nb)
+    return info, it.value
+
+
+def lansy_inf(uplo, a):
+    return lib().oracle_dlansy_inf(uplo, a.shape[0], _p(a), a.shape[0])
+
+
+def set_threads(n):
+    lib().oracle_set_threads(n)
+
+
+def get_threads():
+    return lib().oracle_get_threads()

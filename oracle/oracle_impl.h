@@ -1,0 +1,424 @@
+/*
+ * oracle_impl.h -- precision-generic body of the CPU oracle (TEST
+ * INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the CPU
+ * baseline of bench.py as the checker, never by the product library).
+ *
+ * Included by plasma_oracle.c once with REAL=double, P(x)=d##x and once with
+ * REAL=float, P(x)=s##x.  It restates, on its own tile storage, the
+ * reference's algorithms:
+ *   tile Cholesky        compute/pzpotrf.c:27-126
+ *   tile triangular solve compute/pztrsm.c:113-177 (Left, Lower) and
+ *                        :43-107 (Left, Upper)
+ *   the LAPACK/BLAS tile kernels the reference calls through CBLAS/LAPACKE
+ *   (core_blas/core_zpotrf.c:54-63, core_ztrsm.c:87-100, core_zsyrk.c,
+ *   core_zgemm.c:89-102), written out from the published LAPACK algorithms
+ *   (dpotf2: unblocked Cholesky with the "ajj <= 0 or NaN" test; dtrsm,
+ *   dsyrk, dgemm: the reference BLAS loop orders).
+ * The tile DAG runs as OpenMP tasks with depend() on tile base pointers, as
+ * in core_blas/core_zgemm.c:125-127.
+ */
+
+/* ---- tile storage: tiles[(m) + mt*(n)] each column-major, ld = rows ---- */
+typedef struct {
+    int n, nb, mt;
+    REAL **t;
+} P(tiles_t);
+
+static int P(tile_rows)(const P(tiles_t) *T, int m)
+{
+    return m < T->mt - 1 ? T->nb : T->n - T->nb * (T->mt - 1);
+}
+
+static int P(tiles_alloc)(P(tiles_t) *T, int n, int nb, int ncols)
+{
+    T->n = n;
+    T->nb = nb;
+    T->mt = (n + nb - 1) / nb;
+    int nt = (ncols + nb - 1) / nb;
+    if (nt < 1) nt = 1;
+    T->t = (REAL **)calloc((size_t)T->mt * nt, sizeof(REAL *));
+    if (!T->t) return -1;
+    for (int j = 0; j < nt; j++)
+        for (int i = 0; i < T->mt; i++) {
+            int r = P(tile_rows)(T, i);
+            int c = j < nt - 1 ? nb : ncols - nb * (nt - 1);
+            if (c <= 0) c = 1;
+            T->t[i + (size_t)T->mt * j] = (REAL *)calloc((size_t)r * c, sizeof(REAL));
+        }
+    return 0;
+}
+
+static void P(tiles_free)(P(tiles_t) *T, int ncols)
+{
+    int nt = (ncols + T->nb - 1) / T->nb;
+    if (nt < 1) nt = 1;
+    for (size_t i = 0; i < (size_t)T->mt * nt; i++) free(T->t[i]);
+    free(T->t);
+}
+
+#define TL(T, m, n) ((T)->t[(m) + (size_t)(T)->mt * (n)])
+
+static void P(to_tiles)(P(tiles_t) *T, const REAL *A, int lda, int ncols)
+{
+    int nb = T->nb;
+    for (int j = 0; j < ncols; j++)
+        for (int i = 0; i < T->n; i++) {
+            int m = i / nb, k = j / nb;
+            TL(T, m, k)[(size_t)(j - k * nb) * P(tile_rows)(T, m) + (i - m * nb)] =
+                A[(size_t)j * lda + i];
+        }
+}
+
+static void P(from_tiles)(const P(tiles_t) *T, REAL *A, int lda, int ncols,
+                          int uplo)
+{
+    int nb = T->nb;
+    for (int j = 0; j < ncols; j++)
+        for (int i = 0; i < T->n; i++) {
+            int m = i / nb, k = j / nb;
+            /* full diagonal tiles are copied, as the reference's desc2tr does */
+            if (uplo == ORACLE_LOWER && m < k) continue;
+            if (uplo == ORACLE_UPPER && m > k) continue;
+            A[(size_t)j * lda + i] =
+                TL(T, m, k)[(size_t)(j - k * nb) * P(tile_rows)(T, m) + (i - m * nb)];
+        }
+}
+
+/* ---------------- tile kernels (LAPACK / reference BLAS algorithms) ------ */
+
+/* dpotf2, lower: A = L L^T; returns 0 or the failing column (1-based) */
+static int P(k_potrf_lower)(int n, REAL *A, int lda)
+{
+    for (int j = 0; j < n; j++) {
+        REAL ajj = A[j + (size_t)j * lda];
+        for (int k = 0; k < j; k++)
+            ajj -= A[j + (size_t)k * lda] * A[j + (size_t)k * lda];
+        if (!(ajj > 0)) {
+            A[j + (size_t)j * lda] = ajj;
+            return j + 1;
+        }
+        ajj = (REAL)sqrt((double)ajj);
+        A[j + (size_t)j * lda] = ajj;
+        /* A(j+1:n, j) -= A(j+1:n, 0:j) * A(j, 0:j)^T ; then scale */
+        for (int k = 0; k < j; k++) {
+            REAL ajk = A[j + (size_t)k * lda];
+            for (int i = j + 1; i < n; i++)
+                A[i + (size_t)j * lda] -= A[i + (size_t)k * lda] * ajk;
+        }
+        REAL r = (REAL)1 / ajj;
+        for (int i = j + 1; i < n; i++)
+            A[i + (size_t)j * lda] *= r;
+    }
+    return 0;
+}
+
+/* dpotf2, upper: A = U^T U */
+static int P(k_potrf_upper)(int n, REAL *A, int lda)
+{
+    for (int j = 0; j < n; j++) {
+        REAL ajj = A[j + (size_t)j * lda];
+        for (int k = 0; k < j; k++)
+            ajj -= A[k + (size_t)j * lda] * A[k + (size_t)j * lda];
+        if (!(ajj > 0)) {
+            A[j + (size_t)j * lda] = ajj;
+            return j + 1;
+        }
+        ajj = (REAL)sqrt((double)ajj);
+        A[j + (size_t)j * lda] = ajj;
+        REAL r = (REAL)1 / ajj;
+        for (int c = j + 1; c < n; c++) {
+            REAL s = A[j + (size_t)c * lda];
+            for (int k = 0; k < j; k++)
+                s -= A[k + (size_t)j * lda] * A[k + (size_t)c * lda];
+            A[j + (size_t)c * lda] = s * r;
+        }
+    }
+    return 0;
+}
+
+/* B(m x n) <- B * L^{-T}, L lower n x n (Right, Lower, Trans, NonUnit) */
+static void P(k_trsm_rlt)(int m, int n, const REAL *L, int ldl, REAL *B, int ldb)
+{
+    for (int k = 0; k < n; k++) {
+        REAL r = (REAL)1 / L[k + (size_t)k * ldl];
+        for (int i = 0; i < m; i++) B[i + (size_t)k * ldb] *= r;
+        for (int j = k + 1; j < n; j++) {
+            REAL ljk = L[j + (size_t)k * ldl];
+            if (ljk != 0)
+                for (int i = 0; i < m; i++)
+                    B[i + (size_t)j * ldb] -= ljk * B[i + (size_t)k * ldb];
+        }
+    }
+}
+
+/* B(m x n) <- U^{-T} B, U upper m x m (Left, Upper, Trans, NonUnit) */
+static void P(k_trsm_lut)(int m, int n, const REAL *U, int ldu, REAL *B, int ldb)
+{
+    for (int j = 0; j < n; j++)
+        for (int i = 0; i < m; i++) {
+            REAL s = B[i + (size_t)j * ldb];
+            for (int k = 0; k < i; k++)
+                s -= U[k + (size_t)i * ldu] * B[k + (size_t)j * ldb];
+            B[i + (size_t)j * ldb] = s / U[i + (size_t)i * ldu];
+        }
+}
+
+/* B <- L^{-1} B (Left, Lower, NoTrans) */
+static void P(k_trsm_lln)(int m, int n, const REAL *L, int ldl, REAL *B, int ldb)
+{
+    for (int j = 0; j < n; j++)
+        for (int k = 0; k < m; k++) {
+            REAL bk = B[k + (size_t)j * ldb] / L[k + (size_t)k * ldl];
+            B[k + (size_t)j * ldb] = bk;
+            for (int i = k + 1; i < m; i++)
+                B[i + (size_t)j * ldb] -= bk * L[i + (size_t)k * ldl];
+        }
+}
+
+/* B <- L^{-T} B (Left, Lower, Trans) */
+static void P(k_trsm_llt)(int m, int n, const REAL *L, int ldl, REAL *B, int ldb)
+{
+    for (int j = 0; j < n; j++)
+        for (int i = m - 1; i >= 0; i--) {
+            REAL s = B[i + (size_t)j * ldb];
+            for (int k = i + 1; k < m; k++)
+                s -= L[k + (size_t)i * ldl] * B[k + (size_t)j * ldb];
+            B[i + (size_t)j * ldb] = s / L[i + (size_t)i * ldl];
+        }
+}
+
+/* B <- U^{-1} B (Left, Upper, NoTrans) */
+static void P(k_trsm_lun)(int m, int n, const REAL *U, int ldu, REAL *B, int ldb)
+{
+    for (int j = 0; j < n; j++)
+        for (int k = m - 1; k >= 0; k--) {
+            REAL bk = B[k + (size_t)j * ldb] / U[k + (size_t)k * ldu];
+            B[k + (size_t)j * ldb] = bk;
+            for (int i = 0; i < k; i++)
+                B[i + (size_t)j * ldb] -= bk * U[i + (size_t)k * ldu];
+        }
+}
+
+/* C(m x n) -= A(m x k) B(n x k)^T ; lower_only restricts to i >= j */
+static void P(k_gemm_nt)(int m, int n, int k, const REAL *A, int lda,
+                         const REAL *B, int ldb, REAL *C, int ldc, int lower_only)
+{
+    for (int j = 0; j < n; j++) {
+        int i0 = lower_only ? j : 0;
+        REAL *c = C + (size_t)j * ldc;
+        int l = 0;
+        for (; l + 4 <= k; l += 4) {
+            REAL b0 = B[j + (size_t)l * ldb], b1 = B[j + (size_t)(l + 1) * ldb];
+            REAL b2 = B[j + (size_t)(l + 2) * ldb], b3 = B[j + (size_t)(l + 3) * ldb];
+            const REAL *a0 = A + (size_t)l * lda, *a1 = a0 + lda;
+            const REAL *a2 = a1 + lda, *a3 = a2 + lda;
+            for (int i = i0; i < m; i++)
+                c[i] -= a0[i] * b0 + a1[i] * b1 + a2[i] * b2 + a3[i] * b3;
+        }
+        for (; l < k; l++) {
+            REAL b0 = B[j + (size_t)l * ldb];
+            const REAL *a0 = A + (size_t)l * lda;
+            for (int i = i0; i < m; i++) c[i] -= a0[i] * b0;
+        }
+    }
+}
+
+/* C(m x n) -= A(k x m)^T B(k x n) ; upper_only restricts to i <= j */
+static void P(k_gemm_tn)(int m, int n, int k, const REAL *A, int lda,
+                         const REAL *B, int ldb, REAL *C, int ldc, int upper_only)
+{
+    for (int j = 0; j < n; j++)
+        for (int i = 0; i < (upper_only ? (j + 1 < m ? j + 1 : m) : m); i++) {
+            REAL s = 0;
+            const REAL *a = A + (size_t)i * lda, *b = B + (size_t)j * ldb;
+            for (int l = 0; l < k; l++) s += a[l] * b[l];
+            C[i + (size_t)j * ldc] -= s;
+        }
+}
+
+/* C(m x n) -= A(m x k) B(k x n) */
+static void P(k_gemm_nn)(int m, int n, int k, const REAL *A, int lda,
+                         const REAL *B, int ldb, REAL *C, int ldc)
+{
+    for (int j = 0; j < n; j++)
+        for (int l = 0; l < k; l++) {
+            REAL b = B[l + (size_t)j * ldb];
+            const REAL *a = A + (size_t)l * lda;
+            REAL *c = C + (size_t)j * ldc;
+            for (int i = 0; i < m; i++) c[i] -= a[i] * b;
+        }
+}
+
+/* ---------------- parallel tile algorithms ------------------------------ */
+
+/* compute/pzpotrf.c:27-126 ; returns info (nb*k + local) or 0 */
+static int P(p_potrf)(P(tiles_t) *A, int uplo)
+{
+    int info = 0;
+    const int mt = A->mt, nb = A->nb;
+    #pragma omp parallel
+    #pragma omp master
+    {
+        for (int k = 0; k < mt; k++) {
+            REAL *akk = TL(A, k, k);
+            int nk = P(tile_rows)(A, k);
+            #pragma omp task depend(inout: akk[0]) shared(info)
+            {
+                int st;
+                #pragma omp atomic read
+                st = info;
+                if (st == 0) {
+                    int i = uplo == ORACLE_LOWER ? P(k_potrf_lower)(nk, akk, nk)
+                                                 : P(k_potrf_upper)(nk, akk, nk);
+                    if (i != 0) {
+                        #pragma omp critical (oracle_info)
+                        if (info == 0) info = nb * k + i;
+                    }
+                }
+            }
+            for (int m = k + 1; m < mt; m++) {
+                int nm = P(tile_rows)(A, m);
+                if (uplo == ORACLE_LOWER) {
+                    REAL *amk = TL(A, m, k);
+                    #pragma omp task depend(in: akk[0]) depend(inout: amk[0]) shared(info)
+                    if (info == 0) P(k_trsm_rlt)(nm, nk, akk, nk, amk, nm);
+                } else {
+                    REAL *akm = TL(A, k, m);
+                    #pragma omp task depend(in: akk[0]) depend(inout: akm[0]) shared(info)
+                    if (info == 0) P(k_trsm_lut)(nk, nm, akk, nk, akm, nk);
+                }
+            }
+            for (int m = k + 1; m < mt; m++) {
+                int nm = P(tile_rows)(A, m);
+                for (int n = k + 1; n <= m; n++) {
+                    int nn = P(tile_rows)(A, n);
+                    if (uplo == ORACLE_LOWER) {
+                        REAL *amk = TL(A, m, k), *ank = TL(A, n, k), *amn = TL(A, m, n);
+                        #pragma omp task depend(in: amk[0], ank[0]) depend(inout: amn[0]) shared(info)
+                        if (info == 0)
+                            P(k_gemm_nt)(nm, nn, nk, amk, nm, ank, nn, amn, nm, m == n);
+                    } else {
+                        /* A(n,m) -= A(k,n)^T A(k,m) */
+                        REAL *akn = TL(A, k, n), *akm = TL(A, k, m), *anm = TL(A, n, m);
+                        #pragma omp task depend(in: akn[0], akm[0]) depend(inout: anm[0]) shared(info)
+                        if (info == 0)
+                            P(k_gemm_tn)(nn, nm, nk, akn, nk, akm, nk, anm, nn, m == n);
+                    }
+                }
+            }
+        }
+    }
+    return info;
+}
+
+/* compute/pztrsm.c (Left): trans = 0 solves op = L (or U^T), 1 solves L^T (or U)
+ * B is n x nrhs in tiles (B->mt row tiles, one column block per nb cols). */
+static void P(p_trsm)(P(tiles_t) *A, P(tiles_t) *B, int nrhs, int uplo, int second)
+{
+    const int mt = A->mt, nb = A->nb;
+    const int nt = (nrhs + nb - 1) / nb;
+    #pragma omp parallel
+    #pragma omp master
+    for (int step = 0; step < mt; step++) {
+        /* forward sweep for (Lower,NoTrans) and (Upper,Trans); backward else */
+        int k = second ? mt - 1 - step : step;
+        int nk = P(tile_rows)(A, k);
+        REAL *akk = TL(A, k, k);
+        for (int n = 0; n < nt; n++) {
+            int nc = n < nt - 1 ? nb : nrhs - nb * (nt - 1);
+            REAL *bkn = TL(B, k, n);
+            #pragma omp task depend(in: akk[0]) depend(inout: bkn[0])
+            {
+                if (uplo == ORACLE_LOWER) {
+                    if (!second) P(k_trsm_lln)(nk, nc, akk, nk, bkn, nk);
+                    else         P(k_trsm_llt)(nk, nc, akk, nk, bkn, nk);
+                } else {
+                    if (!second) P(k_trsm_lut)(nk, nc, akk, nk, bkn, nk);
+                    else         P(k_trsm_lun)(nk, nc, akk, nk, bkn, nk);
+                }
+            }
+        }
+        int mlo = second ? 0 : k + 1, mhi = second ? k : mt;
+        for (int m = mlo; m < mhi; m++) {
+            int nm = P(tile_rows)(A, m);
+            for (int n = 0; n < nt; n++) {
+                int nc = n < nt - 1 ? nb : nrhs - nb * (nt - 1);
+                REAL *bkn = TL(B, k, n), *bmn = TL(B, m, n);
+                if (uplo == ORACLE_LOWER) {
+                    if (!second) {        /* B(m) -= L(m,k) B(k) */
+                        REAL *amk = TL(A, m, k);
+                        #pragma omp task depend(in: amk[0], bkn[0]) depend(inout: bmn[0])
+                        P(k_gemm_nn)(nm, nc, nk, amk, nm, bkn, nk, bmn, nm);
+                    } else {              /* B(m) -= L(k,m)^T B(k) */
+                        REAL *akm = TL(A, k, m);
+                        #pragma omp task depend(in: akm[0], bkn[0]) depend(inout: bmn[0])
+                        P(k_gemm_tn)(nm, nc, nk, akm, nk, bkn, nk, bmn, nm, 0);
+                    }
+                } else {
+                    if (!second) {        /* B(m) -= U(k,m)^T B(k) */
+                        REAL *akm = TL(A, k, m);
+                        #pragma omp task depend(in: akm[0], bkn[0]) depend(inout: bmn[0])
+                        P(k_gemm_tn)(nm, nc, nk, akm, nk, bkn, nk, bmn, nm, 0);
+                    } else {              /* B(m) -= U(m,k) B(k) */
+                        REAL *amk = TL(A, m, k);
+                        #pragma omp task depend(in: amk[0], bkn[0]) depend(inout: bmn[0])
+                        P(k_gemm_nn)(nm, nc, nk, amk, nm, bkn, nk, bmn, nm);
+                    }
+                }
+            }
+        }
+    }
+}
+
+/* ---------------- LAPACK-layout entry points ---------------------------- */
+
+int P(oracle_potrf)(int uplo, int n, REAL *A, int lda, int nb)
+{
+    if (n == 0) return 0;
+    P(tiles_t) T;
+    P(tiles_alloc)(&T, n, nb, n);
+    P(to_tiles)(&T, A, lda, n);
+    int info = P(p_potrf)(&T, uplo);
+    if (info == 0)
+        P(from_tiles)(&T, A, lda, n, uplo);
+    P(tiles_free)(&T, n);
+    return info;
+}
+
+int P(oracle_potrs)(int uplo, int n, int nrhs, const REAL *A, int lda,
+                    REAL *B, int ldb, int nb)
+{
+    if (n == 0 || nrhs == 0) return 0;
+    P(tiles_t) TA, TB;
+    P(tiles_alloc)(&TA, n, nb, n);
+    P(tiles_alloc)(&TB, n, nb, nrhs);
+    P(to_tiles)(&TA, A, lda, n);
+    P(to_tiles)(&TB, B, ldb, nrhs);
+    P(p_trsm)(&TA, &TB, nrhs, uplo, 0);
+    P(p_trsm)(&TA, &TB, nrhs, uplo, 1);
+    P(from_tiles)(&TB, B, ldb, nrhs, 0);
+    P(tiles_free)(&TA, n);
+    P(tiles_free)(&TB, nrhs);
+    return 0;
+}
+
+int P(oracle_posv)(int uplo, int n, int nrhs, REAL *A, int lda, REAL *B,
+                   int ldb, int nb)
+{
+    if (n == 0 || nrhs == 0) return 0;
+    P(tiles_t) TA, TB;
+    P(tiles_alloc)(&TA, n, nb, n);
+    P(tiles_alloc)(&TB, n, nb, nrhs);
+    P(to_tiles)(&TA, A, lda, n);
+    P(to_tiles)(&TB, B, ldb, nrhs);
+    int info = P(p_potrf)(&TA, uplo);
+    if (info == 0) {
+        P(p_trsm)(&TA, &TB, nrhs, uplo, 0);
+        P(p_trsm)(&TA, &TB, nrhs, uplo, 1);
+        P(from_tiles)(&TA, A, lda, n, uplo);
+        P(from_tiles)(&TB, B, ldb, nrhs, 0);
+    }
+    P(tiles_free)(&TA, n);
+    P(tiles_free)(&TB, nrhs);
+    return info;
+}

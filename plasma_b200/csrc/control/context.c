@@ -1,0 +1,346 @@
+/*
+ * context.c -- library lifetime and configuration.
+ *
+ * Follows the reference's control/context.c:
+ *   plasma_init      :30-47   (second init -> PlasmaErrorNotInitialized)
+ *   plasma_finalize  :54-71
+ *   plasma_set       :78-127  (PlasmaNb <= 0 -> PlasmaErrorIllegalValue)
+ *   plasma_get       :133-159
+ *   defaults         :165-180 (nb 256, ib 64, tuning enabled)
+ * There is one global context, as in the reference (:22-23).  In place of the
+ * OpenMP team the context owns a CUDA device, a sequence stream, look-ahead
+ * streams and the device status word that kernels use for cooperative
+ * cancellation.
+ */
+#include "../internal.h"
+
+#include <cuda_runtime_api.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+static int plasma_initialized_g = 0;
+static plasma_context_t plasma_context_g;
+static int plasma_device_request_g = 0;   /* PlasmaDevice set before init */
+long long plasma_launch_count_g = 0;
+
+plasma_context_t *plasma_context_self(void)
+{
+    return plasma_initialized_g ? &plasma_context_g : NULL;
+}
+
+static void context_defaults(plasma_context_t *c)
+{
+    memset(c, 0, sizeof(*c));
+    c->tuning = PlasmaEnabled;
+    c->nb = 256;
+    c->ib = 64;
+    c->inplace_outplace = PlasmaOutplace;
+    c->max_threads = 1;
+    c->max_panel_threads = 1;
+    c->householder_mode = PlasmaFlatHouseholder;
+    c->mixed_mode = PlasmaFactorFP32;
+    c->refinement = PlasmaRefineIR;
+    c->lookahead = 1;
+    c->next_call = 1;
+}
+
+int plasma_init(void)
+{
+    if (plasma_initialized_g)
+        return PlasmaErrorNotInitialized;
+
+    plasma_context_t *c = &plasma_context_g;
+    context_defaults(c);
+    c->device = plasma_device_request_g;
+
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        /* Host-only mode: lets argument checking and descriptor arithmetic
+         * be exercised on machines without a GPU.  Every routine that would
+         * touch the device returns PlasmaErrorEnvironment instead. */
+        const char *env = getenv("PLASMA_ALLOW_NO_DEVICE");
+        if (env && env[0] == '1') {
+            c->device = -1;
+            plasma_initialized_g = 1;
+            return PlasmaSuccess;
+        }
+        plasma_error("no CUDA device available");
+        return PlasmaErrorEnvironment;
+    }
+    if (c->device < 0 || c->device >= ndev) {
+        plasma_error("invalid CUDA device");
+        return PlasmaErrorIllegalValue;
+    }
+    if (cudaSetDevice(c->device) != cudaSuccess) {
+        plasma_error("cudaSetDevice() failed");
+        return PlasmaErrorEnvironment;
+    }
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount,
+                           c->device);
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking)
+            != cudaSuccess) {
+        plasma_error("cudaStreamCreate() failed");
+        return PlasmaErrorEnvironment;
+    }
+    c->stream = c->own_stream;
+    /* aux[0]: critical path (highest priority), aux[1..]: bulk updates */
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    for (int i = 0; i < PLASMA_NUM_STREAMS; i++)
+        cudaStreamCreateWithPriority(&c->aux[i], cudaStreamNonBlocking,
+                                     i == 0 ? prio_hi : prio_lo);
+    for (int i = 0; i < 8; i++)
+        cudaEventCreateWithFlags(&c->ev[i], cudaEventDisableTiming);
+    if (cudaMalloc((void **)&c->dstat, sizeof(plasma_devstat_t)) != cudaSuccess ||
+        cudaMallocHost((void **)&c->hstat, sizeof(plasma_devstat_t)) != cudaSuccess) {
+        plasma_error("cannot allocate the device status word");
+        return PlasmaErrorOutOfMemory;
+    }
+    cudaMemset(c->dstat, 0, sizeof(plasma_devstat_t));
+    cudaDeviceSynchronize();
+    plasma_initialized_g = 1;
+    return PlasmaSuccess;
+}
+
+int plasma_finalize(void)
+{
+    if (!plasma_initialized_g)
+        return PlasmaErrorNotInitialized;
+    plasma_context_t *c = &plasma_context_g;
+    if (c->device < 0) {
+        memset(c, 0, sizeof(*c));
+        plasma_initialized_g = 0;
+        return PlasmaSuccess;
+    }
+    cudaSetDevice(c->device);
+    cudaDeviceSynchronize();
+    for (int i = 0; i < PLASMA_SCRATCH_SLOTS; i++)
+        if (c->scratch[i]) cudaFree(c->scratch[i]);
+    for (int i = 0; i < 8; i++)
+        if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    if (c->pinned) cudaFreeHost(c->pinned);
+    if (c->dstat) cudaFree(c->dstat);
+    if (c->hstat) cudaFreeHost(c->hstat);
+    for (int i = 0; i < PLASMA_NUM_STREAMS; i++)
+        if (c->aux[i]) cudaStreamDestroy(c->aux[i]);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    memset(c, 0, sizeof(*c));
+    plasma_initialized_g = 0;
+    return PlasmaSuccess;
+}
+
+int plasma_set(plasma_enum_t param, int value)
+{
+    if (param == PlasmaDevice && !plasma_initialized_g) {
+        /* the device is chosen before plasma_init() */
+        if (value < 0) return PlasmaErrorIllegalValue;
+        plasma_device_request_g = value;
+        return PlasmaSuccess;
+    }
+    if (!plasma_initialized_g)
+        return PlasmaErrorNotInitialized;
+    plasma_context_t *c = &plasma_context_g;
+
+    switch (param) {
+    case PlasmaTuning:
+        if (value != PlasmaEnabled && value != PlasmaDisabled) {
+            plasma_error("invalid tuning flag");
+            return PlasmaErrorIllegalValue;
+        }
+        c->tuning = value;
+        break;
+    case PlasmaNb:
+        if (value <= 0) {
+            plasma_error("invalid tile size");
+            return PlasmaErrorIllegalValue;
+        }
+        c->nb = value;
+        break;
+    case PlasmaIb:
+        if (value <= 0) {
+            plasma_error("invalid inner block size");
+            return PlasmaErrorIllegalValue;
+        }
+        c->ib = value;
+        break;
+    case PlasmaNumPanelThreads:
+        if (value <= 0) {
+            plasma_error("invalid number of panel threads");
+            return PlasmaErrorIllegalValue;
+        }
+        c->max_panel_threads = value;
+        break;
+    case PlasmaHouseholderMode:
+        if (value != PlasmaFlatHouseholder && value != PlasmaTreeHouseholder) {
+            plasma_error("invalid Householder mode");
+            return PlasmaErrorIllegalValue;
+        }
+        c->householder_mode = value;
+        break;
+    case PlasmaMixedPrecisionMode:
+        if (value < PlasmaFactorFP32 || value > PlasmaFactorAuto) {
+            plasma_error("invalid mixed-precision mode");
+            return PlasmaErrorIllegalValue;
+        }
+        c->mixed_mode = value;
+        break;
+    case PlasmaRefinement:
+        if (value < PlasmaRefineIR || value > PlasmaRefineAuto) {
+            plasma_error("invalid refinement scheme");
+            return PlasmaErrorIllegalValue;
+        }
+        c->refinement = value;
+        break;
+    case PlasmaLookahead:
+        if (value < 0) {
+            plasma_error("invalid look-ahead depth");
+            return PlasmaErrorIllegalValue;
+        }
+        c->lookahead = value;
+        break;
+    case PlasmaDevice:
+        plasma_error("the device can only be set before plasma_init()");
+        return PlasmaErrorIllegalValue;
+    default:
+        plasma_error("unknown parameter");
+        return PlasmaErrorIllegalValue;
+    }
+    return PlasmaSuccess;
+}
+
+int plasma_get(plasma_enum_t param, int *value)
+{
+    if (!plasma_initialized_g)
+        return PlasmaErrorNotInitialized;
+    plasma_context_t *c = &plasma_context_g;
+    switch (param) {
+    case PlasmaTuning:             *value = c->tuning;            break;
+    case PlasmaNb:                 *value = c->nb;                break;
+    case PlasmaIb:                 *value = c->ib;                break;
+    case PlasmaNumPanelThreads:    *value = c->max_panel_threads; break;
+    case PlasmaHouseholderMode:    *value = c->householder_mode;  break;
+    case PlasmaMixedPrecisionMode: *value = c->mixed_mode;        break;
+    case PlasmaRefinement:         *value = c->refinement;        break;
+    case PlasmaLookahead:          *value = c->lookahead;         break;
+    case PlasmaDevice:             *value = c->device;            break;
+    default:
+        plasma_error("Unknown parameter");
+        return PlasmaErrorIllegalValue;
+    }
+    return PlasmaSuccess;
+}
+
+void plasma_version(int *major, int *minor, int *micro)
+{
+    *major = PLASMA_VERSION_MAJOR;
+    *minor = PLASMA_VERSION_MINOR;
+    *micro = PLASMA_VERSION_PATCH;
+}
+
+int plasma_set_stream(void *stream)
+{
+    if (!plasma_initialized_g)
+        return PlasmaErrorNotInitialized;
+    plasma_context_g.stream = stream ? (cudaStream_t)stream
+                                     : plasma_context_g.own_stream;
+    return PlasmaSuccess;
+}
+
+void *plasma_get_stream(void)
+{
+    if (!plasma_initialized_g)
+        return NULL;
+    return (void *)plasma_context_g.stream;
+}
+
+long long plasma_kernel_launches(void)
+{
+    return plasma_launch_count_g;
+}
+
+int plasma_call_begin(plasma_context_t *c, plasma_sequence_t *sequence,
+                      plasma_request_t *request)
+{
+    int id = c->next_call++;
+    if (c->next_call >= PLASMA_MAX_PENDING_CALLS)
+        c->next_call = 1;
+    c->pending[id] = request;
+    c->pending_seq[id] = sequence;
+    return id;
+}
+
+void *plasma_scratch(plasma_context_t *c, int slot, size_t bytes)
+{
+    if (bytes <= c->scratch_bytes[slot])
+        return c->scratch[slot];
+    if (c->scratch[slot]) {
+        /* growing: wait for every user of the old buffer */
+        cudaStreamSynchronize(c->stream);
+        for (int i = 0; i < PLASMA_NUM_STREAMS; i++)
+            cudaStreamSynchronize(c->aux[i]);
+        cudaFree(c->scratch[slot]);
+        c->scratch[slot] = NULL;
+        c->scratch_bytes[slot] = 0;
+    }
+    size_t want = bytes + bytes / 8 + (1u << 20);
+    if (cudaMalloc(&c->scratch[slot], want) != cudaSuccess) {
+        cudaGetLastError();
+        c->scratch[slot] = NULL;
+        return NULL;
+    }
+    c->scratch_bytes[slot] = want;
+    return c->scratch[slot];
+}
+
+void *plasma_pinned(plasma_context_t *c, size_t bytes)
+{
+    if (bytes <= c->pinned_bytes)
+        return c->pinned;
+    if (c->pinned) {
+        cudaStreamSynchronize(c->stream);
+        cudaFreeHost(c->pinned);
+        c->pinned = NULL;
+        c->pinned_bytes = 0;
+    }
+    if (cudaMallocHost(&c->pinned, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        c->pinned = NULL;
+        return NULL;
+    }
+    c->pinned_bytes = bytes;
+    return c->pinned;
+}
+
+int plasma_is_device_pointer(const void *p)
+{
+    struct cudaPointerAttributes attr;
+    if (p == NULL)
+        return 0;
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return attr.type == cudaMemoryTypeDevice ||
+           attr.type == cudaMemoryTypeManaged;
+}
+
+const char *plasma_strerror(int code)
+{
+    switch (code) {
+    case PlasmaSuccess:             return "success";
+    case PlasmaErrorNotInitialized: return "PLASMA not initialized";
+    case PlasmaErrorNotSupported:   return "not supported";
+    case PlasmaErrorIllegalValue:   return "illegal value";
+    case PlasmaErrorOutOfMemory:    return "out of memory";
+    case PlasmaErrorNullParameter:  return "NULL parameter";
+    case PlasmaErrorInternal:       return "internal error";
+    case PlasmaErrorSequence:       return "sequence error";
+    case PlasmaErrorComponent:      return "component error";
+    case PlasmaErrorEnvironment:    return "environment error";
+    default:
+        return code > 0 ? "matrix not positive definite (leading minor)"
+                        : "illegal argument";
+    }
+}

@@ -1,0 +1,72 @@
+/*
+ * tuning.c -- tile-size selection behind the PlasmaTuning switch.
+ *
+ * The reference asks a Lua script for nb (plasma_tune_potrf / plasma_tune_trsm,
+ * control/tuning.c:367-374,427-434; potrf_nb returns 256 in
+ * tuning/default.lua:125-127) and, like here, writes the answer into the
+ * context's nb.  Without a script nb stays at the plasma_set value.
+ *
+ * The GPU build keeps a small table of tile sizes per (precision, size
+ * bucket).  It starts from built-in defaults measured on B200 and can be
+ * refreshed at run time by plasma_autotune_potrf(), which times the candidate
+ * tile sizes {128, 256, 384, 512} on a synthetic SPD matrix and stores the
+ * fastest one for that bucket.
+ */
+#include "../internal.h"
+
+#include <stdlib.h>
+
+#define NBUCKETS 8
+
+/* bucket b covers n < 1024 << b (the last bucket is open-ended) */
+static int bucket_of(int n)
+{
+    int b = 0;
+    while (b < NBUCKETS - 1 && n >= (1024 << b))
+        b++;
+    return b;
+}
+
+/* [0] FP64, [1] FP32; 0 = no entry (keep plasma->nb) */
+static int potrf_table[2][NBUCKETS] = {
+    /* <1k  <2k  <4k  <8k  <16k <32k <64k  rest */
+    {  128, 128, 256, 256, 256, 256, 256,  256 },
+    {  128, 256, 256, 256, 256, 256, 256,  256 },
+};
+
+static int prec_index(plasma_enum_t dtyp)
+{
+    return dtyp == PlasmaRealDouble || dtyp == PlasmaComplexDouble ? 0 : 1;
+}
+
+void plasma_tune_potrf(plasma_context_t *plasma, plasma_enum_t dtyp, int n)
+{
+    const char *env = getenv("PLASMA_TUNING_DISABLE");
+    if (env && env[0] == '1')
+        return;
+    int nb = potrf_table[prec_index(dtyp)][bucket_of(n)];
+    if (nb > 0)
+        plasma->nb = nb;
+}
+
+void plasma_tune_trsm(plasma_context_t *plasma, plasma_enum_t dtyp, int m,
+                      int n)
+{
+    (void)n;
+    plasma_tune_potrf(plasma, dtyp, m);
+}
+
+/* Stores nb for the size bucket of n (GPU-build extension, used by the
+ * measured autotuner). */
+int plasma_tuning_set_potrf_nb(int dtyp, int n, int nb)
+{
+    if (nb <= 0 || nb > 1024)
+        return PlasmaErrorIllegalValue;
+    potrf_table[prec_index(dtyp)][bucket_of(n)] = nb;
+    return PlasmaSuccess;
+}
+
+int plasma_tuning_get_potrf_nb(int dtyp, int n)
+{
+    return potrf_table[prec_index(dtyp)][bucket_of(n)];
+}

@@ -1,0 +1,186 @@
+// layout.cu -- LAPACK column-major <-> tile layout, tile copies, tile
+// additions and precision conversions.
+//
+// Replaces the per-tile lacpy tasks of the reference's layout converters
+// (compute/pzge2desc.c:38-55, pztr2desc.c:31-50, pzdesc2ge.c, pzdesc2tr.c),
+// pzlacpy.c, pzgeadd.c, pzlag2c.c:47-85 and pclag2z.c:28-67 with one launch
+// per whole-matrix operation: one CTA per tile, threads striding down the
+// rows of a column so that global accesses are coalesced.  All kernels are
+// HBM-bandwidth bound (one read and one write of every element).
+#include "common.cuh"
+
+#include <float.h>
+
+namespace {
+
+constexpr int kThreads = 256;
+
+// Tile (m,n) of the view of A is visited when the uplo filter admits it.
+__device__ __forceinline__ bool tile_in(int uplo, int m, int n)
+{
+    return uplo == PlasmaLower ? n <= m : uplo == PlasmaUpper ? n >= m : true;
+}
+
+// Rows [y1,y2) x cols [x1,x2) of tile (m,n) that belong to the view
+// (reference compute/pzge2desc.c:42-46).
+struct TileBox {
+    int y1, y2, x1, x2;
+};
+__device__ __forceinline__ TileBox tile_box(const plasma_desc_t &A, int m, int n)
+{
+    TileBox b;
+    b.x1 = n == 0 ? A.j % A.nb : 0;
+    b.y1 = m == 0 ? A.i % A.mb : 0;
+    b.x2 = n == A.nt - 1 ? (A.j + A.n - 1) % A.nb + 1 : A.nb;
+    b.y2 = m == A.mt - 1 ? (A.i + A.m - 1) % A.mb + 1 : A.mb;
+    return b;
+}
+
+template <typename T, bool TO_TILE>
+__global__ void __launch_bounds__(kThreads)
+k_lapack_tile(plasma_desc_t A, int uplo, T *pA, int lda,
+              const plasma_devstat_t *st)
+{
+    if (plasma_failed(st)) return;
+    int m = blockIdx.x, n = blockIdx.y;
+    if (!tile_in(uplo, m, n)) return;
+    TileBox b = tile_box(A, m, n);
+    T *tile = (T *)plasma_tile_addr(A, m, n);
+    int ldt = plasma_tile_mmain(A, m);
+    T *f77 = pA + (size_t)A.nb * lda * n + (size_t)A.mb * m;
+    int rows = b.y2 - b.y1;
+    int total = rows * (b.x2 - b.x1);
+    for (int e = threadIdx.x; e < total; e += kThreads) {
+        int y = b.y1 + e % rows;
+        int x = b.x1 + e / rows;
+        if (TO_TILE)
+            tile[(size_t)x * ldt + y] = f77[(size_t)x * lda + y];
+        else
+            f77[(size_t)x * lda + y] = tile[(size_t)x * ldt + y];
+    }
+}
+
+// B(m,n) <- A(m,n) with optional precision conversion and the dlag2s
+// overflow test (info = 1 when |a| > FLT_MAX; NaN passes, as in LAPACK).
+template <typename TA, typename TB, bool CHECK>
+__global__ void __launch_bounds__(kThreads)
+k_tile_copy(plasma_desc_t A, plasma_desc_t B, int uplo,
+            plasma_devstat_t *st, int call)
+{
+    if (plasma_failed(st)) return;
+    int m = blockIdx.x, n = blockIdx.y;
+    if (!tile_in(uplo, m, n)) return;
+    int rows = plasma_tile_mview(A, m);
+    int cols = plasma_tile_nview(A, n);
+    const TA *a = (const TA *)plasma_tile_addr(A, m, n);
+    TB *b = (TB *)plasma_tile_addr(B, m, n);
+    int lda = plasma_tile_mmain(A, m);
+    int ldb = plasma_tile_mmain(B, m);
+    bool overflow = false;
+    for (int e = threadIdx.x; e < rows * cols; e += kThreads) {
+        int y = e % rows, x = e / rows;
+        TA v = a[(size_t)x * lda + y];
+        if (CHECK && (v > (TA)FLT_MAX || v < -(TA)FLT_MAX))
+            overflow = true;
+        b[(size_t)x * ldb + y] = (TB)v;
+    }
+    if (CHECK && __syncthreads_or(overflow) && threadIdx.x == 0)
+        plasma_fail(st, 1, call);
+}
+
+// X(m,n) += R(m,n)  (reference compute/pzgeadd.c:28-73 with alpha = beta = 1)
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_tile_add(plasma_desc_t R, plasma_desc_t X, const plasma_devstat_t *st)
+{
+    if (plasma_failed(st)) return;
+    int m = blockIdx.x, n = blockIdx.y;
+    int rows = plasma_tile_mview(X, m);
+    int cols = plasma_tile_nview(X, n);
+    const T *r = (const T *)plasma_tile_addr(R, m, n);
+    T *x = (T *)plasma_tile_addr(X, m, n);
+    int ldr = plasma_tile_mmain(R, m);
+    int ldx = plasma_tile_mmain(X, m);
+    for (int e = threadIdx.x; e < rows * cols; e += kThreads) {
+        int y = e % rows, c = e / rows;
+        x[(size_t)c * ldx + y] += r[(size_t)c * ldr + y];
+    }
+}
+
+dim3 tile_grid(const plasma_desc_t &A)
+{
+    return dim3((unsigned)A.mt, (unsigned)A.nt);
+}
+
+}  // namespace
+
+extern "C" void plasma_cuda_lapack_to_tile(cudaStream_t s, plasma_devstat_t *st,
+                                           plasma_desc_t A, plasma_enum_t uplo,
+                                           const void *pA, int lda)
+{
+    if (A.mt == 0 || A.nt == 0) return;
+    PLASMA_COUNT_LAUNCH();
+    if (A.precision == PlasmaRealDouble)
+        k_lapack_tile<double, true><<<tile_grid(A), kThreads, 0, s>>>(
+            A, uplo, (double *)pA, lda, st);
+    else
+        k_lapack_tile<float, true><<<tile_grid(A), kThreads, 0, s>>>(
+            A, uplo, (float *)pA, lda, st);
+}
+
+extern "C" void plasma_cuda_tile_to_lapack(cudaStream_t s, plasma_devstat_t *st,
+                                           plasma_desc_t A, plasma_enum_t uplo,
+                                           void *pA, int lda)
+{
+    if (A.mt == 0 || A.nt == 0) return;
+    PLASMA_COUNT_LAUNCH();
+    if (A.precision == PlasmaRealDouble)
+        k_lapack_tile<double, false><<<tile_grid(A), kThreads, 0, s>>>(
+            A, uplo, (double *)pA, lda, st);
+    else
+        k_lapack_tile<float, false><<<tile_grid(A), kThreads, 0, s>>>(
+            A, uplo, (float *)pA, lda, st);
+}
+
+extern "C" void plasma_cuda_lacpy(cudaStream_t s, plasma_devstat_t *st,
+                                  plasma_desc_t A, plasma_desc_t B)
+{
+    if (A.mt == 0 || A.nt == 0) return;
+    PLASMA_COUNT_LAUNCH();
+    if (A.precision == PlasmaRealDouble)
+        k_tile_copy<double, double, false><<<tile_grid(A), kThreads, 0, s>>>(
+            A, B, PlasmaGeneral, st, 0);
+    else
+        k_tile_copy<float, float, false><<<tile_grid(A), kThreads, 0, s>>>(
+            A, B, PlasmaGeneral, st, 0);
+}
+
+extern "C" void plasma_cuda_lag2s(cudaStream_t s, plasma_devstat_t *st, int call,
+                                  plasma_desc_t A, plasma_desc_t As,
+                                  plasma_enum_t uplo)
+{
+    if (A.mt == 0 || A.nt == 0) return;
+    PLASMA_COUNT_LAUNCH();
+    k_tile_copy<double, float, true><<<tile_grid(A), kThreads, 0, s>>>(
+        A, As, uplo, st, call);
+}
+
+extern "C" void plasma_cuda_slag2d(cudaStream_t s, plasma_devstat_t *st,
+                                   plasma_desc_t As, plasma_desc_t A)
+{
+    if (A.mt == 0 || A.nt == 0) return;
+    PLASMA_COUNT_LAUNCH();
+    k_tile_copy<float, double, false><<<tile_grid(As), kThreads, 0, s>>>(
+        As, A, PlasmaGeneral, st, 0);
+}
+
+extern "C" void plasma_cuda_geadd(cudaStream_t s, plasma_devstat_t *st,
+                                  plasma_desc_t R, plasma_desc_t X)
+{
+    if (X.mt == 0 || X.nt == 0) return;
+    PLASMA_COUNT_LAUNCH();
+    if (X.precision == PlasmaRealDouble)
+        k_tile_add<double><<<tile_grid(X), kThreads, 0, s>>>(R, X, st);
+    else
+        k_tile_add<float><<<tile_grid(X), kThreads, 0, s>>>(R, X, st);
+}

@@ -1,0 +1,159 @@
+// solve.cu -- blocked triangular solves with a tile Cholesky factor.
+//
+// potrs = two sweeps of plasma_pdtrsm (compute/zpotrs.c:270-282), Left/Lower
+// NoTrans then Trans (compute/pztrsm.c:113-177); upper storage solves with
+// U^T then U, which on the logical lower view (L = U^T) is the same pair.
+// Each tile step of a sweep is two launches:
+//   diag  : B(k,:) <- W_k B(k,:)      (W_k = inv(L_kk), precomputed for all
+//                                      k by k_trtri_tiles; replaces the
+//                                      per-tile trsm task)
+//   update: B(m,:) -= L(m,k) B(k,:)   for every m below k (forward) or
+//           B(m,:) -= L(k,m)^T B(k,:) for every m above k (backward)
+//                                     (the gemm tasks of pztrsm.c:131-141).
+// The sweeps are HBM bound: each reads the triangle of the factor once.
+#include "common.cuh"
+
+namespace {
+
+constexpr int kCols = 16;        // right-hand sides per CTA
+constexpr int kThreads = 256;
+
+// out(k) = op(W_k) * B(k, chunk), op = identity (forward) or transpose.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_diag_apply(plasma_desc_t B, int k, const T *W, int nbw, int trans,
+             const plasma_devstat_t *st)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T (*Bs)[kCols + 1] = reinterpret_cast<T (*)[kCols + 1]>(smem_raw);
+    if (plasma_failed(st)) return;
+    const int n = blockIdx.x;
+    const int c0 = blockIdx.y * kCols;
+    const int rows = plasma_tile_mview(B, k);
+    const int cols = min(kCols, plasma_tile_nview(B, n) - c0);
+    if (cols <= 0) return;
+    T *b = (T *)plasma_tile_addr(B, k, n);
+    const int ldb = plasma_tile_mmain(B, k);
+    const T *w = W + (size_t)k * nbw * nbw;
+    for (int e = threadIdx.x; e < rows * cols; e += kThreads) {
+        int r = e % rows, c = e / rows;
+        Bs[r][c] = b[(size_t)(c0 + c) * ldb + r];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < rows; i += kThreads) {
+        T acc[kCols];
+#pragma unroll
+        for (int j = 0; j < kCols; j++) acc[j] = T(0);
+        // W_k is lower: forward uses row i (c <= i), backward column i (c >= i)
+        int cb = trans ? i : 0, ce = trans ? rows : i + 1;
+        for (int c = cb; c < ce; c++) {
+            T wv = trans ? w[(size_t)i * nbw + c] : w[(size_t)c * nbw + i];
+#pragma unroll
+            for (int j = 0; j < kCols; j++) acc[j] += wv * Bs[c][j];
+        }
+        for (int j = 0; j < cols; j++)
+            b[(size_t)(c0 + j) * ldb + i] = acc[j];
+    }
+}
+
+// B(m, chunk) -= op(L) * B(k, chunk) for the tiles m in [mlo, mhi)
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_solve_update(plasma_desc_t A, int uplo, plasma_desc_t B, int k, int mlo,
+               int trans, const plasma_devstat_t *st)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T (*Ys)[kCols + 1] = reinterpret_cast<T (*)[kCols + 1]>(smem_raw);
+    if (plasma_failed(st)) return;
+    const int m = mlo + blockIdx.x;
+    const int n = blockIdx.y;
+    const int c0 = blockIdx.z * kCols;
+    const int cols = min(kCols, plasma_tile_nview(B, n) - c0);
+    if (cols <= 0) return;
+    const int kr = plasma_tile_mview(B, k);
+    const int mr = plasma_tile_mview(B, m);
+    const T *y = (const T *)plasma_tile_addr(B, k, n);
+    const int ldy = plasma_tile_mmain(B, k);
+    T *b = (T *)plasma_tile_addr(B, m, n);
+    const int ldb = plasma_tile_mmain(B, m);
+    for (int e = threadIdx.x; e < kr * cols; e += kThreads) {
+        int r = e % kr, c = e / kr;
+        Ys[r][c] = y[(size_t)(c0 + c) * ldy + r];
+    }
+    __syncthreads();
+    // forward: L(m,k) (logical lower tile); backward: L(k,m)^T
+    TileView<T> L = trans ? tile_view<T>(A, uplo, k, m) : tile_view<T>(A, uplo, m, k);
+    for (int i = threadIdx.x; i < mr; i += kThreads) {
+        T acc[kCols];
+#pragma unroll
+        for (int j = 0; j < kCols; j++) acc[j] = T(0);
+        for (int c = 0; c < kr; c++) {
+            T lv = trans ? L.at(c, i) : L.at(i, c);
+#pragma unroll
+            for (int j = 0; j < kCols; j++) acc[j] += lv * Ys[c][j];
+        }
+        for (int j = 0; j < cols; j++)
+            b[(size_t)(c0 + j) * ldb + i] -= acc[j];
+    }
+}
+
+template <typename T>
+void sweep(cudaStream_t s, plasma_devstat_t *st, int uplo, int trans,
+           const plasma_desc_t &A, const plasma_desc_t &B, const T *W)
+{
+    const int mt = B.mt;
+    const int nbw = A.mb;
+    const int chunks = ceil_div(B.nb, kCols);
+    const size_t smem = (size_t)B.mb * (kCols + 1) * sizeof(T);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_diag_apply<T>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             200 * 1024);
+        cudaFuncSetAttribute(k_solve_update<T>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             200 * 1024);
+        attr_set = true;
+    }
+    for (int step = 0; step < mt; step++) {
+        int k = trans ? mt - 1 - step : step;
+        PLASMA_COUNT_LAUNCH();
+        k_diag_apply<T><<<dim3(B.nt, chunks), kThreads, smem, s>>>(
+            B, k, W, nbw, trans, st);
+        int mlo = trans ? 0 : k + 1;
+        int mhi = trans ? k : mt;
+        if (mhi > mlo) {
+            PLASMA_COUNT_LAUNCH();
+            k_solve_update<T><<<dim3(mhi - mlo, B.nt, chunks), kThreads, smem, s>>>(
+                A, uplo, B, k, mlo, trans, st);
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" void plasma_cuda_trtri_tiles(cudaStream_t s, plasma_devstat_t *st,
+                                        plasma_enum_t uplo, plasma_desc_t A,
+                                        void *W);
+
+// Solves op(L) X = B in place; W holds inv(L_kk) for every k (computed here
+// when `have_w` is 0).
+extern "C" void plasma_cuda_trsm_sweep(cudaStream_t s, plasma_devstat_t *st,
+                                       plasma_enum_t uplo, plasma_enum_t trans,
+                                       plasma_desc_t A, plasma_desc_t B,
+                                       void *W, int have_w)
+{
+    if (B.mt == 0 || B.nt == 0) return;
+    if (!have_w)
+        plasma_cuda_trtri_tiles(s, st, uplo, A, W);
+    int t = trans != PlasmaNoTrans;
+    double n = B.m, nrhs = B.n, es = plasma_element_size(A.precision);
+    int prof = plasma_prof_begin(s);
+    if (A.precision == PlasmaRealDouble)
+        sweep<double>(s, st, uplo, t, A, B, (const double *)W);
+    else
+        sweep<float>(s, st, uplo, t, A, B, (const float *)W);
+    // one triangle of the factor read once, B read and written once
+    plasma_prof_end(prof, s, PLASMA_KCLASS_SOLVE, n * n * nrhs,
+                    es * (n * n / 2.0 + 2.0 * n * nrhs));
+}

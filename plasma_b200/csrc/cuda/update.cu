@@ -1,0 +1,340 @@
+// update.cu -- trailing-matrix update of one Cholesky step:
+//     A(m,n) -= A(m,k) * A(n,k)^T      for k < n <= m < mt,
+// i.e. the SYRK on diagonal tiles and the GEMMs below them that the reference
+// submits as nt(nt-1)/2 + C(nt,3) OpenMP tasks per factorisation
+// (compute/pzpotrf.c:57-77 -> core_blas/core_zsyrk.c, core_zgemm.c:89-136).
+//
+// One persistent launch covers every tile of the step (or of a tile-column
+// range, for look-ahead).  Work items are 128x128 sub-blocks of output
+// tiles; each CTA walks the item list with a grid stride.  The strict upper
+// part of diagonal tiles is never written (dsyrk with uplo = Lower leaves it
+// untouched).
+//
+// FP64 lower storage: 8 warps of DMMA (mma.sync m16n8k8 f64, the FP64
+// tensor-core path of sm_100 -- tcgen05 has no f64 kind), operands staged in
+// shared memory by a 3-stage cp.async pipeline, accumulators in registers.
+// FP32 (and the transposed upper-storage fallback): SIMT FFMA/DFMA 8x8
+// register tiles.
+#include "common.cuh"
+
+namespace {
+
+constexpr int BM = 128;
+constexpr int BN = 128;
+constexpr int THREADS = 256;
+
+// Work item -> output tile (m,n) and sub-block (si,sj).
+struct Item {
+    int m, n, si, sj;
+};
+
+__device__ __forceinline__ bool decode_item(int w, int k, int nlo, int nhi,
+                                            int mt, int sb, Item &it)
+{
+    int per = sb * sb;
+    int p = w / per;
+    int s = w - p * per;
+    it.si = s / sb;
+    it.sj = s - it.si * sb;
+    int n = nlo;
+    while (n < nhi && p >= mt - n) {
+        p -= mt - n;
+        n++;
+    }
+    if (n >= nhi) return false;
+    it.n = n;
+    it.m = n + p;
+    (void)k;
+    return true;
+}
+
+__host__ __device__ __forceinline__ long long count_items(int nlo, int nhi,
+                                                          int mt, int sb)
+{
+    long long pairs = 0;
+    for (int n = nlo; n < nhi; n++) pairs += mt - n;
+    return pairs * sb * sb;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 DMMA kernel (lower storage, tiles column-major)
+// ---------------------------------------------------------------------------
+constexpr int DBK = 16;
+constexpr int DSTAGES = 3;
+constexpr int DPAD = 4;                 // row stride 132 doubles: conflict-free
+constexpr int DLDS_A = BM + DPAD;
+constexpr int DLDS_B = BN + DPAD;
+constexpr int DSMEM = DSTAGES * DBK * (DLDS_A + DLDS_B) * (int)sizeof(double);
+
+struct DmmaOperands {
+    const double *a; int lda; int arows;   // A(m,k) logical rows
+    const double *b; int ldb; int brows;   // A(n,k)
+    int i0, j0, K;
+};
+
+__device__ __forceinline__ void dmma_load_stage(double *As, double *Bs,
+                                                const DmmaOperands &op,
+                                                int kc, int tid)
+{
+    // A chunk: BM rows x DBK cols; element e -> row e%BM, col e/BM
+#pragma unroll
+    for (int q = 0; q < (BM * DBK) / THREADS; q++) {
+        int e = tid + q * THREADS;
+        int r = e % BM, c = e / BM;
+        int gi = op.i0 + r, gk = kc + c;
+        bool v = gi < op.arows && gk < op.K;
+        const double *src = v ? op.a + (size_t)gk * op.lda + gi : op.a;
+        cp_async_8(As + c * DLDS_A + r, src, v);
+    }
+#pragma unroll
+    for (int q = 0; q < (BN * DBK) / THREADS; q++) {
+        int e = tid + q * THREADS;
+        int r = e % BN, c = e / BN;
+        int gj = op.j0 + r, gk = kc + c;
+        bool v = gj < op.brows && gk < op.K;
+        const double *src = v ? op.b + (size_t)gk * op.ldb + gj : op.b;
+        cp_async_8(Bs + c * DLDS_B + r, src, v);
+    }
+}
+
+__global__ void __launch_bounds__(THREADS, 1)
+k_update_dmma(plasma_desc_t A, int k, int nlo, int nhi, int nitems,
+              const plasma_devstat_t *st)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    if (plasma_failed(st)) return;
+    double *As = reinterpret_cast<double *>(smem_raw);
+    double *Bs = As + DSTAGES * DBK * DLDS_A;
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm = warp >> 2;          // 0..1 -> 64 rows each
+    const int wn = warp & 3;           // 0..3 -> 32 cols each
+    const int mt = A.mt;
+    const int sb = (A.mb + BM - 1) / BM;
+
+    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+        Item it;
+        if (!decode_item(w, k, nlo, nhi, mt, sb, it)) break;
+        if (it.m == it.n && it.sj > it.si) continue;     // strict upper block
+        DmmaOperands op;
+        op.a = (const double *)plasma_tile_addr(A, it.m, k);
+        op.lda = plasma_tile_mmain(A, it.m);
+        op.arows = plasma_tile_mview(A, it.m);
+        op.b = (const double *)plasma_tile_addr(A, it.n, k);
+        op.ldb = plasma_tile_mmain(A, it.n);
+        op.brows = plasma_tile_mview(A, it.n);
+        op.i0 = it.si * BM;
+        op.j0 = it.sj * BN;
+        op.K = plasma_tile_nview(A, k);
+        if (op.i0 >= op.arows || op.j0 >= op.brows) continue;
+
+        double acc[4][4][4];
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int b = 0; b < 4; b++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) acc[a][b][c] = 0.0;
+
+        const int nk = (op.K + DBK - 1) / DBK;
+        __syncthreads();   // previous item's readers are done with smem
+#pragma unroll
+        for (int s = 0; s < DSTAGES - 1; s++) {
+            if (s < nk)
+                dmma_load_stage(As + s * DBK * DLDS_A, Bs + s * DBK * DLDS_B,
+                                op, s * DBK, tid);
+            cp_async_commit();
+        }
+        for (int kt = 0; kt < nk; kt++) {
+            cp_async_wait<DSTAGES - 2>();
+            __syncthreads();
+            // prefetch stage kt + STAGES-1 (its slot was consumed at kt-1)
+            int pf = kt + DSTAGES - 1;
+            if (pf < nk) {
+                int sl = pf % DSTAGES;
+                dmma_load_stage(As + sl * DBK * DLDS_A, Bs + sl * DBK * DLDS_B,
+                                op, pf * DBK, tid);
+            }
+            cp_async_commit();
+
+            const double *as = As + (kt % DSTAGES) * DBK * DLDS_A + wm * 64;
+            const double *bs = Bs + (kt % DSTAGES) * DBK * DLDS_B + wn * 32;
+#pragma unroll
+            for (int k8 = 0; k8 < DBK; k8 += 8) {
+                double bf[4][2];
+#pragma unroll
+                for (int ni = 0; ni < 4; ni++) {
+                    bf[ni][0] = bs[(k8 + t) * DLDS_B + ni * 8 + g];
+                    bf[ni][1] = bs[(k8 + t + 4) * DLDS_B + ni * 8 + g];
+                }
+#pragma unroll
+                for (int mi = 0; mi < 4; mi++) {
+                    double af[4];
+                    af[0] = as[(k8 + t) * DLDS_A + mi * 16 + g];
+                    af[1] = as[(k8 + t) * DLDS_A + mi * 16 + g + 8];
+                    af[2] = as[(k8 + t + 4) * DLDS_A + mi * 16 + g];
+                    af[3] = as[(k8 + t + 4) * DLDS_A + mi * 16 + g + 8];
+#pragma unroll
+                    for (int ni = 0; ni < 4; ni++)
+                        dmma_16x8x8(acc[mi][ni], af, bf[ni]);
+                }
+            }
+        }
+        cp_async_wait<0>();
+
+        // epilogue: C -= acc, masking rows/cols outside the tile and the
+        // strict upper triangle of a diagonal tile
+        double *C = (double *)plasma_tile_addr(A, it.m, it.n);
+        const int ldc = plasma_tile_mmain(A, it.m);
+        const bool diag = it.m == it.n;
+#pragma unroll
+        for (int mi = 0; mi < 4; mi++) {
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                int i = op.i0 + wm * 64 + mi * 16 + g + h * 8;
+                if (i >= op.arows) continue;
+#pragma unroll
+                for (int ni = 0; ni < 4; ni++) {
+#pragma unroll
+                    for (int e = 0; e < 2; e++) {
+                        int j = op.j0 + wn * 32 + ni * 8 + 2 * t + e;
+                        if (j < op.brows && (!diag || i >= j))
+                            C[(size_t)j * ldc + i] -= acc[mi][ni][h * 2 + e];
+                    }
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// SIMT kernel (FP32, or FP64 with transposed upper storage)
+// ---------------------------------------------------------------------------
+constexpr int SBK = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(THREADS)
+k_update_simt(plasma_desc_t A, int uplo, int k, int nlo, int nhi, int nitems,
+              const plasma_devstat_t *st)
+{
+    __shared__ T As[SBK][BM + 4];
+    __shared__ T Bs[SBK][BN + 4];
+    if (plasma_failed(st)) return;
+    const int tid = threadIdx.x;
+    const int tx = tid % 16, ty = tid / 16;
+    const int mt = A.mt;
+    const int sb = (A.mb + BM - 1) / BM;
+
+    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+        Item it;
+        if (!decode_item(w, k, nlo, nhi, mt, sb, it)) break;
+        if (it.m == it.n && it.sj > it.si) continue;
+        TileView<T> a = tile_view<T>(A, uplo, it.m, k);
+        TileView<T> b = tile_view<T>(A, uplo, it.n, k);
+        TileView<T> c = tile_view<T>(A, uplo, it.m, it.n);
+        const int i0 = it.si * BM, j0 = it.sj * BN;
+        if (i0 >= a.rows || j0 >= b.rows) continue;
+        const int K = a.cols;
+
+        T acc[8][8];
+#pragma unroll
+        for (int x = 0; x < 8; x++)
+#pragma unroll
+            for (int y = 0; y < 8; y++) acc[x][y] = T(0);
+
+        for (int kc = 0; kc < K; kc += SBK) {
+            __syncthreads();
+            for (int e = tid; e < BM * SBK; e += THREADS) {
+                int r, cc;
+                if (a.trans) { cc = e % SBK; r = e / SBK; }
+                else         { r = e % BM;   cc = e / BM; }
+                int gi = i0 + r, gk = kc + cc;
+                As[cc][r] = (gi < a.rows && gk < K) ? a.at(gi, gk) : T(0);
+                int gj = j0 + r;
+                Bs[cc][r] = (gj < b.rows && gk < K) ? b.at(gj, gk) : T(0);
+            }
+            __syncthreads();
+#pragma unroll
+            for (int kk = 0; kk < SBK; kk++) {
+                T x[8], y[8];
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    x[q] = As[kk][ty * 4 + q];
+                    x[q + 4] = As[kk][64 + ty * 4 + q];
+                    y[q] = Bs[kk][tx * 4 + q];
+                    y[q + 4] = Bs[kk][64 + tx * 4 + q];
+                }
+#pragma unroll
+                for (int p = 0; p < 8; p++)
+#pragma unroll
+                    for (int q = 0; q < 8; q++) acc[p][q] += x[p] * y[q];
+            }
+        }
+        const bool diag = it.m == it.n;
+#pragma unroll
+        for (int p = 0; p < 8; p++) {
+            int i = i0 + (p < 4 ? ty * 4 + p : 64 + ty * 4 + p - 4);
+            if (i >= a.rows) continue;
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                int j = j0 + (q < 4 ? tx * 4 + q : 64 + tx * 4 + q - 4);
+                if (j < b.rows && (!diag || i >= j))
+                    c.at(i, j) -= acc[p][q];
+            }
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" void plasma_cuda_update(cudaStream_t s, plasma_devstat_t *st,
+                                   plasma_enum_t uplo, plasma_desc_t A, int k,
+                                   int nlo, int nhi, int num_sms)
+{
+    if (nhi <= nlo) return;
+    int sb = (A.mb + BM - 1) / BM;
+    long long nitems = count_items(nlo, nhi, A.mt, sb);
+    if (nitems <= 0) return;
+    PLASMA_COUNT_LAUNCH();
+    // algorithmic work of this launch: SYRK on diagonal tiles, GEMM below
+    double flops = 0.0, bytes = 0.0;
+    {
+        const double K = plasma_tile_nview(A, k);
+        const double es = (double)plasma_element_size(A.precision);
+        for (int n = nlo; n < nhi; n++) {
+            double cn = plasma_tile_mview(A, n);
+            for (int m = n; m < A.mt; m++) {
+                double rm = plasma_tile_mview(A, m);
+                flops += (m == n) ? cn * (cn + 1) * K : 2.0 * rm * cn * K;
+                bytes += es * (m == n ? cn * (cn + 1) : 2.0 * rm * cn);
+            }
+        }
+    }
+    int prof = plasma_prof_begin(s);
+    if (A.precision == PlasmaRealDouble && uplo == PlasmaLower) {
+        static bool attr_set = false;
+        if (!attr_set) {
+            cudaFuncSetAttribute(k_update_dmma,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 DSMEM);
+            attr_set = true;
+        }
+        // one CTA per work item: SMs free up often, so the high-priority
+        // critical-path kernels of the next step are scheduled in between
+        long long grid = nitems;
+        (void)num_sms;
+        k_update_dmma<<<(unsigned)grid, THREADS, DSMEM, s>>>(
+            A, k, nlo, nhi, (int)nitems, st);
+    } else {
+        long long grid = nitems < 2LL * num_sms ? nitems : 2LL * num_sms;
+        if (A.precision == PlasmaRealDouble)
+            k_update_simt<double><<<(unsigned)grid, THREADS, 0, s>>>(
+                A, uplo, k, nlo, nhi, (int)nitems, st);
+        else
+            k_update_simt<float><<<(unsigned)grid, THREADS, 0, s>>>(
+                A, uplo, k, nlo, nhi, (int)nitems, st);
+    }
+    plasma_prof_end(prof, s, PLASMA_KCLASS_UPDATE, flops, bytes);
+}

@@ -1,0 +1,189 @@
+/*
+ * internal.h -- declarations shared by the C host layer (control/, compute/)
+ * and the CUDA launch layer (cuda/).  Nothing here is part of the public ABI.
+ *
+ * Execution model.  The reference opens "omp parallel / omp master" and turns
+ * every tile operation into an OpenMP task whose depend() clauses form the DAG
+ * (compute/pzpotrf.c:37-80, core_blas/core_zgemm.c:125-127).  Here the host
+ * walks the same loops but launches one CUDA kernel per *tile step*
+ * (all TRSMs of a panel, all SYRK/GEMM updates of a step) and orders them with
+ * CUDA streams and events.  The cooperative cancellation of the reference
+ * (every task tests sequence->status, core_blas/core_zpotrf.c:74) becomes a
+ * device status word that every kernel reads first and that the failing kernel
+ * writes.
+ */
+#ifndef PLASMA_B200_INTERNAL_H
+#define PLASMA_B200_INTERNAL_H
+
+#include "plasma.h"
+#include "plasma_b200.h"
+
+#include <cuda_runtime_api.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Device status word shared by all kernels of a context. */
+typedef struct {
+    int status;   /* 0 = running fine; > 0 = LAPACK-style info; < 0 = error */
+    int call;     /* id of the plasma_omp_* call whose kernel failed       */
+    int spare[2];
+} plasma_devstat_t;
+
+#define PLASMA_MAX_PENDING_CALLS 4096
+#define PLASMA_NUM_STREAMS 4
+#define PLASMA_SCRATCH_SLOTS 4
+
+/* scratch slots */
+enum {
+    PLASMA_SLOT_STAGING = 0,   /* column-major copies of host operands       */
+    PLASMA_SLOT_WORK    = 1,   /* inverses of diagonal tiles, panels          */
+    PLASMA_SLOT_SMALL   = 2,   /* norms and other vectors                     */
+    PLASMA_SLOT_MIXED   = 3    /* low-precision operand copies (dsposv)       */
+};
+
+typedef struct {
+    int tuning;
+    int nb;
+    int ib;
+    plasma_enum_t inplace_outplace;
+    int max_threads;
+    int max_panel_threads;
+    plasma_enum_t householder_mode;
+
+    /* GPU-build state */
+    int device;
+    int mixed_mode;      /* PlasmaFactor* */
+    int refinement;      /* PlasmaRefine* */
+    int lookahead;       /* >= 0 */
+    int num_sms;
+    cudaStream_t stream;                     /* the sequence stream         */
+    cudaStream_t own_stream;                 /* created by plasma_init()    */
+    cudaStream_t aux[PLASMA_NUM_STREAMS];    /* look-ahead / update streams */
+    plasma_devstat_t *dstat;                 /* device status word          */
+    plasma_devstat_t *hstat;                 /* pinned host mirror          */
+
+    /* ids of plasma_omp_* calls since the last plasma_sequence_wait() */
+    int next_call;
+    plasma_request_t *pending[PLASMA_MAX_PENDING_CALLS];
+    plasma_sequence_t *pending_seq[PLASMA_MAX_PENDING_CALLS];
+
+    /* growable device scratch slots (never shrink until finalize) */
+    void  *scratch[PLASMA_SCRATCH_SLOTS];
+    size_t scratch_bytes[PLASMA_SCRATCH_SLOTS];
+    void  *pinned;
+    size_t pinned_bytes;
+    cudaEvent_t ev[8];                        /* DAG edges (reused)        */
+} plasma_context_t;
+
+plasma_context_t *plasma_context_self(void);
+
+/* Opt-in profiling (control/profile.c): brackets one launch on stream s. */
+int plasma_prof_begin(cudaStream_t s);
+void plasma_prof_end(int slot, cudaStream_t s, int kclass, double flops,
+                     double bytes);
+
+/* Registers a plasma_omp_* call; returns the id its kernels report. */
+int plasma_call_begin(plasma_context_t *plasma, plasma_sequence_t *sequence,
+                      plasma_request_t *request);
+
+/* Device scratch of at least `bytes` in one of the slots above.  The buffer
+ * stays valid until the same slot is requested with a larger size; all users
+ * are ordered on the context streams, and growth waits for them. */
+void *plasma_scratch(plasma_context_t *plasma, int slot, size_t bytes);
+void *plasma_pinned(plasma_context_t *plasma, size_t bytes);
+
+/* Queries whether p is device memory of the context's device. */
+int plasma_is_device_pointer(const void *p);
+
+static inline int imin(int a, int b) { return a < b ? a : b; }
+static inline int imax(int a, int b) { return a > b ? a : b; }
+
+/* ----------------------------------------------------------------------------
+ * Tile-step kernels (cuda/ directory).  Every launcher takes the stream, the
+ * device status word and -- for kernels that can fail -- the call id.
+ * prec is PlasmaRealDouble or PlasmaRealFloat.
+ * ------------------------------------------------------------------------- */
+
+/* Column-major (ld) <-> tile layout of the view of A.  For uplo = Lower/Upper
+ * only the tiles of that triangle are copied (reference compute/pztr2desc.c). */
+void plasma_cuda_lapack_to_tile(cudaStream_t s, plasma_devstat_t *st,
+                                plasma_desc_t A, plasma_enum_t uplo,
+                                const void *pA, int lda);
+void plasma_cuda_tile_to_lapack(cudaStream_t s, plasma_devstat_t *st,
+                                plasma_desc_t A, plasma_enum_t uplo,
+                                void *pA, int lda);
+
+/* All diagonal-tile inverses W_k = inv(L_kk) (lower logical view) into W
+ * (A.mt tiles of A.mb x A.mb, column-major). */
+void plasma_cuda_trtri_tiles(cudaStream_t s, plasma_devstat_t *st,
+                             plasma_enum_t uplo, plasma_desc_t A, void *W);
+
+/* op(L) X = B in place (trans = PlasmaNoTrans or PlasmaTrans); W as above,
+ * computed first when have_w == 0. */
+void plasma_cuda_trsm_sweep(cudaStream_t s, plasma_devstat_t *st,
+                            plasma_enum_t uplo, plasma_enum_t trans,
+                            plasma_desc_t A, plasma_desc_t B,
+                            void *W, int have_w);
+
+/* Diagonal-tile Cholesky of tile (k,k) (uplo Lower or Upper), writing
+ * info = iinfo + j on a non-positive pivot in column j (1-based).  If winv is
+ * not NULL it also receives W = inv(L_kk) (lower, ld = nb) used by the
+ * panel solve. */
+void plasma_cuda_potrf_tile(cudaStream_t s, plasma_devstat_t *st, int call,
+                            plasma_enum_t uplo, plasma_desc_t A, int k,
+                            int iinfo, void *winv);
+
+/* Panel solve of step k: A(m,k) <- A(m,k) * L_kk^{-T} for m = k+1..mt-1
+ * (upper: A(k,m) <- U_kk^{-T} A(k,m)), given W = inv(L_kk). mlo..mhi-1 is the
+ * tile range processed. */
+void plasma_cuda_trsm_panel(cudaStream_t s, plasma_devstat_t *st,
+                            plasma_enum_t uplo, plasma_desc_t A, int k,
+                            int mlo, int mhi, const void *winv);
+
+/* Trailing update of step k restricted to tile columns n in [nlo, nhi) and
+ * rows m >= n:  A(m,n) -= A(m,k) A(n,k)^T (SYRK on the diagonal, GEMM below).
+ */
+void plasma_cuda_update(cudaStream_t s, plasma_devstat_t *st,
+                        plasma_enum_t uplo, plasma_desc_t A, int k,
+                        int nlo, int nhi, int num_sms);
+
+/* dsposv helpers. */
+/* Infinity norm of symmetric A (uplo triangle) into *dnorm (device). */
+void plasma_cuda_lansy_inf(cudaStream_t s, plasma_devstat_t *st,
+                           plasma_enum_t uplo, plasma_desc_t A,
+                           double *dnorm, double *work);
+/* As <- (float)A tile by tile; sets status 1 on overflow (dlag2s). */
+void plasma_cuda_lag2s(cudaStream_t s, plasma_devstat_t *st, int call,
+                       plasma_desc_t A, plasma_desc_t As, plasma_enum_t uplo);
+void plasma_cuda_slag2d(cudaStream_t s, plasma_devstat_t *st,
+                        plasma_desc_t As, plasma_desc_t A);
+/* R <- B - A X with symmetric A given by its uplo triangle; then columnwise
+ * max-abs of X and R into xnorm / rnorm (device). */
+void plasma_cuda_residual(cudaStream_t s, plasma_devstat_t *st,
+                          plasma_enum_t uplo, plasma_desc_t A,
+                          plasma_desc_t B, plasma_desc_t X, plasma_desc_t R,
+                          double *xnorm, double *rnorm);
+/* X <- X + R (general descriptors of equal shape). */
+void plasma_cuda_geadd(cudaStream_t s, plasma_devstat_t *st,
+                       plasma_desc_t R, plasma_desc_t X);
+/* B <- A (general descriptors of equal shape, same precision). */
+void plasma_cuda_lacpy(cudaStream_t s, plasma_devstat_t *st,
+                       plasma_desc_t A, plasma_desc_t B);
+
+/* Host-side DAG walkers (compute/). */
+void plasma_pXpotrf(plasma_context_t *plasma, plasma_enum_t uplo,
+                    plasma_desc_t A, plasma_sequence_t *sequence,
+                    plasma_request_t *request, int call);
+void plasma_pXpotrs(plasma_context_t *plasma, plasma_enum_t uplo,
+                    plasma_desc_t A, plasma_desc_t B,
+                    plasma_sequence_t *sequence, plasma_request_t *request);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PLASMA_B200_INTERNAL_H */

@@ -1,0 +1,78 @@
+"""Writes tests/golden/lapack_fixtures.npz: LAPACK (scipy) answers for seeded
+SPD inputs.  The reference's own tester defines correctness against LAPACK
+(test/test_zpotrf.c:124-141 compares with LAPACKE_dpotrf; the posv/dsposv
+testers check the scaled residual), so these are the known answers the
+oracle and the GPU library are pinned to.
+
+Run:  python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+import scipy
+import scipy.linalg.lapack as lapack
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+import gen  # noqa: E402
+
+OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lapack_fixtures.npz")
+
+
+def main():
+    d = {"scipy_version": np.array(scipy.__version__)}
+    # small cases: full outputs
+    for n in (1, 2, 7, 33, 64, 100):
+        a, b = gen.diag_dominant(n, 3, seed=1000 + n)
+        lo, info_l = lapack.dpotrf(a, lower=1, clean=1)
+        up, info_u = lapack.dpotrf(a, lower=0, clean=1)
+        _, x, info_x = lapack.dposv(a, b, lower=1)
+        assert info_l == 0 and info_u == 0 and info_x == 0
+        d[f"small{n}_A"] = a
+        d[f"small{n}_B"] = b
+        d[f"small{n}_L"] = np.tril(lo)
+        d[f"small{n}_U"] = np.triu(up)
+        d[f"small{n}_X"] = x
+    # ragged sizes (n not a multiple of the tile size): checksums only
+    for n in (300, 1000):
+        a, b = gen.diag_dominant(n, 5, seed=2000 + n)
+        lo, info = lapack.dpotrf(a, lower=1, clean=1)
+        _, x, _ = lapack.dposv(a, b, lower=1)
+        v = gen.probe_vector(n)
+        d[f"ragged{n}_diagL"] = np.diag(lo).copy()
+        d[f"ragged{n}_Lv"] = np.tril(lo) @ v
+        d[f"ragged{n}_X"] = x
+    # the CPU parity configuration: n = 2048, nrhs = 1, seed 42
+    n = 2048
+    a, b = gen.diag_dominant(n, 1, seed=42)
+    lo, info = lapack.dpotrf(a, lower=1, clean=1)
+    _, x, _ = lapack.dposv(a, b, lower=1)
+    v = gen.probe_vector(n)
+    d["cfg1_diagL"] = np.diag(lo).copy()
+    d["cfg1_Lv"] = np.tril(lo) @ v
+    d["cfg1_Ltv"] = np.tril(lo).T @ v
+    d["cfg1_X"] = x
+    d["cfg1_normL"] = np.array(np.linalg.norm(np.tril(lo)))
+    # non positive definite: LAPACK's info for a zeroed row/column
+    for n, col in ((100, 37), (300, 0), (300, 299), (513, 256)):
+        a, _ = gen.diag_dominant(n, 1, seed=3000 + n)
+        a = gen.zerocol(a, col)
+        _, info_l = lapack.dpotrf(a, lower=1)
+        _, info_u = lapack.dpotrf(a, lower=0)
+        d[f"nonspd{n}_{col}_info_lower"] = np.array(info_l)
+        d[f"nonspd{n}_{col}_info_upper"] = np.array(info_u)
+    # prescribed spectrum (mixed-precision cases), n = 256
+    for kappa in (1e2, 1e5, 1e8):
+        a = gen.spectrum(256, kappa, seed=11)
+        rng = np.random.default_rng(12)
+        xt = rng.standard_normal((256, 1))
+        bb = a @ xt
+        _, x, info = lapack.dposv(a, bb, lower=1)
+        d[f"spec{int(np.log10(kappa))}_X"] = x
+        d[f"spec{int(np.log10(kappa))}_xtrue"] = xt
+    np.savez_compressed(OUT, **d)
+    print("wrote", OUT, os.path.getsize(OUT), "bytes")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,335 @@
+"""GPU parity: the library (through its C ABI) against the LAPACK fixtures and
+the CPU oracle, with the reference tester's acceptance tests
+(test/test_zpotrf.c:124-152, test_zpotrs.c:140-169, test_zposv.c:137-167,
+test_zcposv.c:139-193; tol = 50).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import gen
+import oracle
+import plasma_b200 as pb
+from conftest import EPS, SEPS, TOL, factor_error, factor_residual, solve_residual
+
+pytestmark = pytest.mark.gpu
+LO, UP = pb.PlasmaLower, pb.PlasmaUpper
+
+
+@pytest.fixture(scope="module")
+def L():
+    import torch
+    assert torch.cuda.is_available()
+    lib = pb.lib()
+    rc = lib.plasma_init()
+    assert rc == 0, rc
+    yield lib
+    lib.plasma_finalize()
+
+
+def set_nb(L, nb):
+    assert L.plasma_set(pb.PlasmaTuning, pb.PlasmaDisabled) == 0
+    assert L.plasma_set(pb.PlasmaNb, nb) == 0
+
+
+def dpotrf(L, uplo, a):
+    f = np.asfortranarray(a.copy())
+    info = L.plasma_dpotrf(uplo, f.shape[0], f.ctypes.data, f.shape[0])
+    return info, f
+
+
+# ------------------------------------------------------------------ potrf
+@pytest.mark.parametrize("n", [1, 2, 7, 33, 64, 100])
+@pytest.mark.parametrize("nb", [16, 32, 64, 128])
+def test_dpotrf_small_vs_lapack(L, golden, n, nb):
+    set_nb(L, nb)
+    a = golden[f"small{n}_A"]
+    for uplo, key in ((LO, "L"), (UP, "U")):
+        info, f = dpotrf(L, uplo, a)
+        assert info == 0
+        got = np.tril(f) if uplo == LO else np.triu(f)
+        assert factor_error(got, golden[f"small{n}_{key}"], a) < TOL * EPS
+        # strict other triangle untouched (LAPACK semantics)
+        other = np.triu(f, 1) if uplo == LO else np.tril(f, -1)
+        ref = np.triu(a, 1) if uplo == LO else np.tril(a, -1)
+        np.testing.assert_array_equal(other, ref)
+
+
+@pytest.mark.parametrize("n,nb", [(300, 128), (1000, 128), (1000, 256), (300, 64)])
+def test_dpotrf_ragged_vs_lapack(L, golden, n, nb):
+    set_nb(L, nb)
+    a, _ = gen.diag_dominant(n, 5, seed=2000 + n)
+    info, f = dpotrf(L, LO, a)
+    assert info == 0
+    l = np.tril(f)
+    v = gen.probe_vector(n)
+    np.testing.assert_allclose(np.diag(l), golden[f"ragged{n}_diagL"], rtol=1e-13)
+    np.testing.assert_allclose(l @ v, golden[f"ragged{n}_Lv"], rtol=1e-12)
+    assert factor_residual(l, a) < TOL
+    # upper storage on the same matrix
+    info, f = dpotrf(L, UP, a)
+    assert info == 0
+    u = np.triu(f)
+    np.testing.assert_allclose(np.diag(u), golden[f"ragged{n}_diagL"], rtol=1e-13)
+    assert factor_residual(u, a, lower=False) < TOL
+
+
+def test_dpotrf_cfg1_vs_lapack_and_oracle(L, golden):
+    """n = 2048, nb = 256, seed 42 (the CPU parity configuration)."""
+    set_nb(L, 256)
+    a, b = gen.diag_dominant(2048, 1, seed=42)
+    info, f = dpotrf(L, LO, a)
+    assert info == 0
+    l = np.tril(f)
+    v = gen.probe_vector(2048)
+    np.testing.assert_allclose(np.diag(l), golden["cfg1_diagL"], rtol=1e-14)
+    np.testing.assert_allclose(l @ v, golden["cfg1_Lv"], rtol=1e-12)
+    np.testing.assert_allclose(l.T @ v, golden["cfg1_Ltv"], rtol=1e-12)
+    fo = np.asfortranarray(a.copy())
+    assert oracle.potrf(oracle.LOWER, fo, 256) == 0
+    assert factor_error(l, np.tril(fo), a) < TOL * EPS
+    assert factor_residual(l, a) < TOL
+
+
+@pytest.mark.parametrize("n,col", [(100, 37), (300, 0), (300, 299), (513, 256)])
+def test_dpotrf_nonspd_info(L, golden, n, col):
+    a, _ = gen.diag_dominant(n, 1, seed=3000 + n)
+    a = gen.zerocol(a, col)
+    for nb in (64, 128):
+        set_nb(L, nb)
+        for uplo, key in ((LO, "lower"), (UP, "upper")):
+            info, f = dpotrf(L, uplo, a)
+            assert info == int(golden[f"nonspd{n}_{col}_info_{key}"])
+            np.testing.assert_array_equal(f, a)   # failed call leaves pA alone
+    # the context recovers: a good matrix factors next
+    good, _ = gen.diag_dominant(64, 1, seed=1)
+    assert dpotrf(L, LO, good)[0] == 0
+
+
+def test_dpotrf_nan_reports_info(L):
+    set_nb(L, 32)
+    a, _ = gen.diag_dominant(70, 1, seed=4)
+    a[40, 40] = np.nan
+    info, _ = dpotrf(L, LO, a)
+    assert info == 41
+
+
+def test_dpotrf_lda_padding(L):
+    set_nb(L, 32)
+    n, lda = 75, 90
+    a, _ = gen.diag_dominant(n, 1, seed=8)
+    big = np.full((lda, n), 7.0, order="F")
+    big[:n, :] = a
+    info = L.plasma_dpotrf(LO, n, big.ctypes.data, lda)
+    assert info == 0
+    assert np.all(big[n:, :] == 7.0)
+    assert factor_residual(np.tril(big[:n, :]), a) < TOL
+
+
+# ------------------------------------------------------------------ solves
+@pytest.mark.parametrize("n", [7, 64, 100])
+@pytest.mark.parametrize("nb", [16, 32])
+def test_dposv_dpotrs_small(L, golden, n, nb):
+    set_nb(L, nb)
+    a, b = golden[f"small{n}_A"], golden[f"small{n}_B"]
+    for uplo in (LO, UP):
+        f = np.asfortranarray(a.copy())
+        x = np.asfortranarray(b.copy())
+        assert L.plasma_dposv(uplo, n, b.shape[1], f.ctypes.data, n, x.ctypes.data, n) == 0
+        assert solve_residual(a, x, b) < TOL * EPS
+        np.testing.assert_allclose(x, golden[f"small{n}_X"], rtol=1e-12, atol=1e-15)
+        x2 = np.asfortranarray(b.copy())
+        assert L.plasma_dpotrs(uplo, n, b.shape[1], f.ctypes.data, n, x2.ctypes.data, n) == 0
+        np.testing.assert_allclose(x2, x, rtol=1e-13, atol=1e-16)
+
+
+@pytest.mark.parametrize("n,nb,nrhs", [(300, 128, 5), (1000, 128, 5), (1000, 256, 17)])
+def test_dposv_ragged(L, golden, n, nb, nrhs):
+    set_nb(L, nb)
+    a, b = gen.diag_dominant(n, nrhs, seed=2000 + n)
+    x = np.asfortranarray(b.copy())
+    f = np.asfortranarray(a.copy())
+    assert L.plasma_dposv(LO, n, nrhs, f.ctypes.data, n, x.ctypes.data, n) == 0
+    assert solve_residual(a, x, b) < TOL * EPS
+    if nrhs == 5:
+        np.testing.assert_allclose(x, golden[f"ragged{n}_X"], rtol=1e-12, atol=1e-15)
+    xo = np.asfortranarray(b.copy())
+    assert oracle.posv(oracle.LOWER, np.asfortranarray(a.copy()), xo, nb) == 0
+    np.testing.assert_allclose(x, xo, rtol=1e-12, atol=1e-15)
+
+
+def test_dposv_cfg1(L, golden):
+    set_nb(L, 256)
+    a, b = gen.diag_dominant(2048, 1, seed=42)
+    f = np.asfortranarray(a.copy())
+    x = np.asfortranarray(b.copy())
+    assert L.plasma_dposv(LO, 2048, 1, f.ctypes.data, 2048, x.ctypes.data, 2048) == 0
+    assert solve_residual(a, x, b) < TOL * EPS
+    np.testing.assert_allclose(x, golden["cfg1_X"], rtol=1e-12)
+
+
+def test_device_pointer_path(L):
+    """LAPACK-layout routines on device memory (no host copies)."""
+    import torch
+    set_nb(L, 128)
+    n, nrhs = 777, 4
+    a, b = gen.diag_dominant(n, nrhs, seed=21)
+    # column-major device buffers: row-major storage of the transpose
+    A = torch.from_numpy(np.ascontiguousarray(a.T)).cuda()
+    B = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
+    assert L.plasma_dposv(LO, n, nrhs, A.data_ptr(), n, B.data_ptr(), n) == 0
+    torch.cuda.synchronize()
+    x = B.cpu().numpy().T
+    assert solve_residual(a, x, b) < TOL * EPS
+    l = np.tril(A.cpu().numpy().T)
+    assert factor_residual(l, a) < TOL
+
+
+# ------------------------------------------------------------------ FP32
+@pytest.mark.parametrize("n,nb", [(100, 32), (1000, 256), (513, 128)])
+def test_spotrf_sposv(L, n, nb):
+    set_nb(L, nb)
+    a, b = gen.diag_dominant(n, 3, seed=n)
+    a32, b32 = np.asfortranarray(a.astype(np.float32)), np.asfortranarray(b.astype(np.float32))
+    for uplo in (LO, UP):
+        f = a32.copy(order="F")
+        assert L.plasma_spotrf(uplo, n, f.ctypes.data, n) == 0
+        fo = a32.copy(order="F")
+        assert oracle.potrf(uplo, fo, nb) == 0
+        t = np.tril if uplo == LO else np.triu
+        err = np.linalg.norm(t(f).astype(np.float64) - t(fo)) / np.linalg.norm(a)
+        assert err < TOL * SEPS
+        x = b32.copy(order="F")
+        assert L.plasma_sposv(uplo, n, 3, a32.copy(order="F").ctypes.data, n,
+                              x.ctypes.data, n) == 0
+        assert solve_residual(a, x.astype(np.float64), b) < TOL * SEPS
+
+
+# ------------------------------------------------------------------ dsposv
+@pytest.mark.parametrize("n,nb,nrhs", [(64, 32, 1), (300, 128, 2), (2048, 256, 1)])
+def test_dsposv_diag_dominant(L, n, nb, nrhs):
+    set_nb(L, nb)
+    a, b = gen.diag_dominant(n, nrhs, seed=5000 + n)
+    x = np.zeros((n, nrhs), order="F")
+    it = ctypes.c_int(-99)
+    a0, b0 = a.copy(), b.copy()
+    info = L.plasma_dsposv(LO, n, nrhs, a.ctypes.data, n, b.ctypes.data, n,
+                           x.ctypes.data, n, ctypes.byref(it))
+    assert info == 0
+    assert 0 <= it.value <= 30
+    assert solve_residual(a, x, b) < TOL * EPS
+    np.testing.assert_array_equal(a, a0)     # A and B are not modified
+    np.testing.assert_array_equal(b, b0)
+    xo = np.zeros_like(x, order="F")
+    info_o, it_o = oracle.dsposv(oracle.LOWER, a, b, xo, nb)
+    assert info_o == 0
+    np.testing.assert_allclose(x, xo, rtol=1e-12, atol=1e-15)
+
+
+@pytest.mark.parametrize("kappa", [1e2, 1e5])
+def test_dsposv_spectrum(L, golden, kappa):
+    set_nb(L, 64)
+    n = 256
+    a = gen.spectrum(n, kappa, seed=11)
+    xt = golden[f"spec{int(np.log10(kappa))}_xtrue"]
+    b = np.asfortranarray(a @ xt)
+    x = np.zeros_like(b, order="F")
+    it = ctypes.c_int()
+    assert L.plasma_dsposv(UP, n, 1, a.ctypes.data, n, b.ctypes.data, n,
+                           x.ctypes.data, n, ctypes.byref(it)) == 0
+    assert solve_residual(a, x, b) < TOL * EPS
+    xl = golden[f"spec{int(np.log10(kappa))}_X"]
+    assert np.abs(x - xl).max() / np.abs(xl).max() < kappa * 1e-13
+
+
+def test_dsposv_fallback(L):
+    set_nb(L, 32)
+    n = 128
+    a = gen.spectrum(n, 1e12, seed=11)
+    b = np.asfortranarray(np.random.default_rng(1).standard_normal((n, 1)))
+    x = np.zeros_like(b, order="F")
+    it = ctypes.c_int()
+    assert L.plasma_dsposv(LO, n, 1, a.ctypes.data, n, b.ctypes.data, n,
+                           x.ctypes.data, n, ctypes.byref(it)) == 0
+    assert it.value == -31
+    assert solve_residual(a, x, b) < TOL * EPS
+
+
+def test_dsposv_nonspd(L):
+    """Not positive definite: the FP64 path reports LAPACK's info."""
+    set_nb(L, 64)
+    n = 200
+    a, b = gen.diag_dominant(n, 1, seed=6)
+    a = gen.zerocol(a, 150)
+    x = np.zeros_like(b, order="F")
+    it = ctypes.c_int()
+    info = L.plasma_dsposv(LO, n, 1, a.ctypes.data, n, b.ctypes.data, n,
+                           x.ctypes.data, n, ctypes.byref(it))
+    assert info == 151
+    assert it.value == -31
+
+
+# ------------------------------------------------------------------ async API
+def test_async_tile_interface(L):
+    """plasma_desc_* + plasma_omp_* + plasma_sequence_wait, as a tile-API
+    caller of the reference would chain them."""
+    set_nb(L, 64)
+    n, nrhs = 200, 3
+    a, b = gen.diag_dominant(n, nrhs, seed=31)
+    A, B = pb.plasma_desc_t(), pb.plasma_desc_t()
+    assert L.plasma_desc_triangular_create(pb.PlasmaRealDouble, LO, 64, 64, n, n,
+                                           0, 0, n, n, ctypes.byref(A)) == 0
+    assert L.plasma_desc_general_create(pb.PlasmaRealDouble, 64, 64, n, nrhs,
+                                        0, 0, n, nrhs, ctypes.byref(B)) == 0
+    seq, req = pb.new_sequence()
+    af, bf = np.asfortranarray(a.copy()), np.asfortranarray(b.copy())
+    L.plasma_omp_dtr2desc(af.ctypes.data, n, A, ctypes.byref(seq), ctypes.byref(req))
+    L.plasma_omp_dge2desc(bf.ctypes.data, n, B, ctypes.byref(seq), ctypes.byref(req))
+    L.plasma_omp_dposv(LO, A, B, ctypes.byref(seq), ctypes.byref(req))
+    L.plasma_omp_ddesc2ge(B, bf.ctypes.data, n, ctypes.byref(seq), ctypes.byref(req))
+    assert L.plasma_sequence_wait(ctypes.byref(seq)) == 0
+    assert solve_residual(a, bf, b) < TOL * EPS
+    # a failing factorisation is reported on its own request
+    bad = gen.zerocol(a, 100)
+    seq2, req2 = pb.new_sequence()
+    bad = np.asfortranarray(bad)
+    L.plasma_omp_dtr2desc(bad.ctypes.data, n, A, ctypes.byref(seq2), ctypes.byref(req2))
+    L.plasma_omp_dpotrf(LO, A, ctypes.byref(seq2), ctypes.byref(req2))
+    assert L.plasma_sequence_wait(ctypes.byref(seq2)) == 101
+    assert req2.status == 101
+    L.plasma_desc_destroy(ctypes.byref(A))
+    L.plasma_desc_destroy(ctypes.byref(B))
+
+
+def test_lookahead_off_matches(L):
+    set_nb(L, 128)
+    a, _ = gen.diag_dominant(1000, 1, seed=99)
+    L.plasma_set(pb.PlasmaLookahead, 0)
+    i0, f0 = dpotrf(L, LO, a)
+    L.plasma_set(pb.PlasmaLookahead, 1)
+    i1, f1 = dpotrf(L, LO, a)
+    assert i0 == 0 and i1 == 0
+    # same kernels, same order of operations per tile: identical bits
+    np.testing.assert_array_equal(f0, f1)
+
+
+def test_large_dposv_property(L):
+    """n = 8192, nrhs = 16 (a benchmark size): tester residual < 50 eps."""
+    import torch
+    set_nb(L, 256)
+    n, nrhs = 8192, 16
+    g = torch.Generator(device="cuda").manual_seed(7)
+    A = torch.rand(n, n, generator=g, device="cuda", dtype=torch.float64) - 0.5
+    A = torch.tril(A) + torch.tril(A, -1).T
+    A.diagonal().add_(n)
+    B = torch.rand(n, nrhs, generator=g, device="cuda", dtype=torch.float64) * 2 - 1
+    Af = A.clone()          # symmetric: row-major == column-major
+    Xf = B.T.contiguous()   # column-major n x nrhs
+    assert L.plasma_dposv(LO, n, nrhs, Af.data_ptr(), n, Xf.data_ptr(), n) == 0
+    torch.cuda.synchronize()
+    X = Xf.T
+    R = B - A @ X
+    an = A.abs().sum(1).max()
+    res = (R.abs().sum(1).max() / (n * an * X.abs().sum(1).max())).item()
+    assert res < TOL * EPS

@@ -1,0 +1,137 @@
+"""The CPU oracle pinned against LAPACK known answers (CPU only).
+
+The reference's testers accept a result when it agrees with LAPACK within
+tol * eps, tol = 50 (test/test_zpotrf.c:124-152, test/test_zposv.c:137-167,
+test/test_zcposv.c:139-193).  The oracle must pass the same checks on the
+committed fixtures before it is trusted to judge the GPU library.
+"""
+import numpy as np
+import pytest
+
+import gen
+import oracle
+from conftest import EPS, TOL, factor_error, solve_residual
+
+LO, UP = oracle.LOWER, oracle.UPPER
+
+
+@pytest.mark.parametrize("n", [1, 2, 7, 33, 64, 100])
+@pytest.mark.parametrize("nb", [1, 16, 32, 256])
+def test_potrf_matches_lapack(golden, n, nb):
+    a = golden[f"small{n}_A"]
+    for uplo, key in ((LO, "L"), (UP, "U")):
+        f = np.asfortranarray(a.copy())
+        assert oracle.potrf(uplo, f, nb) == 0
+        got = np.tril(f) if uplo == LO else np.triu(f)
+        err = factor_error(got, golden[f"small{n}_{key}"], a)
+        assert err < TOL * EPS, (uplo, err)
+
+
+@pytest.mark.parametrize("n", [7, 64, 100])
+@pytest.mark.parametrize("nb", [5, 32])
+def test_posv_potrs_match_lapack(golden, n, nb):
+    a, b = golden[f"small{n}_A"], golden[f"small{n}_B"]
+    for uplo in (LO, UP):
+        f = np.asfortranarray(a.copy())
+        x = np.asfortranarray(b.copy())
+        assert oracle.posv(uplo, f, x, nb) == 0
+        assert solve_residual(a, x, b) < TOL * EPS
+        np.testing.assert_allclose(x, golden[f"small{n}_X"], rtol=1e-12, atol=1e-14)
+        # potrs with the factor just computed
+        x2 = np.asfortranarray(b.copy())
+        assert oracle.potrs(uplo, f, x2, nb) == 0
+        np.testing.assert_allclose(x2, x, rtol=1e-13, atol=1e-15)
+
+
+@pytest.mark.parametrize("n", [300, 1000])
+def test_ragged_checksums(golden, n):
+    a, b = gen.diag_dominant(n, 5, seed=2000 + n)
+    f = np.asfortranarray(a.copy())
+    assert oracle.potrf(LO, f, 128) == 0
+    l = np.tril(f)
+    v = gen.probe_vector(n)
+    np.testing.assert_allclose(np.diag(l), golden[f"ragged{n}_diagL"], rtol=1e-14)
+    np.testing.assert_allclose(l @ v, golden[f"ragged{n}_Lv"], rtol=1e-12)
+    x = np.asfortranarray(b.copy())
+    assert oracle.posv(LO, np.asfortranarray(a.copy()), x, 128) == 0
+    np.testing.assert_allclose(x, golden[f"ragged{n}_X"], rtol=1e-12, atol=1e-15)
+
+
+def test_cfg1_parity_case(golden):
+    """n = 2048, nb = 256, nrhs = 1, seed 42: the CPU parity configuration."""
+    a, b = gen.diag_dominant(2048, 1, seed=42)
+    f = np.asfortranarray(a.copy())
+    assert oracle.potrf(LO, f, 256) == 0
+    l = np.tril(f)
+    v = gen.probe_vector(2048)
+    np.testing.assert_allclose(np.diag(l), golden["cfg1_diagL"], rtol=1e-14)
+    np.testing.assert_allclose(l @ v, golden["cfg1_Lv"], rtol=1e-12)
+    x = np.asfortranarray(b.copy())
+    assert oracle.potrs(LO, f, x, 256) == 0
+    assert solve_residual(a, x, b) < TOL * EPS
+    np.testing.assert_allclose(x, golden["cfg1_X"], rtol=1e-12)
+
+
+@pytest.mark.parametrize("n,col", [(100, 37), (300, 0), (300, 299), (513, 256)])
+def test_nonspd_info_matches_lapack(golden, n, col):
+    a, _ = gen.diag_dominant(n, 1, seed=3000 + n)
+    a = gen.zerocol(a, col)
+    for uplo, key in ((LO, "lower"), (UP, "upper")):
+        for nb in (64, 128):
+            f = np.asfortranarray(a.copy())
+            info = oracle.potrf(uplo, f, nb)
+            assert info == int(golden[f"nonspd{n}_{col}_info_{key}"]), (uplo, nb)
+
+
+@pytest.mark.parametrize("n", [64, 300])
+def test_dsposv_converges_like_reference(n):
+    a, b = gen.diag_dominant(n, 2, seed=5000 + n)
+    x = np.zeros_like(b, order="F")
+    info, it = oracle.dsposv(LO, a, b, x, 64)
+    assert info == 0
+    assert 0 <= it <= 30
+    assert solve_residual(a, x, b) < TOL * EPS
+
+
+def test_dsposv_fallback_on_fp32_failure():
+    """kappa far beyond 1/eps_fp32: the FP32 factor fails or IR stalls; the
+    FP64 path answers with iter = -31 (zcposv.c:524)."""
+    n = 128
+    a = gen.spectrum(n, 1e12, seed=11)
+    rng = np.random.default_rng(1)
+    b = np.asfortranarray(rng.standard_normal((n, 1)))
+    x = np.zeros_like(b, order="F")
+    info, it = oracle.dsposv(LO, a, b, x, 32)
+    assert info == 0
+    assert it == -31
+    assert solve_residual(a, x, b) < TOL * EPS
+
+
+@pytest.mark.parametrize("kappa", [1e2, 1e5])
+def test_dsposv_spectrum_against_lapack(golden, kappa):
+    n = 256
+    a = gen.spectrum(n, kappa, seed=11)
+    xt = golden[f"spec{int(np.log10(kappa))}_xtrue"]
+    b = np.asfortranarray(a @ xt)
+    x = np.zeros_like(b, order="F")
+    info, it = oracle.dsposv(LO, a, b, x, 64)
+    assert info == 0 and it >= 0
+    assert solve_residual(a, x, b) < TOL * EPS
+    xl = golden[f"spec{int(np.log10(kappa))}_X"]
+    # forward error bounded by kappa * backward error, like LAPACK's answer
+    assert np.abs(x - xl).max() / np.abs(xl).max() < kappa * 1e-13
+
+
+def test_lansy_inf():
+    a, _ = gen.diag_dominant(77, 1, seed=9)
+    want = np.abs(a).sum(axis=1).max()
+    assert abs(oracle.lansy_inf(LO, np.asfortranarray(np.tril(a))) - want) < 1e-12 * want
+    assert abs(oracle.lansy_inf(UP, np.asfortranarray(np.triu(a))) - want) < 1e-12 * want
+
+
+def test_single_precision_potrf():
+    a, _ = gen.diag_dominant(100, 1, seed=77)
+    f = np.asfortranarray(a.astype(np.float32))
+    assert oracle.potrf(LO, f, 32) == 0
+    l = np.tril(f).astype(np.float64)
+    assert np.linalg.norm(a - l @ l.T) / (100 * np.linalg.norm(a)) < 50 * np.finfo(np.float32).eps
