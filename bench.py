@@ -88,13 +88,14 @@ def make_system(n, nrhs, kappa, device, seed=11):
 
 
 def measured_peaks(torch):
-    """Roofline denominators.  BF16 and HBM from MEASURED_PEAKS.json; the FP64
-    and FP32/TF32 tensor peaks are not in that file, so they are measured
-    here the same way (cuBLAS GEMM, best of 5, CUDA events)."""
+    """Roofline denominators in TFLOP/s (hbm_gbs in GB/s).  BF16 and HBM from
+    MEASURED_PEAKS.json; the FP64 and FP32/TF32 peaks are not in that file, so
+    they are measured here the same way (cuBLAS GEMM, best of 5, CUDA
+    events)."""
     peaks = {}
     try:
         mp = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-        peaks["bf16"] = mp.get("bf16_tflops")
+        peaks["bf16"] = mp.get("bf16_tflops")  # already TFLOP/s
         peaks["bf16_sustained"] = mp.get("bf16_tflops_sustained")
         peaks["hbm_gbs"] = mp.get("hbm_gbs")
         peaks["source"] = "MEASURED_PEAKS.json"
@@ -118,7 +119,7 @@ def measured_peaks(torch):
             torch.cuda.synchronize()
             best = min(best, e0.elapsed_time(e1))
         torch.backends.cuda.matmul.allow_tf32 = False
-        return 2.0 * n ** 3 / best / 1e9
+        return 2.0 * n ** 3 / best / 1e9     # flops per ms / 1e9 = TFLOP/s
 
     peaks["fp64"] = gemm_tf(torch.float64, False)
     peaks["fp32"] = gemm_tf(torch.float32, False)
@@ -409,16 +410,14 @@ def main():
         "speedup_vs_dposv": (dposv["ms"] / ms) if dposv else None,
         "roofline": {"bound": "tensor" if args.mode != "fp32" else "fp32-simt",
                      "kernel": "trailing update (SYRK+GEMM)",
-                     "achieved": achieved / 1e3 if achieved else None,
-                     "peak": pk / 1e3 if pk else None, "unit": "TFLOP/s",
+                     "achieved": achieved, "peak": pk, "unit": "TFLOP/s",
                      "frac": (achieved / pk) if achieved and pk else None,
                      "peak_source": f"{pk_name} cuBLAS GEMM measured live"
                      if pk_name != "bf16" else "MEASURED_PEAKS.json bf16_tflops",
                      "traffic": traffic,
                      "launches": upd["launches"], "avg_launch_ms": upd["ms"] / max(1, upd["launches"])},
         "phases_ms_per_step": {k: v["ms"] / args.steps for k, v in prof.items()},
-        "peaks_tflops": {k: (v / 1e3 if isinstance(v, float) and k not in ("hbm_gbs",) else v)
-                         for k, v in peaks.items()},
+        "peaks_tflops": peaks,
         "e2e": e2e,
         "cpu_baseline": cpu,
         "clocks": clk,

@@ -115,7 +115,6 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
     cudaEvent_t e0 = NULL, e1 = NULL, e2 = NULL;
     if (rep) {
         memset(rep, 0, sizeof(*rep));
-        rep->factor_mode = PlasmaFactorFP32;
         rep->refinement = PlasmaRefineIR;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
@@ -132,7 +131,13 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
     int lowfail = 0;
     plasma_cuda_lag2s(S, st, call, B, Xs, PlasmaGeneral);
     plasma_cuda_lag2s(S, st, call, A, As, uplo);
-    plasma_pXpotrf(plasma, uplo, As, sequence, request, call);
+    /* As may be padded to whole tiles: identity on the padding */
+    if (As.m > A.m)
+        plasma_cuda_set_diag(S, As, A.m, As.m, 1.0);
+    int mode = plasma->mixed_mode == PlasmaFactorAuto ? PlasmaFactorTF32
+                                                      : plasma->mixed_mode;
+    if (rep) rep->factor_mode = mode;
+    plasma_pXpotrf_mode(plasma, uplo, As, sequence, request, call, mode);
     if (take_status(plasma) != 0)
         lowfail = 1;
     if (rep)
@@ -300,6 +305,9 @@ int plasma_dsposv_ex(plasma_enum_t uplo, int n, int nrhs,
     if (plasma->tuning)
         plasma_tune_potrf(plasma, PlasmaRealFloat, n);
     int nb = plasma->nb;
+    /* the low-precision operands are padded to whole tiles (identity on the
+     * padding) so that the tensor-core kernels never see a ragged tile */
+    int npad = ((n + nb - 1) / nb) * nb;
 
     plasma_desc_t A, B, X, R, As, Xs;
     memset(&A, 0, sizeof(A)); memset(&B, 0, sizeof(B));
@@ -314,10 +322,10 @@ int plasma_dsposv_ex(plasma_enum_t uplo, int n, int nrhs,
                                              0, 0, n, nrhs, &X)) != 0 ||
         (retval = plasma_desc_general_create(PlasmaRealDouble, nb, nb, n, nrhs,
                                              0, 0, n, nrhs, &R)) != 0 ||
-        (retval = plasma_desc_general_create(PlasmaRealFloat, nb, nb, n, n,
-                                             0, 0, n, n, &As)) != 0 ||
-        (retval = plasma_desc_general_create(PlasmaRealFloat, nb, nb, n, nrhs,
-                                             0, 0, n, nrhs, &Xs)) != 0) {
+        (retval = plasma_desc_general_create(PlasmaRealFloat, nb, nb, npad, npad,
+                                             0, 0, npad, npad, &As)) != 0 ||
+        (retval = plasma_desc_general_create(PlasmaRealFloat, nb, nb, npad, nrhs,
+                                             0, 0, npad, nrhs, &Xs)) != 0) {
         plasma_error("plasma_desc_general_create() failed");
         plasma_desc_destroy(&A); plasma_desc_destroy(&B);
         plasma_desc_destroy(&X); plasma_desc_destroy(&R);

@@ -54,7 +54,13 @@ void plasma_omp_Xpotrf(plasma_enum_t uplo, plasma_desc_t A,
         return;
     }
     int call = plasma_call_begin(plasma, sequence, request);
-    plasma_pXpotrf(plasma, uplo, A, sequence, request, call);
+    /* GPU-build extension: an FP32 factorisation follows
+     * PlasmaMixedPrecisionMode (TF32 / BF16 products on the tensor cores,
+     * FP32 accumulation); the default FP32 mode is plain FP32 arithmetic. */
+    int mode = A.precision == PlasmaRealFloat ? plasma->mixed_mode : 0;
+    if (mode == PlasmaFactorAuto)
+        mode = PlasmaFactorTF32;
+    plasma_pXpotrf_mode(plasma, uplo, A, sequence, request, call, mode);
 }
 
 static int Xpotrf(plasma_enum_t prec, plasma_enum_t uplo, int n, void *pA,

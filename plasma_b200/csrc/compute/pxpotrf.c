@@ -25,12 +25,37 @@
 #include "../internal.h"
 
 #include <cuda_runtime_api.h>
+#include <stdint.h>
+
+typedef struct {
+    plasma_devstat_t *st;
+    plasma_enum_t uplo;
+    plasma_desc_t A;
+    int sms;
+    int mode;          /* PlasmaFactorTF32 / BF16 on the tensor cores, else 0 */
+    char *panel[2];    /* rounded copies of panels k (alternating buffers)   */
+} walk_t;
+
+static void update(walk_t *w, cudaStream_t s, int k, int nlo, int nhi)
+{
+    if (w->mode) {
+        if (plasma_cuda_update_tc(s, w->st, w->mode, w->A, k, nlo, nhi, w->panel[k & 1]))
+            return;
+    }
+    plasma_cuda_update(s, w->st, w->uplo, w->A, k, nlo, nhi, w->sms);
+}
 
 void plasma_pXpotrf(plasma_context_t *plasma, plasma_enum_t uplo,
                     plasma_desc_t A, plasma_sequence_t *sequence,
                     plasma_request_t *request, int call)
 {
-    (void)request;
+    plasma_pXpotrf_mode(plasma, uplo, A, sequence, request, call, 0);
+}
+
+void plasma_pXpotrf_mode(plasma_context_t *plasma, plasma_enum_t uplo,
+                         plasma_desc_t A, plasma_sequence_t *sequence,
+                         plasma_request_t *request, int call, int mode)
+{
     if (sequence->status != PlasmaSuccess)
         return;
     const int mt = A.mt;
@@ -38,13 +63,38 @@ void plasma_pXpotrf(plasma_context_t *plasma, plasma_enum_t uplo,
         return;
     plasma_devstat_t *st = plasma->dstat;
     cudaStream_t S = plasma->stream;
-    const int sms = plasma->num_sms;
+
+    walk_t w;
+    w.st = st;
+    w.uplo = uplo;
+    w.A = A;
+    w.sms = plasma->num_sms;
+    w.mode = 0;
+    w.panel[0] = w.panel[1] = NULL;
+    if ((mode == PlasmaFactorTF32 || mode == PlasmaFactorBF16) &&
+        plasma_cuda_update_tc_ok(A, uplo)) {
+        size_t esz = mode == PlasmaFactorBF16 ? 2 : 4;
+        size_t one = ((size_t)A.mt * A.mb * A.mb * esz + 1023) & ~(size_t)1023;
+        char *buf = (char *)plasma_scratch(plasma, PLASMA_SLOT_MIXED, 2 * one + 1024);
+        if (buf != NULL) {
+            buf = (char *)(((uintptr_t)buf + 1023) & ~(uintptr_t)1023);
+            w.mode = mode;
+            w.panel[0] = buf;
+            w.panel[1] = buf + one;
+        }
+    }
+    /* FP32 panels: TF32 products next to a TF32/BF16 update, else the
+     * FP32-accurate split */
+    if (A.precision == PlasmaRealFloat)
+        plasma_cuda_panel_set_split(w.mode ? 1 : 3);
 
     if (plasma->lookahead == 0 || mt < 3) {
         for (int k = 0; k < mt; k++) {
             plasma_cuda_potrf_tile(S, st, call, uplo, A, k, A.nb * k, NULL);
             plasma_cuda_trsm_panel(S, st, uplo, A, k, k + 1, mt, NULL);
-            plasma_cuda_update(S, st, uplo, A, k, k + 1, mt, sms);
+            if (w.mode)
+                plasma_cuda_panel_round(S, st, w.mode, A, k, w.panel[k & 1]);
+            update(&w, S, k, k + 1, mt);
         }
         return;
     }
@@ -67,23 +117,27 @@ void plasma_pXpotrf(plasma_context_t *plasma, plasma_enum_t uplo,
         plasma_cuda_trsm_panel(crit, st, uplo, A, k, k + 1, mt, NULL);
         if (k + 1 >= mt)
             break;
-        cudaEventRecord(ev_panel, crit);
-
-        /* critical: the next panel column, after the bulk stream is done
-         * with it (its step k-1 update of column k+1) */
+        /* the bulk stream is done with column k+1 (its step k-1 update) and,
+         * since N(k-1) follows the whole step k-2 update on that stream, with
+         * the panel buffer that the rounded copy of panel k is about to reuse */
         if (have_next)
             cudaStreamWaitEvent(crit, ev_next, 0);
-        plasma_cuda_update(crit, st, uplo, A, k, k + 1, k + 2, sms);
+        if (w.mode)
+            plasma_cuda_panel_round(crit, st, w.mode, A, k, w.panel[k & 1]);
+        cudaEventRecord(ev_panel, crit);
+
+        /* critical: the next panel column */
+        update(&w, crit, k, k + 1, k + 2);
 
         /* bulk: the rest of step k */
         have_next = 0;
         if (k + 2 < mt) {
             cudaStreamWaitEvent(bulk, ev_panel, 0);
-            plasma_cuda_update(bulk, st, uplo, A, k, k + 2, k + 3, sms);
+            update(&w, bulk, k, k + 2, k + 3);
             cudaEventRecord(ev_next, bulk);
             have_next = 1;
             if (k + 3 < mt)
-                plasma_cuda_update(bulk, st, uplo, A, k, k + 3, mt, sms);
+                update(&w, bulk, k, k + 3, mt);
         }
     }
     cudaEventRecord(ev_crit_end, crit);

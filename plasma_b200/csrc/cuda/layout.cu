@@ -70,8 +70,9 @@ k_tile_copy(plasma_desc_t A, plasma_desc_t B, int uplo,
     if (plasma_failed(st)) return;
     int m = blockIdx.x, n = blockIdx.y;
     if (!tile_in(uplo, m, n)) return;
-    int rows = plasma_tile_mview(A, m);
-    int cols = plasma_tile_nview(A, n);
+    // source and destination may have different (padded) shapes
+    int rows = min(plasma_tile_mview(A, m), plasma_tile_mview(B, m));
+    int cols = min(plasma_tile_nview(A, n), plasma_tile_nview(B, n));
     const TA *a = (const TA *)plasma_tile_addr(A, m, n);
     TB *b = (TB *)plasma_tile_addr(B, m, n);
     int lda = plasma_tile_mmain(A, m);
@@ -105,6 +106,17 @@ k_tile_add(plasma_desc_t R, plasma_desc_t X, const plasma_devstat_t *st)
         int y = e % rows, c = e / rows;
         x[(size_t)c * ldx + y] += r[(size_t)c * ldr + y];
     }
+}
+
+// A(i,i) = v for i in [i0, i1)
+template <typename T>
+__global__ void k_set_diag(plasma_desc_t A, int i0, int i1, T v)
+{
+    int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= i1) return;
+    int m = i / A.mb, r = i % A.mb;
+    T *t = (T *)plasma_tile_addr(A, m, m);
+    t[(size_t)r * plasma_tile_mmain(A, m) + r] = v;
 }
 
 dim3 tile_grid(const plasma_desc_t &A)
@@ -183,4 +195,16 @@ extern "C" void plasma_cuda_geadd(cudaStream_t s, plasma_devstat_t *st,
         k_tile_add<double><<<tile_grid(X), kThreads, 0, s>>>(R, X, st);
     else
         k_tile_add<float><<<tile_grid(X), kThreads, 0, s>>>(R, X, st);
+}
+
+extern "C" void plasma_cuda_set_diag(cudaStream_t s, plasma_desc_t A, int i0,
+                                     int i1, double value)
+{
+    if (i1 <= i0) return;
+    PLASMA_COUNT_LAUNCH();
+    int n = i1 - i0;
+    if (A.precision == PlasmaRealDouble)
+        k_set_diag<double><<<(n + 255) / 256, 256, 0, s>>>(A, i0, i1, value);
+    else
+        k_set_diag<float><<<(n + 255) / 256, 256, 0, s>>>(A, i0, i1, (float)value);
 }

@@ -277,12 +277,21 @@ void launch_trtri(cudaStream_t s, plasma_devstat_t *st, int uplo,
 
 }  // namespace
 
+extern "C" int plasma_cuda_potrf_diag_fast(cudaStream_t s, plasma_devstat_t *st,
+                                          int call, plasma_enum_t uplo,
+                                          plasma_desc_t A, int k, int iinfo);
+extern "C" int plasma_cuda_trsm_panel_fast(cudaStream_t s, plasma_devstat_t *st,
+                                          plasma_enum_t uplo, plasma_desc_t A,
+                                          int k, int mlo, int mhi);
+
 extern "C" void plasma_cuda_potrf_tile(cudaStream_t s, plasma_devstat_t *st,
                                        int call, plasma_enum_t uplo,
                                        plasma_desc_t A, int k, int iinfo,
                                        void *winv)
 {
     (void)winv;
+    if (plasma_cuda_potrf_diag_fast(s, st, call, uplo, A, k, iinfo))
+        return;
     PLASMA_COUNT_LAUNCH();
     double nk = plasma_tile_mview(A, k);
     int prof = plasma_prof_begin(s);
@@ -301,6 +310,8 @@ extern "C" void plasma_cuda_trsm_panel(cudaStream_t s, plasma_devstat_t *st,
 {
     (void)winv;
     if (mhi <= mlo) return;
+    if (plasma_cuda_trsm_panel_fast(s, st, uplo, A, k, mlo, mhi))
+        return;
     PLASMA_COUNT_LAUNCH();
     double nk = plasma_tile_mview(A, k), rows = 0;
     for (int m = mlo; m < mhi; m++) rows += plasma_tile_mview(A, m);

@@ -58,38 +58,69 @@ __host__ __device__ __forceinline__ long long count_items(int nlo, int nhi,
 
 // ---------------------------------------------------------------------------
 // FP64 DMMA kernel (lower storage, tiles column-major)
+//
+// CTA tile 128 x 64 (C rows x cols), 8 warps as 4 x 2, warp tile 32 x 32 =
+// 2 x 4 m16n8k8 fragments; K streamed in chunks of 16 through a 4-stage
+// cp.async ring.  At most 128 registers per thread so that two CTAs share an
+// SM: one CTA's epilogue (a read-modify-write of C from HBM) overlaps the
+// other's tensor-core main loop.  The C block is prefetched into L2 when the
+// item starts, so the epilogue reads hit L2.
 // ---------------------------------------------------------------------------
+constexpr int DBM = 128;
+constexpr int DBN = 64;
 constexpr int DBK = 16;
-constexpr int DSTAGES = 3;
-constexpr int DPAD = 4;                 // row stride 132 doubles: conflict-free
-constexpr int DLDS_A = BM + DPAD;
-constexpr int DLDS_B = BN + DPAD;
+constexpr int DSTAGES = 4;
+constexpr int DPAD = 4;                 // row strides 132 / 68 doubles
+constexpr int DLDS_A = DBM + DPAD;
+constexpr int DLDS_B = DBN + DPAD;
 constexpr int DSMEM = DSTAGES * DBK * (DLDS_A + DLDS_B) * (int)sizeof(double);
 
 struct DmmaOperands {
     const double *a; int lda; int arows;   // A(m,k) logical rows
     const double *b; int ldb; int brows;   // A(n,k)
     int i0, j0, K;
+    bool vec;                              // 16-byte copies are legal
 };
 
 __device__ __forceinline__ void dmma_load_stage(double *As, double *Bs,
                                                 const DmmaOperands &op,
                                                 int kc, int tid)
 {
-    // A chunk: BM rows x DBK cols; element e -> row e%BM, col e/BM
+    if (op.vec) {
+        // pairs of rows: A chunk 64 pairs x 16 cols, B chunk 32 pairs x 16
 #pragma unroll
-    for (int q = 0; q < (BM * DBK) / THREADS; q++) {
+        for (int q = 0; q < (DBM * DBK / 2) / THREADS; q++) {
+            int e = tid + q * THREADS;
+            int r = 2 * (e % (DBM / 2)), c = e / (DBM / 2);
+            int gi = op.i0 + r, gk = kc + c;
+            bool v = gi < op.arows && gk < op.K;
+            const double *src = v ? op.a + (size_t)gk * op.lda + gi : op.a;
+            cp_async_16(As + c * DLDS_A + r, src, v);
+        }
+#pragma unroll
+        for (int q = 0; q < (DBN * DBK / 2) / THREADS; q++) {
+            int e = tid + q * THREADS;
+            int r = 2 * (e % (DBN / 2)), c = e / (DBN / 2);
+            int gj = op.j0 + r, gk = kc + c;
+            bool v = gj < op.brows && gk < op.K;
+            const double *src = v ? op.b + (size_t)gk * op.ldb + gj : op.b;
+            cp_async_16(Bs + c * DLDS_B + r, src, v);
+        }
+        return;
+    }
+#pragma unroll
+    for (int q = 0; q < (DBM * DBK) / THREADS; q++) {
         int e = tid + q * THREADS;
-        int r = e % BM, c = e / BM;
+        int r = e % DBM, c = e / DBM;
         int gi = op.i0 + r, gk = kc + c;
         bool v = gi < op.arows && gk < op.K;
         const double *src = v ? op.a + (size_t)gk * op.lda + gi : op.a;
         cp_async_8(As + c * DLDS_A + r, src, v);
     }
 #pragma unroll
-    for (int q = 0; q < (BN * DBK) / THREADS; q++) {
+    for (int q = 0; q < (DBN * DBK) / THREADS; q++) {
         int e = tid + q * THREADS;
-        int r = e % BN, c = e / BN;
+        int r = e % DBN, c = e / DBN;
         int gj = op.j0 + r, gk = kc + c;
         bool v = gj < op.brows && gk < op.K;
         const double *src = v ? op.b + (size_t)gk * op.ldb + gj : op.b;
@@ -97,7 +128,7 @@ __device__ __forceinline__ void dmma_load_stage(double *As, double *Bs,
     }
 }
 
-__global__ void __launch_bounds__(THREADS, 1)
+__global__ void __launch_bounds__(THREADS, 2)
 k_update_dmma(plasma_desc_t A, int k, int nlo, int nhi, int nitems,
               const plasma_devstat_t *st)
 {
@@ -109,30 +140,53 @@ k_update_dmma(plasma_desc_t A, int k, int nlo, int nhi, int nitems,
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, t = lane & 3;
-    const int wm = warp >> 2;          // 0..1 -> 64 rows each
-    const int wn = warp & 3;           // 0..3 -> 32 cols each
+    const int wm = warp >> 1;          // 0..3 -> 32 rows each
+    const int wn = warp & 1;           // 0..1 -> 32 cols each
     const int mt = A.mt;
-    const int sb = (A.mb + BM - 1) / BM;
+    const int sbm = (A.mb + DBM - 1) / DBM;
+    const int sbn = (A.mb + DBN - 1) / DBN;
 
     for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
         Item it;
-        if (!decode_item(w, k, nlo, nhi, mt, sb, it)) break;
-        if (it.m == it.n && it.sj > it.si) continue;     // strict upper block
+        {
+            int per = sbm * sbn;
+            int p = w / per, s = w - p * per;
+            it.si = s / sbn;
+            it.sj = s - it.si * sbn;
+            int n = nlo;
+            while (n < nhi && p >= mt - n) { p -= mt - n; n++; }
+            if (n >= nhi) break;
+            it.n = n;
+            it.m = n + p;
+        }
         DmmaOperands op;
+        op.i0 = it.si * DBM;
+        op.j0 = it.sj * DBN;
+        // a block of a diagonal tile that lies strictly above the diagonal
+        if (it.m == it.n && op.j0 > op.i0 + DBM - 1) continue;
         op.a = (const double *)plasma_tile_addr(A, it.m, k);
         op.lda = plasma_tile_mmain(A, it.m);
         op.arows = plasma_tile_mview(A, it.m);
         op.b = (const double *)plasma_tile_addr(A, it.n, k);
         op.ldb = plasma_tile_mmain(A, it.n);
         op.brows = plasma_tile_mview(A, it.n);
-        op.i0 = it.si * BM;
-        op.j0 = it.sj * BN;
         op.K = plasma_tile_nview(A, k);
         if (op.i0 >= op.arows || op.j0 >= op.brows) continue;
+        op.vec = ((op.lda | op.ldb | op.arows | op.brows) & 1) == 0;
 
-        double acc[4][4][4];
+        double *C = (double *)plasma_tile_addr(A, it.m, it.n);
+        const int ldc = plasma_tile_mmain(A, it.m);
+        // warm L2 with the C block: 64 columns x 128 rows = 512 lines
+        for (int e = tid; e < DBN * (DBM / 16); e += THREADS) {
+            int j = op.j0 + e / (DBM / 16);
+            int i = op.i0 + (e % (DBM / 16)) * 16;
+            if (j < op.brows && i < op.arows)
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(C + (size_t)j * ldc + i));
+        }
+
+        double acc[2][4][4];
 #pragma unroll
-        for (int a = 0; a < 4; a++)
+        for (int a = 0; a < 2; a++)
 #pragma unroll
             for (int b = 0; b < 4; b++)
 #pragma unroll
@@ -150,7 +204,6 @@ k_update_dmma(plasma_desc_t A, int k, int nlo, int nhi, int nitems,
         for (int kt = 0; kt < nk; kt++) {
             cp_async_wait<DSTAGES - 2>();
             __syncthreads();
-            // prefetch stage kt + STAGES-1 (its slot was consumed at kt-1)
             int pf = kt + DSTAGES - 1;
             if (pf < nk) {
                 int sl = pf % DSTAGES;
@@ -159,7 +212,7 @@ k_update_dmma(plasma_desc_t A, int k, int nlo, int nhi, int nitems,
             }
             cp_async_commit();
 
-            const double *as = As + (kt % DSTAGES) * DBK * DLDS_A + wm * 64;
+            const double *as = As + (kt % DSTAGES) * DBK * DLDS_A + wm * 32;
             const double *bs = Bs + (kt % DSTAGES) * DBK * DLDS_B + wn * 32;
 #pragma unroll
             for (int k8 = 0; k8 < DBK; k8 += 8) {
@@ -170,7 +223,7 @@ k_update_dmma(plasma_desc_t A, int k, int nlo, int nhi, int nitems,
                     bf[ni][1] = bs[(k8 + t + 4) * DLDS_B + ni * 8 + g];
                 }
 #pragma unroll
-                for (int mi = 0; mi < 4; mi++) {
+                for (int mi = 0; mi < 2; mi++) {
                     double af[4];
                     af[0] = as[(k8 + t) * DLDS_A + mi * 16 + g];
                     af[1] = as[(k8 + t) * DLDS_A + mi * 16 + g + 8];
@@ -184,26 +237,36 @@ k_update_dmma(plasma_desc_t A, int k, int nlo, int nhi, int nitems,
         }
         cp_async_wait<0>();
 
-        // epilogue: C -= acc, masking rows/cols outside the tile and the
-        // strict upper triangle of a diagonal tile
-        double *C = (double *)plasma_tile_addr(A, it.m, it.n);
-        const int ldc = plasma_tile_mmain(A, it.m);
+        // epilogue: C -= acc.  All loads of one row fragment are issued
+        // before any store so that their latencies overlap.
         const bool diag = it.m == it.n;
 #pragma unroll
-        for (int mi = 0; mi < 4; mi++) {
+        for (int mi = 0; mi < 2; mi++) {
+            double cv[2][4][2];
 #pragma unroll
             for (int h = 0; h < 2; h++) {
-                int i = op.i0 + wm * 64 + mi * 16 + g + h * 8;
-                if (i >= op.arows) continue;
+                int i = op.i0 + wm * 32 + mi * 16 + g + h * 8;
 #pragma unroll
-                for (int ni = 0; ni < 4; ni++) {
+                for (int ni = 0; ni < 4; ni++)
 #pragma unroll
                     for (int e = 0; e < 2; e++) {
                         int j = op.j0 + wn * 32 + ni * 8 + 2 * t + e;
-                        if (j < op.brows && (!diag || i >= j))
-                            C[(size_t)j * ldc + i] -= acc[mi][ni][h * 2 + e];
+                        bool ok = i < op.arows && j < op.brows && (!diag || i >= j);
+                        cv[h][ni][e] = ok ? C[(size_t)j * ldc + i] : 0.0;
                     }
-                }
+            }
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                int i = op.i0 + wm * 32 + mi * 16 + g + h * 8;
+#pragma unroll
+                for (int ni = 0; ni < 4; ni++)
+#pragma unroll
+                    for (int e = 0; e < 2; e++) {
+                        int j = op.j0 + wn * 32 + ni * 8 + 2 * t + e;
+                        bool ok = i < op.arows && j < op.brows && (!diag || i >= j);
+                        if (ok)
+                            C[(size_t)j * ldc + i] = cv[h][ni][e] - acc[mi][ni][h * 2 + e];
+                    }
             }
         }
     }
@@ -294,8 +357,13 @@ extern "C" void plasma_cuda_update(cudaStream_t s, plasma_devstat_t *st,
                                    int nlo, int nhi, int num_sms)
 {
     if (nhi <= nlo) return;
+    const bool dmma = A.precision == PlasmaRealDouble && uplo == PlasmaLower;
     int sb = (A.mb + BM - 1) / BM;
     long long nitems = count_items(nlo, nhi, A.mt, sb);
+    if (dmma) {
+        long long pairs = count_items(nlo, nhi, A.mt, 1);
+        nitems = pairs * ((A.mb + DBM - 1) / DBM) * ((A.mb + DBN - 1) / DBN);
+    }
     if (nitems <= 0) return;
     PLASMA_COUNT_LAUNCH();
     // algorithmic work of this launch: SYRK on diagonal tiles, GEMM below
@@ -313,7 +381,7 @@ extern "C" void plasma_cuda_update(cudaStream_t s, plasma_devstat_t *st,
         }
     }
     int prof = plasma_prof_begin(s);
-    if (A.precision == PlasmaRealDouble && uplo == PlasmaLower) {
+    if (dmma) {
         static bool attr_set = false;
         if (!attr_set) {
             cudaFuncSetAttribute(k_update_dmma,
@@ -328,7 +396,7 @@ extern "C" void plasma_cuda_update(cudaStream_t s, plasma_devstat_t *st,
         k_update_dmma<<<(unsigned)grid, THREADS, DSMEM, s>>>(
             A, k, nlo, nhi, (int)nitems, st);
     } else {
-        long long grid = nitems < 2LL * num_sms ? nitems : 2LL * num_sms;
+        long long grid = nitems;     // one CTA per item (see above)
         if (A.precision == PlasmaRealDouble)
             k_update_simt<double><<<(unsigned)grid, THREADS, 0, s>>>(
                 A, uplo, k, nlo, nhi, (int)nitems, st);

@@ -174,10 +174,31 @@ void plasma_cuda_geadd(cudaStream_t s, plasma_devstat_t *st,
 void plasma_cuda_lacpy(cudaStream_t s, plasma_devstat_t *st,
                        plasma_desc_t A, plasma_desc_t B);
 
-/* Host-side DAG walkers (compute/). */
+/* Tensor-core (tcgen05) trailing update of FP32 factors with TF32 or BF16
+ * products (cuda/update_tc.cu). */
+int plasma_cuda_update_tc_ok(plasma_desc_t A, plasma_enum_t uplo);
+int plasma_cuda_update_tc(cudaStream_t s, plasma_devstat_t *st, int mode,
+                          plasma_desc_t A, int k, int nlo, int nhi,
+                          const void *panel);
+/* Copy of panel k rounded to the product precision of mode (TF32 or BF16),
+ * tile m at panel + m*nb*nb elements. */
+void plasma_cuda_panel_round(cudaStream_t s, plasma_devstat_t *st, int mode,
+                             plasma_desc_t A, int k, void *panel);
+/* FP32 panel kernels: 3 = FP32-accurate split TF32 products, 1 = TF32. */
+void plasma_cuda_panel_set_split(int split);
+/* A(i,i) = value for i in [i0, i1) (identity padding of FP32 factors). */
+void plasma_cuda_set_diag(cudaStream_t s, plasma_desc_t A, int i0, int i1,
+                          double value);
+
+/* Host-side DAG walkers (compute/).  mode selects the trailing update of
+ * FP32 factors: 0 or PlasmaFactorFP32 = FP32 arithmetic, PlasmaFactorTF32 /
+ * PlasmaFactorBF16 = tensor-core products accumulated in FP32. */
 void plasma_pXpotrf(plasma_context_t *plasma, plasma_enum_t uplo,
                     plasma_desc_t A, plasma_sequence_t *sequence,
                     plasma_request_t *request, int call);
+void plasma_pXpotrf_mode(plasma_context_t *plasma, plasma_enum_t uplo,
+                         plasma_desc_t A, plasma_sequence_t *sequence,
+                         plasma_request_t *request, int call, int mode);
 void plasma_pXpotrs(plasma_context_t *plasma, plasma_enum_t uplo,
                     plasma_desc_t A, plasma_desc_t B,
                     plasma_sequence_t *sequence, plasma_request_t *request);

@@ -333,3 +333,77 @@ def test_large_dposv_property(L):
     an = A.abs().sum(1).max()
     res = (R.abs().sum(1).max() / (n * an * X.abs().sum(1).max())).item()
     assert res < TOL * EPS
+
+
+# ------------------------------------------------------------------ tensor-core factors
+def dsposv_ex(L, uplo, a, b):
+    n, nrhs = b.shape
+    x = np.zeros((n, nrhs), order="F")
+    it = ctypes.c_int(-99)
+    info = pb.plasma_dsposv_info_t()
+    rc = L.plasma_dsposv_ex(uplo, n, nrhs, a.ctypes.data, n, b.ctypes.data, n,
+                            x.ctypes.data, n, ctypes.byref(it), ctypes.byref(info))
+    return rc, it.value, x, info
+
+
+@pytest.mark.parametrize("mode", [pb.PlasmaFactorTF32, pb.PlasmaFactorBF16])
+@pytest.mark.parametrize("n,nb", [(1024, 256), (1000, 256), (640, 128)])
+def test_dsposv_tensor_core_factor(L, mode, n, nb):
+    """TF32 / BF16 products on tcgen05 with FP32 accumulation, refined to
+    FP64 accuracy (ragged n is padded to whole tiles internally)."""
+    set_nb(L, nb)
+    L.plasma_set(pb.PlasmaMixedPrecisionMode, mode)
+    try:
+        a, b = gen.diag_dominant(n, 2, seed=700 + n)
+        rc, it, x, info = dsposv_ex(L, LO, a, b)
+        assert rc == 0
+        assert info.factor_mode == mode
+        assert 0 <= it <= 30              # diagonally dominant: IR converges
+        assert solve_residual(a, x, b) < TOL * EPS
+        xo = np.zeros_like(x, order="F")
+        assert oracle.dsposv(oracle.LOWER, a, b, xo, nb)[0] == 0
+        np.testing.assert_allclose(x, xo, rtol=1e-12, atol=1e-15)
+    finally:
+        L.plasma_set(pb.PlasmaMixedPrecisionMode, pb.PlasmaFactorFP32)
+
+
+@pytest.mark.parametrize("mode", [pb.PlasmaFactorTF32, pb.PlasmaFactorBF16])
+def test_tensor_core_factor_quality(L, mode):
+    """The low-precision factor itself: ||A - L L^T|| / ||A|| at the level of
+    the product precision (checked through one refinement-free solve)."""
+    set_nb(L, 256)
+    L.plasma_set(pb.PlasmaMixedPrecisionMode, mode)
+    try:
+        n = 1536
+        a = gen.spectrum(n, 1e2, seed=11)
+        xt = np.random.default_rng(12).standard_normal((n, 1))
+        b = np.asfortranarray(a @ xt)
+        rc, it, x, info = dsposv_ex(L, LO, a, b)
+        assert rc == 0 and it >= 0
+        assert solve_residual(a, x, b) < TOL * EPS
+        assert np.abs(x - xt).max() / np.abs(xt).max() < 1e-12
+        # convergence speed reflects the product precision
+        assert it <= (6 if mode == pb.PlasmaFactorTF32 else 12)
+    finally:
+        L.plasma_set(pb.PlasmaMixedPrecisionMode, pb.PlasmaFactorFP32)
+
+
+@pytest.mark.parametrize("mode,bound", [(pb.PlasmaFactorFP32, 2e-6),
+                                        (pb.PlasmaFactorTF32, 4e-3),
+                                        (pb.PlasmaFactorBF16, 3e-2)])
+@pytest.mark.parametrize("n,nb", [(1024, 256), (768, 128)])
+def test_low_precision_factor_backward_error(L, mode, bound, n, nb):
+    """spotrf with the product precision of PlasmaMixedPrecisionMode on a
+    matrix whose off-diagonal part matters: ||A - L L^T||_F / ||A||_F is at
+    the level of the product precision (a wrong tile or operand gives O(1))."""
+    set_nb(L, nb)
+    L.plasma_set(pb.PlasmaMixedPrecisionMode, mode)
+    try:
+        a = gen.spectrum(n, 1e3, seed=11)
+        f = np.asfortranarray(a.astype(np.float32))
+        assert L.plasma_spotrf(LO, n, f.ctypes.data, n) == 0
+        l = np.tril(f).astype(np.float64)
+        berr = np.linalg.norm(a - l @ l.T) / np.linalg.norm(a)
+        assert berr < bound, berr
+    finally:
+        L.plasma_set(pb.PlasmaMixedPrecisionMode, pb.PlasmaFactorFP32)
