@@ -43,13 +43,6 @@ void plasma_tune_potrf(plasma_context_t *plasma, plasma_enum_t dtyp, int n);
 
 #define ITERMAX 30
 
-static int conv(const double *Rnorm, const double *Xnorm, int n, double cte)
-{
-    for (int i = 0; i < n; i++)
-        if (!(Rnorm[i] <= Xnorm[i] * cte))
-            return 0;
-    return 1;
-}
 
 /* Reads the device status (after a stream sync); returns it and clears it so
  * that the next phase starts clean. */
@@ -66,22 +59,177 @@ static int take_status(plasma_context_t *plasma)
     return s;
 }
 
-/* R = B - A X, norms to the host arrays, returns conv() */
-static int residual_check(plasma_context_t *plasma, plasma_enum_t uplo,
-                          plasma_desc_t A, plasma_desc_t B, plasma_desc_t X,
-                          plasma_desc_t R, double *d_norms, double *Rnorm,
-                          double *Xnorm, double cte)
+/* ------------------------------------------------------------------------
+ * Refinement on contiguous vectors, one right-hand side at a time.
+ * ---------------------------------------------------------------------- */
+#define GMRES_RESTART 40
+#define GMRES_TOL 1e-6
+
+typedef struct {
+    plasma_context_t *plasma;
+    plasma_enum_t uplo;
+    plasma_desc_t A, As;
+    const void *W32;
+    int call;
+    size_t n, npad;
+    double *b, *x, *r, *w, *z, *V;   /* FP64 vectors, V: (m+1) x n basis */
+    const double *dscale;             /* D^{-1} of a scaled factor, or NULL */
+    int fast;                         /* one-launch sweeps (else tile sweeps) */
+    float *ws;                        /* FP32 work vector (npad)        */
+    double *dh, *dnorm, *dwork;       /* small device buffers           */
+    double *symv_work;
+    int gmres_iters;
+} refine_t;
+
+/* out = M^{-1} in with M the low-precision factorisation of A */
+static void precond(refine_t *R, const double *in, double *out)
 {
-    int nrhs = B.n;
-    double *d_x = d_norms, *d_r = d_norms + nrhs;
-    plasma_cuda_residual(plasma->stream, plasma->dstat, uplo, A, B, X, R,
-                         d_x, d_r);
-    cudaMemcpyAsync(Xnorm, d_x, sizeof(double) * nrhs, cudaMemcpyDeviceToHost,
-                    plasma->stream);
-    cudaMemcpyAsync(Rnorm, d_r, sizeof(double) * nrhs, cudaMemcpyDeviceToHost,
-                    plasma->stream);
-    cudaStreamSynchronize(plasma->stream);
-    return conv(Rnorm, Xnorm, nrhs, cte);
+    cudaStream_t S = R->plasma->stream;
+    /* M = D^{-1} L L^T D^{-1} when the factor is of the scaled matrix
+     * D A D (+ shift): M^{-1} v = D (L L^T)^{-1} D v */
+    plasma_cuda_d2s(S, in, R->dscale, R->ws, R->n, R->npad, R->plasma->dstat, R->call);
+    if (R->fast) {
+        plasma_sweep(R->plasma, R->uplo, 0, R->As, R->W32, R->ws);
+        plasma_sweep(R->plasma, R->uplo, 1, R->As, R->W32, R->ws);
+    } else {
+        /* the vector viewed as an npad x 1 tile descriptor */
+        plasma_desc_t V;
+        plasma_desc_general_init(PlasmaRealFloat, R->ws, R->As.mb, R->As.nb,
+                                 (int)R->npad, 1, 0, 0, (int)R->npad, 1, &V);
+        plasma_cuda_trsm_sweep(S, R->plasma->dstat, R->uplo, PlasmaNoTrans,
+                               R->As, V, (void *)R->W32, 1);
+        plasma_cuda_trsm_sweep(S, R->plasma->dstat, R->uplo, PlasmaTrans,
+                               R->As, V, (void *)R->W32, 1);
+    }
+    plasma_cuda_s2d(S, R->ws, R->dscale, out, R->n);
+}
+
+/* r = b - A x, returns the max norms of x and r through the host pointers */
+static void residual_vec(refine_t *R, double *xn, double *rn)
+{
+    cudaStream_t S = R->plasma->stream;
+    plasma_cuda_symv(S, R->plasma->dstat, R->uplo, R->A, R->x, R->b, R->r,
+                     R->dnorm, R->dnorm + 1, R->symv_work);
+    double h[2];
+    cudaMemcpyAsync(h, R->dnorm, sizeof(h), cudaMemcpyDeviceToHost, S);
+    cudaStreamSynchronize(S);
+    *xn = h[0];
+    *rn = h[1];
+}
+
+static double dot_host(refine_t *R, const double *a, const double *b)
+{
+    cudaStream_t S = R->plasma->stream;
+    double v;
+    plasma_cuda_dots(S, a, 0, 1, b, R->n, R->dh, R->dwork);
+    cudaMemcpyAsync(&v, R->dh, sizeof(double), cudaMemcpyDeviceToHost, S);
+    cudaStreamSynchronize(S);
+    return v;
+}
+
+/* One GMRES solve of M^{-1} A d = M^{-1} r (restart length GMRES_RESTART,
+ * relative tolerance GMRES_TOL), x += d.  Returns the inner iterations. */
+static int gmres_correction(refine_t *R)
+{
+    cudaStream_t S = R->plasma->stream;
+    const size_t n = R->n;
+    const int m = GMRES_RESTART;
+    double H[GMRES_RESTART + 1][GMRES_RESTART];
+    double cs[GMRES_RESTART], sn[GMRES_RESTART], g[GMRES_RESTART + 1];
+    double hcol[GMRES_RESTART + 1], hcol2[GMRES_RESTART + 1], y[GMRES_RESTART];
+
+    precond(R, R->r, R->z);
+    double beta = sqrt(dot_host(R, R->z, R->z));
+    if (!(beta > 0.0))
+        return 0;
+    plasma_cuda_axpby(S, 1.0 / beta, R->z, R->V, n, 0);
+    for (int i = 0; i <= m; i++) g[i] = 0.0;
+    g[0] = beta;
+    int k = 0;
+    for (int j = 0; j < m; j++) {
+        double *vj = R->V + (size_t)j * n;
+        /* w = M^{-1} A v_j */
+        plasma_cuda_symv(S, R->plasma->dstat, R->uplo, R->A, vj, NULL, R->z,
+                         NULL, NULL, R->symv_work);
+        precond(R, R->z, R->w);
+        /* classical Gram-Schmidt, twice */
+        plasma_cuda_dots(S, R->V, n, j + 1, R->w, n, R->dh, R->dwork);
+        plasma_cuda_sub_combo(S, R->V, n, j + 1, R->dh, R->w, n);
+        cudaMemcpyAsync(hcol, R->dh, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, S);
+        plasma_cuda_dots(S, R->V, n, j + 1, R->w, n, R->dh, R->dwork);
+        plasma_cuda_sub_combo(S, R->V, n, j + 1, R->dh, R->w, n);
+        cudaMemcpyAsync(hcol2, R->dh, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, S);
+        cudaStreamSynchronize(S);
+        for (int i = 0; i <= j; i++) hcol[i] += hcol2[i];
+        double hn = sqrt(dot_host(R, R->w, R->w));
+        hcol[j + 1] = hn;
+        if (hn > 0.0)
+            plasma_cuda_axpby(S, 1.0 / hn, R->w, R->V + (size_t)(j + 1) * n, n, 0);
+        /* Givens rotations on the new Hessenberg column */
+        for (int i = 0; i < j; i++) {
+            double t = cs[i] * hcol[i] + sn[i] * hcol[i + 1];
+            hcol[i + 1] = -sn[i] * hcol[i] + cs[i] * hcol[i + 1];
+            hcol[i] = t;
+        }
+        double a = hcol[j], bb = hcol[j + 1];
+        double rr = hypot(a, bb);
+        cs[j] = rr > 0.0 ? a / rr : 1.0;
+        sn[j] = rr > 0.0 ? bb / rr : 0.0;
+        hcol[j] = rr;
+        hcol[j + 1] = 0.0;
+        g[j + 1] = -sn[j] * g[j];
+        g[j] = cs[j] * g[j];
+        for (int i = 0; i <= j; i++) H[i][j] = hcol[i];
+        k = j + 1;
+        R->gmres_iters++;
+        if (fabs(g[j + 1]) <= GMRES_TOL * beta || !(hn > 0.0))
+            break;
+    }
+    /* back substitution H(0:k,0:k) y = g(0:k) */
+    for (int i = k - 1; i >= 0; i--) {
+        double t = g[i];
+        for (int l = i + 1; l < k; l++) t -= H[i][l] * y[l];
+        y[i] = H[i][i] != 0.0 ? t / H[i][i] : 0.0;
+    }
+    cudaMemcpyAsync(R->dh, y, sizeof(double) * k, cudaMemcpyHostToDevice, S);
+    plasma_cuda_combo(S, R->V, n, k, R->dh, R->x, n, 1);
+    return k;
+}
+
+/* Solves for the current b: initial x = M^{-1} b, then refinement until the
+ * reference stopping rule holds.  Returns the number of refinement steps, or
+ * -1 when it did not converge within ITERMAX. */
+static int refine_column(refine_t *R, int scheme, double cte, double *xn_out,
+                         double *rn_out, int *used_gmres)
+{
+    precond(R, R->b, R->x);
+    double prev = INFINITY;
+    int gm = scheme == PlasmaRefineGMRES;
+    for (int it = 0; it <= ITERMAX; it++) {
+        double xn, rn;
+        residual_vec(R, &xn, &rn);
+        *xn_out = xn;
+        *rn_out = rn;
+        if (take_status(R->plasma) != 0)
+            return -1;                     /* FP32 overflow in a conversion */
+        /* stopping rule of the reference's conv(), zcposv.c:275-287 */
+        if (rn <= xn * cte)
+            return it;
+        if (it == ITERMAX)
+            break;
+        /* automatic scheme: switch to GMRES-IR when IR stops contracting */
+        if (scheme == PlasmaRefineAuto && !gm && it > 0 && rn > 0.5 * prev)
+            gm = 1;
+        prev = rn;
+        if (gm) {
+            *used_gmres = 1;
+            gmres_correction(R);
+        } else {
+            precond(R, R->r, R->z);
+            plasma_cuda_axpby(R->plasma->stream, 1.0, R->z, R->x, R->n, 1);
+        }
+    }
+    return -1;
 }
 
 /*
@@ -103,19 +251,20 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
 
     double *d_small = (double *)plasma_scratch(plasma, PLASMA_SLOT_SMALL,
                                                sizeof(double) * (2 * nrhs + 8));
+    const int fast_sweep = plasma_sweep_reserve(plasma, As);
+    size_t wtiles = (size_t)As.mt * As.mb * As.mb * sizeof(float);
+    size_t wblocks = plasma_cuda_trsv_w_bytes(As);
     void *W32 = plasma_scratch(plasma, PLASMA_SLOT_WORK,
-                               (size_t)As.mt * As.mb * As.mb * sizeof(float));
+                               wtiles > wblocks ? wtiles : wblocks);
     if (d_small == NULL || W32 == NULL) {
         plasma_request_fail(sequence, request, PlasmaErrorOutOfMemory);
         return;
     }
     double *d_anorm = d_small + 2 * nrhs;
-    double *d_norms = d_small;
 
     cudaEvent_t e0 = NULL, e1 = NULL, e2 = NULL;
     if (rep) {
         memset(rep, 0, sizeof(*rep));
-        rep->refinement = PlasmaRefineIR;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
         cudaEventCreate(&e2);
@@ -127,48 +276,126 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
     plasma_cuda_lansy_inf(S, st, uplo, A, d_anorm, NULL);
     cudaMemcpyAsync(&Anorm, d_anorm, sizeof(double), cudaMemcpyDeviceToHost, S);
 
-    /* low-precision phase */
-    int lowfail = 0;
-    plasma_cuda_lag2s(S, st, call, B, Xs, PlasmaGeneral);
-    plasma_cuda_lag2s(S, st, call, A, As, uplo);
-    /* As may be padded to whole tiles: identity on the padding */
-    if (As.m > A.m)
-        plasma_cuda_set_diag(S, As, A.m, As.m, 1.0);
-    int mode = plasma->mixed_mode == PlasmaFactorAuto ? PlasmaFactorTF32
-                                                      : plasma->mixed_mode;
-    if (rep) rep->factor_mode = mode;
-    plasma_pXpotrf_mode(plasma, uplo, As, sequence, request, call, mode);
-    if (take_status(plasma) != 0)
-        lowfail = 1;
-    if (rep)
-        cudaEventRecord(e1, S);
-
-    int converged = 0;
-    if (!lowfail) {
-        double cte = Anorm * eps * sqrt((double)A.n);
-        plasma_cuda_trsm_sweep(S, st, uplo, PlasmaNoTrans, As, Xs, W32, 0);
-        plasma_cuda_trsm_sweep(S, st, uplo, PlasmaTrans, As, Xs, W32, 1);
-        plasma_cuda_slag2d(S, st, Xs, X);
-        if (residual_check(plasma, uplo, A, B, X, R, d_norms, Rnorm, Xnorm, cte)) {
-            *iter = 0;
-            converged = 1;
-        }
-        for (int it = 0; !converged && it < ITERMAX; it++) {
-            plasma_cuda_lag2s(S, st, call, R, Xs, PlasmaGeneral);
-            plasma_cuda_trsm_sweep(S, st, uplo, PlasmaNoTrans, As, Xs, W32, 1);
-            plasma_cuda_trsm_sweep(S, st, uplo, PlasmaTrans, As, Xs, W32, 1);
-            plasma_cuda_slag2d(S, st, Xs, R);
-            plasma_cuda_geadd(S, st, R, X);
-            int ok = residual_check(plasma, uplo, A, B, X, R, d_norms, Rnorm,
-                                    Xnorm, cte);
-            if (take_status(plasma) != 0)
-                break;       /* overflow of the residual in FP32 */
-            if (ok) {
-                *iter = it + 1;
-                converged = 1;
-            }
-        }
+    /* ------------------------------------------------------------------
+     * Low-precision phase.  An attempt = convert A, optionally scale it to
+     * unit diagonal and shift it by c*u (Higham & Pranesh 2019), factor it
+     * with the attempt's product precision, refine.  The reference's FP32
+     * mode makes one unscaled attempt; TF32 / BF16 retry once scaled and
+     * shifted when the factorisation breaks down; Auto escalates
+     * BF16 -> TF32 -> FP32.  Whatever fails ends in the FP64 path below.
+     * ---------------------------------------------------------------- */
+    typedef struct { int mode; int scaled; } attempt_t;
+    attempt_t plan[4];
+    int nplan = 0;
+    const int cfg = plasma->mixed_mode;
+    if (cfg == PlasmaFactorAuto) {
+        plan[nplan++] = (attempt_t){PlasmaFactorBF16, 0};
+        plan[nplan++] = (attempt_t){PlasmaFactorBF16, 1};
+        plan[nplan++] = (attempt_t){PlasmaFactorTF32, 1};
+        plan[nplan++] = (attempt_t){PlasmaFactorFP32, 0};
+    } else if (cfg == PlasmaFactorFP32) {
+        plan[nplan++] = (attempt_t){PlasmaFactorFP32, 0};
+    } else {
+        plan[nplan++] = (attempt_t){cfg, 0};
+        plan[nplan++] = (attempt_t){cfg, 1};
     }
+    const int scheme = plasma->refinement;
+    const size_t n = (size_t)A.m, npad = (size_t)As.m;
+    const int mres = GMRES_RESTART;
+    double cte = 0.0;
+    int converged = 0, used_gmres = 0, gm_iters = 0, attempts = 0;
+    int factor_failed = 0;
+
+    plasma_cuda_lag2s(S, st, call, B, Xs, PlasmaGeneral);
+    size_t need = sizeof(double) * (size_t)n * (6 + mres + 1) +
+                  sizeof(double) * npad + sizeof(float) * npad + 4096;
+    char *wk = (char *)plasma_scratch(plasma, PLASMA_SLOT_REFINE, need);
+    double *small = (double *)plasma_scratch(plasma, PLASMA_SLOT_SMALL,
+                                             sizeof(double) * (2 * nrhs + 8) +
+                                             sizeof(double) * (mres + 8) +
+                                             plasma_cuda_dots_work(mres + 2));
+    double *sw = (double *)plasma_scratch(plasma, PLASMA_SLOT_SYMV,
+                                          plasma_cuda_symv_work(A));
+    if (wk == NULL || small == NULL || sw == NULL) {
+        plasma_request_fail(sequence, request, PlasmaErrorOutOfMemory);
+        return;
+    }
+    refine_t RF;
+    memset(&RF, 0, sizeof(RF));
+    RF.plasma = plasma;
+    RF.uplo = uplo;
+    RF.A = A;
+    RF.As = As;
+    RF.W32 = W32;
+    RF.fast = fast_sweep;
+    RF.call = call;
+    RF.n = n;
+    RF.npad = npad;
+    double *vp = (double *)wk;
+    RF.b = vp; vp += n;
+    RF.x = vp; vp += n;
+    RF.r = vp; vp += n;
+    RF.w = vp; vp += n;
+    RF.z = vp; vp += n;
+    RF.V = vp; vp += (size_t)n * (mres + 1);
+    double *dvec = vp; vp += npad;
+    RF.ws = (float *)vp;
+    RF.dnorm = small + 2 * nrhs + 2;
+    RF.dh = RF.dnorm + 4;
+    RF.dwork = RF.dh + mres + 4;
+    RF.symv_work = sw;
+
+    for (int a = 0; a < nplan && !converged; a++) {
+        const int mode = plan[a].mode;
+        attempts++;
+        if (rep) rep->factor_mode = mode;
+        if (a > 0 && rep) cudaEventRecord(e0, S);
+        plasma_cuda_lag2s(S, st, call, A, As, uplo);
+        /* As may be padded to whole tiles: identity on the padding */
+        if (As.m > A.m)
+            plasma_cuda_set_diag(S, As, A.m, As.m, 1.0);
+        RF.dscale = NULL;
+        if (plan[a].scaled) {
+            /* unit diagonal, then + c u I with u the unit roundoff of the
+             * products and c = 4 */
+            double u = mode == PlasmaFactorBF16 ? 0x1p-8 :
+                       mode == PlasmaFactorTF32 ? 0x1p-11 : 0x1p-24;
+            plasma_cuda_diag_rsqrt(S, A, dvec, n, npad);
+            plasma_cuda_scale_shift(S, As, uplo, dvec, (float)(4.0 * u));
+            RF.dscale = dvec;
+        }
+        plasma_pXpotrf_mode(plasma, uplo, As, sequence, request, call, mode);
+        factor_failed = take_status(plasma) != 0;
+        if (rep)
+            cudaEventRecord(e1, S);
+        if (factor_failed)
+            continue;
+
+        cte = Anorm * eps * sqrt((double)A.n);
+        /* inverses of the diagonal blocks of the factor, used by every sweep */
+        if (fast_sweep)
+            plasma_cuda_trtri_blocks(S, st, uplo, As, W32);
+        else
+            plasma_cuda_trtri_tiles(S, st, uplo, As, W32);
+        converged = 1;
+        int itmax = 0;
+        for (int j = 0; j < nrhs; j++) {
+            plasma_cuda_column(S, B, j, RF.b, 1);
+            double xn = 0, rn = 0;
+            int it = refine_column(&RF, scheme, cte, &xn, &rn, &used_gmres);
+            Xnorm[j] = xn;
+            Rnorm[j] = rn;
+            if (it < 0) {
+                converged = 0;
+                break;
+            }
+            if (it > itmax) itmax = it;
+            plasma_cuda_column(S, X, j, RF.x, 0);
+        }
+        if (converged)
+            *iter = itmax;
+    }
+    gm_iters = RF.gmres_iters;
     if (rep) {
         cudaEventRecord(e2, S);
         cudaEventSynchronize(e2);
@@ -179,7 +406,9 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
         rep->refine_ms = ms2;
         rep->ir_iterations = converged ? *iter : ITERMAX;
         rep->anorm = Anorm;
-        rep->attempts = 1;
+        rep->attempts = attempts;
+        rep->refinement = used_gmres ? PlasmaRefineGMRES : PlasmaRefineIR;
+        rep->gmres_iterations = gm_iters;
     }
     if (converged) {
         if (rep) {

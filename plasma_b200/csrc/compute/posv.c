@@ -30,10 +30,20 @@ void plasma_pXpotrs(plasma_context_t *plasma, plasma_enum_t uplo,
     if (sequence->status != PlasmaSuccess)
         return;
     size_t elem = plasma_element_size(A.precision);
-    void *W = plasma_scratch(plasma, PLASMA_SLOT_WORK,
-                             (size_t)A.mt * A.mb * A.mb * elem);
+    size_t wb = (size_t)A.mt * A.mb * A.mb * elem;
+    size_t wv = plasma_cuda_trsv_w_bytes(A);
+    void *W = plasma_scratch(plasma, PLASMA_SLOT_WORK, wb > wv ? wb : wv);
     if (W == NULL) {
         plasma_request_fail(sequence, request, PlasmaErrorOutOfMemory);
+        return;
+    }
+    /* one right-hand side: B is a contiguous vector, solved by the
+     * one-launch sweeps; otherwise step-by-step tile sweeps */
+    if (B.n == 1 && B.nt == 1 && B.i == 0 && B.j == 0 && B.gn == 1 &&
+        plasma_sweep_reserve(plasma, A)) {
+        plasma_cuda_trtri_blocks(plasma->stream, plasma->dstat, uplo, A, W);
+        plasma_sweep(plasma, uplo, 0, A, W, B.matrix);
+        plasma_sweep(plasma, uplo, 1, A, W, B.matrix);
         return;
     }
     plasma_cuda_trsm_sweep(plasma->stream, plasma->dstat, uplo, PlasmaNoTrans,

@@ -120,6 +120,7 @@ int plasma_finalize(void)
         if (c->scratch[i]) cudaFree(c->scratch[i]);
     for (int i = 0; i < 8; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    if (c->sweep_sync) cudaFree(c->sweep_sync);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->dstat) cudaFree(c->dstat);
     if (c->hstat) cudaFreeHost(c->hstat);
@@ -343,4 +344,41 @@ const char *plasma_strerror(int code)
         return code > 0 ? "matrix not positive definite (leading minor)"
                         : "illegal argument";
     }
+}
+
+/* Allocates the ready flags of one-launch sweeps with factor A; 0 when A's
+ * tiles admit no one-launch sweep or the allocation fails. */
+int plasma_sweep_reserve(plasma_context_t *c, plasma_desc_t A)
+{
+    int sb = plasma_cuda_trsv_block(A);
+    if (sb == 0)
+        return 0;
+    size_t need = plasma_cuda_trsv_sync_bytes((A.m + sb - 1) / sb);
+    if (need > c->sweep_sync_bytes) {
+        if (c->sweep_sync) {
+            cudaStreamSynchronize(c->stream);
+            cudaFree(c->sweep_sync);
+        }
+        c->sweep_sync = NULL;
+        c->sweep_sync_bytes = 0;
+        if (cudaMalloc(&c->sweep_sync, need) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        cudaMemsetAsync(c->sweep_sync, 0, need, c->stream);
+        c->sweep_sync_bytes = need;
+    }
+    return 1;
+}
+
+int plasma_sweep(plasma_context_t *c, plasma_enum_t uplo, int backward,
+                 plasma_desc_t A, const void *W, void *vec)
+{
+    if (!plasma_sweep_reserve(c, A))
+        return 0;
+    /* epochs are non-zero and change with every sweep */
+    if (++c->sweep_epoch <= 0)
+        c->sweep_epoch = 1;
+    return plasma_cuda_trsv(c->stream, c->dstat, uplo, backward, A, W, vec,
+                            c->sweep_sync, c->sweep_epoch, c->num_sms);
 }

@@ -35,14 +35,16 @@ typedef struct {
 
 #define PLASMA_MAX_PENDING_CALLS 4096
 #define PLASMA_NUM_STREAMS 4
-#define PLASMA_SCRATCH_SLOTS 4
+#define PLASMA_SCRATCH_SLOTS 6
 
 /* scratch slots */
 enum {
     PLASMA_SLOT_STAGING = 0,   /* column-major copies of host operands       */
     PLASMA_SLOT_WORK    = 1,   /* inverses of diagonal tiles, panels          */
     PLASMA_SLOT_SMALL   = 2,   /* norms and other vectors                     */
-    PLASMA_SLOT_MIXED   = 3    /* low-precision operand copies (dsposv)       */
+    PLASMA_SLOT_MIXED   = 3,   /* low-precision operand copies (dsposv)       */
+    PLASMA_SLOT_REFINE  = 4,   /* refinement vectors and Krylov basis         */
+    PLASMA_SLOT_SYMV    = 5    /* per-tile partial products of the residual   */
 };
 
 typedef struct {
@@ -77,6 +79,10 @@ typedef struct {
     void  *pinned;
     size_t pinned_bytes;
     cudaEvent_t ev[8];                        /* DAG edges (reused)        */
+    /* ready flags of the one-launch triangular sweeps */
+    void  *sweep_sync;
+    size_t sweep_sync_bytes;
+    int    sweep_epoch;
 } plasma_context_t;
 
 plasma_context_t *plasma_context_self(void);
@@ -189,6 +195,47 @@ void plasma_cuda_panel_set_split(int split);
 /* A(i,i) = value for i in [i0, i1) (identity padding of FP32 factors). */
 void plasma_cuda_set_diag(cudaStream_t s, plasma_desc_t A, int i0, int i1,
                           double value);
+
+/* Refinement kernels (cuda/symv.cu, trsv.cu, vec.cu). */
+size_t plasma_cuda_symv_work(plasma_desc_t A);
+int plasma_cuda_symv(cudaStream_t s, plasma_devstat_t *st, plasma_enum_t uplo,
+                     plasma_desc_t A, const double *x, const double *b,
+                     double *r, double *xnorm, double *rnorm, double *work);
+int plasma_cuda_trsv_block(plasma_desc_t A);
+size_t plasma_cuda_trsv_sync_bytes(int nblk);
+size_t plasma_cuda_trsv_w_bytes(plasma_desc_t A);
+void plasma_cuda_trtri_blocks(cudaStream_t s, plasma_devstat_t *st,
+                              plasma_enum_t uplo, plasma_desc_t A, void *W);
+int plasma_cuda_trsv(cudaStream_t s, plasma_devstat_t *st, plasma_enum_t uplo,
+                     int backward, plasma_desc_t A, const void *W, void *vec,
+                     void *sync, int epoch, int num_sms);
+size_t plasma_cuda_dots_work(int nv);
+void plasma_cuda_dots(cudaStream_t s, const double *V, size_t ldv, int nv,
+                      const double *w, size_t n, double *out, double *work);
+void plasma_cuda_sub_combo(cudaStream_t s, const double *V, size_t ldv, int nv,
+                           const double *h, double *w, size_t n);
+void plasma_cuda_axpby(cudaStream_t s, double alpha, const double *x, double *y,
+                       size_t n, int accumulate);
+void plasma_cuda_combo(cudaStream_t s, const double *V, size_t ldv, int nv,
+                       const double *c, double *y, size_t n, int accumulate);
+void plasma_cuda_d2s(cudaStream_t s, const double *x, const double *sc,
+                     float *y, size_t n, size_t npad, plasma_devstat_t *st,
+                     int call);
+void plasma_cuda_s2d(cudaStream_t s, const float *x, const double *sc,
+                     double *y, size_t n);
+/* d = 1/sqrt(diag(A)) (1 on the padding) and As <- D As D + shift I: the
+ * diagonal scaling and shift of a low-precision factor's operand. */
+void plasma_cuda_diag_rsqrt(cudaStream_t s, plasma_desc_t A, double *d,
+                            size_t n, size_t npad);
+void plasma_cuda_scale_shift(cudaStream_t s, plasma_desc_t As, int uplo,
+                             const double *d, float shift);
+void plasma_cuda_column(cudaStream_t s, plasma_desc_t D, int j, void *v,
+                        int to_vec);
+/* One-launch sweep with the context's ready-flag buffer (W from
+ * plasma_cuda_trtri_blocks); returns 0 when the factor is not eligible. */
+int plasma_sweep_reserve(plasma_context_t *plasma, plasma_desc_t A);
+int plasma_sweep(plasma_context_t *plasma, plasma_enum_t uplo, int backward,
+                 plasma_desc_t A, const void *W, void *vec);
 
 /* Host-side DAG walkers (compute/).  mode selects the trailing update of
  * FP32 factors: 0 or PlasmaFactorFP32 = FP32 arithmetic, PlasmaFactorTF32 /

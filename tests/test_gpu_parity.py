@@ -256,6 +256,22 @@ def test_dsposv_fallback(L):
     assert solve_residual(a, x, b) < TOL * EPS
 
 
+@pytest.mark.parametrize("n,nb", [(1000, 192), (700, 96)])
+def test_dsposv_sweep_block_sizes(L, n, nb):
+    """Refinement sweeps with 64-row blocks (nb = 192) and the tile-sweep
+    fallback (nb = 96) converge to the FP64 answer."""
+    set_nb(L, nb)
+    a = gen.spectrum(n, 1e3, seed=1300 + n)
+    b = np.asfortranarray(np.random.default_rng(n).standard_normal((n, 1)))
+    x = np.zeros((n, 1), order="F")
+    it = ctypes.c_int(0)
+    assert L.plasma_dsposv(LO, n, 1, np.asfortranarray(a.copy()).ctypes.data, n,
+                           np.asfortranarray(b.copy()).ctypes.data, n,
+                           x.ctypes.data, n, ctypes.byref(it)) == 0
+    assert it.value >= 0
+    assert solve_residual(a, x, b) < TOL * EPS
+
+
 def test_dsposv_nonspd(L):
     """Not positive definite: the FP64 path reports LAPACK's info."""
     set_nb(L, 64)
@@ -407,3 +423,50 @@ def test_low_precision_factor_backward_error(L, mode, bound, n, nb):
         assert berr < bound, berr
     finally:
         L.plasma_set(pb.PlasmaMixedPrecisionMode, pb.PlasmaFactorFP32)
+
+
+@pytest.mark.parametrize("mode", [pb.PlasmaFactorTF32, pb.PlasmaFactorBF16])
+@pytest.mark.parametrize("refine", [pb.PlasmaRefineGMRES, pb.PlasmaRefineAuto])
+def test_gmres_ir_ill_conditioned(L, mode, refine):
+    """kappa = 1e5: classical IR with a TF32/BF16 factor stalls; GMRES-IR
+    preconditioned by the same factor reaches the FP64 stopping rule."""
+    set_nb(L, 256)
+    L.plasma_set(pb.PlasmaMixedPrecisionMode, mode)
+    L.plasma_set(pb.PlasmaRefinement, refine)
+    try:
+        n, kappa = 1536, 1e5
+        a = gen.spectrum(n, kappa, seed=11)
+        xt = np.random.default_rng(12).standard_normal((n, 1))
+        b = np.asfortranarray(a @ xt)
+        rc, it, x, info = dsposv_ex(L, LO, a, b)
+        assert rc == 0
+        assert it >= 0, "fell back to FP64"
+        assert info.refinement == pb.PlasmaRefineGMRES
+        assert info.gmres_iterations > 0
+        assert solve_residual(a, x, b) < TOL * EPS
+        assert np.abs(x - xt).max() / np.abs(xt).max() < kappa * 1e-14
+    finally:
+        L.plasma_set(pb.PlasmaMixedPrecisionMode, pb.PlasmaFactorFP32)
+        L.plasma_set(pb.PlasmaRefinement, pb.PlasmaRefineIR)
+
+
+@pytest.mark.parametrize("uplo", [LO, UP])
+@pytest.mark.parametrize("n,nb", [(1000, 128), (777, 256), (64, 64), (1000, 192),
+                                  (500, 96), (4100, 512)])
+def test_single_rhs_sweeps(L, uplo, n, nb):
+    """nrhs = 1 uses the one-launch block sweeps (ticketed row blocks with
+    ready flags) when nb is a multiple of 64 and the tile sweeps otherwise
+    (nb = 96); compare with the oracle."""
+    set_nb(L, nb)
+    a, b = gen.diag_dominant(n, 1, seed=1100 + n)
+    x = np.asfortranarray(b.copy())
+    assert L.plasma_dposv(uplo, n, 1, np.asfortranarray(a.copy()).ctypes.data, n,
+                          x.ctypes.data, n) == 0
+    xo = np.asfortranarray(b.copy())
+    assert oracle.posv(uplo, np.asfortranarray(a.copy()), xo, nb) == 0
+    np.testing.assert_allclose(x, xo, rtol=1e-12, atol=1e-15)
+    # FP32
+    a32 = np.asfortranarray(a.astype(np.float32))
+    x32 = np.asfortranarray(b.astype(np.float32))
+    assert L.plasma_sposv(uplo, n, 1, a32.ctypes.data, n, x32.ctypes.data, n) == 0
+    assert solve_residual(a, x32.astype(np.float64), b) < TOL * SEPS
