@@ -73,6 +73,25 @@ void plasma_profile_enable(int on);
 int plasma_profile_query(int kclass, long long *launches, double *ms,
                          double *flops, double *bytes);
 
+/*
+ * No reference counterpart.  plasma_omp_dpotrs for one right-hand side
+ * (A: FP64 Cholesky factor in square tiles, nb a multiple of 64; B: n x 1)
+ * that takes no device memory from the library: its scratch (the inverses
+ * of the 64 x 64 diagonal blocks and the sweep ready flags) is a file-scope
+ * device array of 4 MiB + 4 KiB, so n <= PLASMA_NOALLOC_MAX_N.  Larger n
+ * fails the request with PlasmaErrorIllegalValue, other shapes with
+ * PlasmaErrorNotSupported.  The first call on a device looks the array's
+ * address up (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls share the one array: calls that overlap (other
+ * streams, other host threads) race, and the array keeps the last call's
+ * contents (each sweep clears its own ticket and abort words; the flags are
+ * matched against a per-call epoch, not against zero).
+ */
+#define PLASMA_NOALLOC_MAX_N 8192
+void plasma_omp_dpotrs_noalloc(plasma_enum_t uplo, plasma_desc_t A,
+                               plasma_desc_t B, plasma_sequence_t *sequence,
+                               plasma_request_t *request);
+
 /* Human-readable name of a return code. */
 const char *plasma_strerror(int code);
 

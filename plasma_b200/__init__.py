@@ -118,6 +118,7 @@ _SIGNATURES = [
     ("plasma_omp_dpotrf", None, [c_int, _DESC, _SEQ, _REQ]),
     ("plasma_omp_spotrf", None, [c_int, _DESC, _SEQ, _REQ]),
     ("plasma_omp_dpotrs", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
+    ("plasma_omp_dpotrs_noalloc", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
     ("plasma_omp_spotrs", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
     ("plasma_omp_dposv", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
     ("plasma_omp_sposv", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
