@@ -76,7 +76,10 @@ int plasma_profile_query(int kclass, long long *launches, double *ms,
 /*
  * No reference counterpart.  plasma_omp_dpotrs for one right-hand side
  * (A: FP64 Cholesky factor in square tiles, nb a multiple of 64; B: n x 1)
- * that takes no device memory from the library: its scratch (the inverses
+ * for callers that cannot allocate device memory while they solve (device
+ * memory owned by another allocator, or a latency-bound loop where
+ * cudaMalloc/cudaFree would synchronise the device).  It takes no device
+ * memory from the library: its scratch (the inverses
  * of the 64 x 64 diagonal blocks and the sweep ready flags) is a file-scope
  * device array of 4 MiB + 4 KiB, so n <= PLASMA_NOALLOC_MAX_N.  Larger n
  * fails the request with PlasmaErrorIllegalValue, other shapes with

@@ -4,6 +4,14 @@
 // allocates.  No reference counterpart; the computation is that of
 // plasma_omp_dpotrs for one right-hand side.
 //
+// It serves callers that must not allocate device memory during a solve:
+// a process whose device memory is already handed out to another allocator
+// (a framework's caching pool that holds nearly all of HBM, a service with a
+// fixed, pre-planned footprint), and a latency-bound solve loop, where
+// cudaMalloc/cudaFree would synchronise the device and stall the work of
+// other streams.  The library's plain potrs grows its workspace with
+// cudaMalloc on first use at a new size; this entry point never does.
+//
 // Scratch: the inverses of the 64 x 64 diagonal blocks of the factor
 // (64 * 64 doubles per block, PLASMA_NOALLOC_MAX_N / 64 blocks = 4 MiB) and
 // the sweep's ticket, abort word and per-block ready flags (4 KiB).  The
@@ -112,8 +120,14 @@ extern "C" void plasma_omp_dpotrs_noalloc(plasma_enum_t uplo, plasma_desc_t A,
 
     const int dev = plasma->device;
     if (g_scratch_addr[dev] == NULL) {
+        // the array's host-side name is not a device address: look the
+        // address up once per device, with that device current
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (cur != dev) cudaSetDevice(dev);
         double *p = NULL;
         cudaError_t rc = cudaGetSymbolAddress((void **)&p, g_potrs_scratch);
+        if (cur != dev && cur >= 0) cudaSetDevice(cur);
         if (rc != cudaSuccess || p == NULL) {
             cudaGetLastError();
             plasma_error("plasma_omp_dpotrs_noalloc: cudaGetSymbolAddress of "

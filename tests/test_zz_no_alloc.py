@@ -1,6 +1,9 @@
 """plasma_omp_dpotrs_noalloc (no reference counterpart): the single
-right-hand-side FP64 potrs whose scratch is a static device array, checked
-against plasma_omp_dpotrs on the same factor, on two calls in a row.
+right-hand-side FP64 potrs for callers that cannot allocate device memory
+while they solve (memory owned by another allocator, or a latency-bound loop
+that must not synchronise the device through cudaMalloc).  Its scratch is a
+static device array; it is checked against plasma_omp_dpotrs on the same
+factor, on two calls in a row.
 Collected last: the static array must hold no state that a later call
 depends on, whatever ran before."""
 import ctypes
