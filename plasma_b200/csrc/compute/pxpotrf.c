@@ -32,14 +32,16 @@ typedef struct {
     plasma_enum_t uplo;
     plasma_desc_t A;
     int sms;
-    int mode;          /* PlasmaFactorTF32 / BF16 on the tensor cores, else 0 */
+    int mode;          /* PLASMA_TC_* product precision of the tensor-core
+                          update, or 0 for the DMMA/SIMT update            */
     char *panel[2];    /* rounded copies of panels k (alternating buffers)   */
 } walk_t;
 
 static void update(walk_t *w, cudaStream_t s, int k, int nlo, int nhi)
 {
     if (w->mode) {
-        if (plasma_cuda_update_tc(s, w->st, w->mode, w->A, k, nlo, nhi, w->panel[k & 1]))
+        if (plasma_cuda_update_tc(s, w->st, w->mode, w->A, k, nlo, nhi,
+                                  w->panel[k & 1], w->sms))
             return;
     }
     plasma_cuda_update(s, w->st, w->uplo, w->A, k, nlo, nhi, w->sms);
@@ -71,14 +73,16 @@ void plasma_pXpotrf_mode(plasma_context_t *plasma, plasma_enum_t uplo,
     w.sms = plasma->num_sms;
     w.mode = 0;
     w.panel[0] = w.panel[1] = NULL;
-    if ((mode == PlasmaFactorTF32 || mode == PlasmaFactorBF16) &&
-        plasma_cuda_update_tc_ok(A, uplo)) {
-        size_t esz = mode == PlasmaFactorBF16 ? 2 : 4;
-        size_t one = ((size_t)A.mt * A.mb * A.mb * esz + 1023) & ~(size_t)1023;
+    /* FP32 factors: every mode runs its update on the tensor cores when the
+     * tiles allow it (FP32 as the three-product TF32 split) */
+    int tc = mode == PlasmaFactorTF32 ? PLASMA_TC_TF32
+           : mode == PlasmaFactorBF16 ? PLASMA_TC_BF16 : PLASMA_TC_TF32X3;
+    if (plasma_cuda_update_tc_ok(A, uplo)) {
+        size_t one = (plasma_cuda_panel_bytes(tc, A) + 1023) & ~(size_t)1023;
         char *buf = (char *)plasma_scratch(plasma, PLASMA_SLOT_MIXED, 2 * one + 1024);
         if (buf != NULL) {
             buf = (char *)(((uintptr_t)buf + 1023) & ~(uintptr_t)1023);
-            w.mode = mode;
+            w.mode = tc;
             w.panel[0] = buf;
             w.panel[1] = buf + one;
         }
@@ -86,7 +90,8 @@ void plasma_pXpotrf_mode(plasma_context_t *plasma, plasma_enum_t uplo,
     /* FP32 panels: TF32 products next to a TF32/BF16 update, else the
      * FP32-accurate split */
     if (A.precision == PlasmaRealFloat)
-        plasma_cuda_panel_set_split(w.mode ? 1 : 3);
+        plasma_cuda_panel_set_split(w.mode == PLASMA_TC_TF32 ||
+                                    w.mode == PLASMA_TC_BF16 ? 1 : 3);
 
     if (plasma->lookahead == 0 || mt < 3) {
         for (int k = 0; k < mt; k++) {

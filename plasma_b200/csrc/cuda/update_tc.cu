@@ -1,27 +1,40 @@
-// update_tc.cu -- trailing update of the low-precision Cholesky on the
-// fifth-generation tensor cores (tcgen05, accumulators in tensor memory).
+// update_tc.cu -- trailing update of the FP32 Cholesky on the fifth-
+// generation tensor cores (tcgen05, accumulators in tensor memory).
 //
-//     C(m,n) -= A(m,k) * A(n,k)^T     C in FP32, operands TF32 or BF16
+//     C(m,n) -= A(m,k) * A(n,k)^T     C in FP32
 //
 // This is the SYRK/GEMM part of plasma_pspotrf (the FP32 tile Cholesky that
 // the reference runs inside dsposv, compute/zcposv.c:452 ->
-// compute/pzpotrf.c:57-77) with the products formed at reduced precision and
-// accumulated in FP32.
+// compute/pzpotrf.c:57-77).  Three product precisions, all accumulated in
+// FP32 in tensor memory:
+//   TF32   : one kind::tf32 MMA per k-step on the TF32-rounded panel;
+//   BF16   : one kind::f16 MMA per k-step on the BF16-rounded panel;
+//   TF32X3 : the panel split as a = hi + lo (hi = tf32(a), lo = tf32(a - hi))
+//            and a*b formed as lo*hi + hi*lo + hi*hi, three kind::tf32 MMAs,
+//            which keeps about 22 bits of every product (the FP32 factor).
 //
-// One CTA computes a 128 x nb block (nb = 256 or 128) of one output tile:
-//   warp 0     : TMA producer -- 3-D tensor maps over the column-major tiles
-//                of the rounded panel copy (128-byte swizzle; 32-byte swizzle
-//                atoms for TF32, the only MN-major TF32 layout), two-stage
-//                ring of 48 KB stages, plus an L2 prefetch of the C block;
-//   warp 1     : MMA issuer -- one thread issues tcgen05.mma (M = 128,
-//                N = nb, MN-major A and B straight from the column-major
-//                tiles), tcgen05.commit frees a stage / signals the end;
-//   warps 2-9  : epilogue -- tcgen05.ld of the accumulator, C -= P on FP32
-//                tiles in global memory (coalesced along rows), masking the
-//                strict upper triangle of diagonal tiles.
-// Two CTAs share an SM, so one CTA's HBM-bound epilogue overlaps the other's
-// MMAs.  Every mbarrier wait is bounded (about a second); on expiry the CTA
-// records PlasmaErrorInternal, drains what it issued and frees its TMEM.
+// One CTA owns a run of `ipc` consecutive work items (a 128 x nb block of one
+// output tile each; items of one tile column are adjacent, so they share the
+// B operand in L2):
+//   warp 0     : TMA producer -- 4-D tensor maps over the column-major panel
+//                tiles (128-byte swizzle; 32-byte swizzle atoms for TF32, the
+//                only MN-major TF32 layout), a 3-stage ring of 48 KB stages;
+//   warp 1     : MMA issuer -- one thread issues tcgen05.mma (M = 128, N = nb,
+//                MN-major A and B), tcgen05.commit frees a stage and, after
+//                the last k-step of an item, publishes its accumulator;
+//   warp 2     : tensor-memory allocation (two accumulators of nb columns);
+//   warps 4-11 : epilogue -- tcgen05.ld of an accumulator, -P staged in
+//                shared memory in 32 x 32 blocks (zero above the diagonal of
+//                diagonal tiles) and added to C by TMA reductions
+//                (cp.reduce.async.bulk.tensor .add.f32): the read-modify-write
+//                of C runs in the memory system, asynchronously, one add per
+//                element, so the result is deterministic; then the
+//                accumulator is handed back to the MMA warp.
+// With two accumulators the epilogue of item j overlaps the MMAs of item j+1.
+// CTAs stay short (a few items) so that the kernels of the critical panel
+// stream find free SMs while a large update runs.  Every mbarrier wait is
+// bounded (about 2 s); on expiry the CTA records PlasmaErrorInternal, lets
+// what it issued drain and frees its tensor memory.
 #include "common.cuh"
 
 #include <cuda.h>
@@ -31,13 +44,31 @@
 namespace {
 
 constexpr int TC_M = 128;
-constexpr int TC_THREADS = 320;          // 10 warps
+constexpr int TC_THREADS = 384;          // 12 warps
+constexpr int TC_EPI_WARP0 = 4;
 constexpr int TC_EPI_WARPS = 8;
 constexpr int TC_STAGE_BYTES = 48 * 1024;
-constexpr int TC_STAGES = 2;
-constexpr int TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024 + 256;
+constexpr int TC_STAGES = 3;
+constexpr int TC_EPI_BUFS = 2;           // staging buffers per epilogue warp
+constexpr int TC_EPI_BUF_BYTES = 32 * 32 * 4;
+constexpr int TC_SMEM = TC_STAGES * TC_STAGE_BYTES +
+                        TC_EPI_WARPS * TC_EPI_BUFS * TC_EPI_BUF_BYTES + 1024;
 
-enum { MODE_TF32 = 1, MODE_BF16 = 2 };
+enum { MODE_TF32 = PLASMA_TC_TF32, MODE_BF16 = PLASMA_TC_BF16,
+       MODE_TF32X3 = PLASMA_TC_TF32X3 };
+
+template <int MODE>
+struct Geo {
+    static constexpr int ESZ = MODE == MODE_BF16 ? 2 : 4;
+    static constexpr int MNBOX = 128 / ESZ;           // elements per 128-byte row
+    static constexpr int BK = MODE == MODE_BF16 ? 64 : (MODE == MODE_TF32 ? 32 : 16);
+    static constexpr int KI = MODE == MODE_BF16 ? 16 : 8;   // K per instruction
+    static constexpr int PARTS = MODE == MODE_TF32X3 ? 2 : 1;
+    static constexpr uint32_t LAYOUT = MODE == MODE_BF16 ? 2u : 1u;
+    static constexpr uint32_t SBO = MODE == MODE_BF16 ? 1024u : 512u;
+    static constexpr int CHUNK = BK * 128;            // one MN chunk of a stage
+    static constexpr int A_BYTES = (TC_M / MNBOX) * CHUNK;
+};
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar, int count)
 {
@@ -66,7 +97,7 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-// Bounded wait: false after ~1 s (or at once when the CTA already gave up).
+// Bounded wait: false after ~2 s (or at once when the CTA already gave up).
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity,
                                           volatile int *abort_flag)
 {
@@ -81,14 +112,42 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity,
     return true;
 }
 
-__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map,
-                                            uint64_t *bar, int c0, int c1, int c2)
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map,
+                                            uint64_t *bar, int c0, int c1, int c2,
+                                            int c3)
 {
     asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cta.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%3, %4, %5}], [%2];"
-        :: "r"(smem_u32(dst)), "l"(map), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+        "cp.async.bulk.tensor.4d.shared::cta.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5, %6}], [%2];"
+        :: "r"(smem_u32(dst)), "l"(map), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2),
+           "r"(c3)
         : "memory");
+}
+
+// C(tile)[y .. y+31, x .. x+31] += staged 32 x 32 block (column-major)
+__device__ __forceinline__ void tma_reduce_add_3d(const CUtensorMap *map, const void *src,
+                                                  int c0, int c1, int c2)
+{
+    asm volatile(
+        "cp.reduce.async.bulk.tensor.3d.global.shared::cta.add.tile.bulk_group"
+        " [%0, {%2, %3, %4}], [%1];"
+        :: "l"(map), "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2) : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit()
+{
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void bulk_wait_read()
+{
+    asm volatile("cp.async.bulk.wait_group.read %0;" :: "n"(N) : "memory");
+}
+
+__device__ __forceinline__ void bulk_wait_all()
+{
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 
 // Shared-memory matrix descriptor of an MN-major operand.  BF16 uses the
@@ -110,7 +169,7 @@ __device__ __forceinline__ uint64_t smem_desc(const void *p, uint32_t lbo, uint3
 
 __device__ __forceinline__ uint32_t instr_desc(int mode, int n)
 {
-    uint32_t fmt = mode == MODE_TF32 ? 2u : 1u;   // TF32 : BF16
+    uint32_t fmt = mode == MODE_BF16 ? 1u : 2u;   // BF16 : TF32
     return (1u << 4)                 // D format F32
          | (fmt << 7) | (fmt << 10)  // A, B format
          | (1u << 15) | (1u << 16)   // A, B MN-major
@@ -123,7 +182,7 @@ __device__ __forceinline__ void mma(uint32_t tmem, uint64_t a, uint64_t b,
                                     uint32_t idesc, uint32_t acc)
 {
     const uint32_t z = 0;      // no output lane disabled
-    if (MODE == MODE_TF32)
+    if (MODE != MODE_BF16)
         asm volatile(
             "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
             "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
@@ -161,65 +220,67 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
 }
 
 struct TcArgs {
-    plasma_desc_t A;    // FP32 general descriptor holding C (and TF32 operands)
+    plasma_desc_t A;    // FP32 general or packed-lower descriptor holding C
     int k, nlo, nhi;
-    int op_base;        // tile index of panel tile 0 in the operand map
-    int op_stride;      // tile-index step per tile row in the operand map
+    int mt;             // tiles per part in the operand map (lo part at +mt)
+    long long nitems;
+    int ipc;            // items per CTA
 };
 
-// work item -> (m, n, si); false when the item lies strictly above the
-// diagonal of a diagonal tile
-__device__ __forceinline__ bool tc_item(const TcArgs &g, int w, int &m, int &n, int &si)
+// work item -> (m, n, si); items run over si fastest, then m, then n
+__device__ __forceinline__ void tc_item(const TcArgs &g, long long w, int &m, int &n,
+                                        int &si)
 {
     const int sb = g.A.mb / TC_M;
-    int p = w / sb;
-    si = w - p * sb;
+    long long p = w / sb;
+    si = (int)(w - p * sb);
     n = g.nlo;
-    while (n < g.nhi && p >= g.A.mt - n) { p -= g.A.mt - n; n++; }
-    if (n >= g.nhi) return false;
-    m = n + p;
-    return true;
+    while (n < g.nhi - 1 && p >= g.A.mt - n) { p -= g.A.mt - n; n++; }
+    m = n + (int)p;
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(TC_THREADS, 2)
-k_update_tc(const __grid_constant__ CUtensorMap opmap, TcArgs g,
+__global__ void __launch_bounds__(TC_THREADS, 1)
+k_update_tc(const __grid_constant__ CUtensorMap opmap,
+            const __grid_constant__ CUtensorMap cmap, TcArgs g,
             plasma_devstat_t *st)
 {
+    using G = Geo<MODE>;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    __shared__ uint64_t full_bar[TC_STAGES], empty_bar[TC_STAGES], acc_bar;
+    __shared__ uint64_t full_bar[TC_STAGES], empty_bar[TC_STAGES];
+    __shared__ uint64_t tfull_bar[2], tempty_bar[2];
     __shared__ uint32_t tmem_base_s;
     __shared__ volatile int abort_s;
 
     if (plasma_failed(st)) return;
-    int m, n, si;
-    if (!tc_item(g, blockIdx.x, m, n, si)) return;
+    const long long first = (long long)blockIdx.x * g.ipc;
+    if (first >= g.nitems) return;
+    const int nit = (int)min((long long)g.ipc, g.nitems - first);
 
     const int nb = g.A.mb;                         // N of the MMA
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    unsigned char *stage_base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    // element geometry
-    constexpr int ESZ = MODE == MODE_TF32 ? 4 : 2;
-    constexpr int MNBOX = 128 / ESZ;              // elements per 128-byte row
-    constexpr int BK = MODE == MODE_TF32 ? 32 : 64;
-    constexpr int KI = MODE == MODE_TF32 ? 8 : 16; // K per instruction
-    const int chunk_bytes = BK * 128;             // one MN chunk of a stage
-    const int a_bytes = (TC_M / MNBOX) * chunk_bytes;
-    const int stage_bytes = a_bytes + (nb / MNBOX) * chunk_bytes;
-    const int nkb = g.A.nb / BK;                  // K = nb
+    unsigned char *stage_base =
+        (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    const int b_bytes = (nb / G::MNBOX) * G::CHUNK;
+    const int stage_bytes = G::PARTS * (G::A_BYTES + b_bytes);
+    const int nkb = nb / G::BK;                    // K = nb
+    const uint32_t tmem_cols = 2 * nb;
 
     if (tid == 0) {
         for (int s = 0; s < TC_STAGES; s++) {
             mbar_init(&full_bar[s], 1);
             mbar_init(&empty_bar[s], 1);
         }
-        mbar_init(&acc_bar, 1);
+        for (int a = 0; a < 2; a++) {
+            mbar_init(&tfull_bar[a], 1);
+            mbar_init(&tempty_bar[a], TC_EPI_WARPS);
+        }
         abort_s = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) {
+    if (warp == 2) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                     :: "r"(smem_u32(&tmem_base_s)), "r"(256));
+                     :: "r"(smem_u32(&tmem_base_s)), "r"(tmem_cols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -227,90 +288,130 @@ k_update_tc(const __grid_constant__ CUtensorMap opmap, TcArgs g,
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base_s;
 
-    float *C = (float *)plasma_tile_addr(g.A, m, n);
-    const int ldc = plasma_tile_mmain(g.A, m);
-    const int i0 = si * TC_M;
-
     if (warp == 0 && lane == 0) {
         // ---------------- producer
-        // warm L2 with the C block: nb columns of 128 rows (512 bytes each)
-        for (int j = 0; j < nb; j++)
-            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
-                         :: "l"(C + (size_t)j * ldc + i0), "r"(TC_M * 4) : "memory");
-        const int ta = g.op_base + m * g.op_stride;   // operand tile of A(m,k)
-        const int tb = g.op_base + n * g.op_stride;   // operand tile of A(n,k)
-        for (int kb = 0; kb < nkb; kb++) {
-            int s = kb % TC_STAGES;
-            if (kb >= TC_STAGES &&
-                !mbar_wait(&empty_bar[s], ((kb / TC_STAGES) - 1) & 1, &abort_s))
-                break;
-            unsigned char *sa = stage_base + s * TC_STAGE_BYTES;
-            unsigned char *sbp = sa + a_bytes;
-            mbar_expect_tx(&full_bar[s], (uint32_t)stage_bytes);
-            for (int c = 0; c < TC_M / MNBOX; c++)
-                tma_load_3d(sa + c * chunk_bytes, &opmap, &full_bar[s],
-                            i0 + c * MNBOX, kb * BK, ta);
-            for (int c = 0; c < nb / MNBOX; c++)
-                tma_load_3d(sbp + c * chunk_bytes, &opmap, &full_bar[s],
-                            c * MNBOX, kb * BK, tb);
+        int it = 0;                                   // k-blocks issued so far
+        bool ok = true;
+        for (int j = 0; j < nit && ok; j++) {
+            int m, n, si;
+            tc_item(g, first + j, m, n, si);
+            const int i0 = si * TC_M;
+            for (int kb = 0; kb < nkb; kb++, it++) {
+                const int s = it % TC_STAGES;
+                if (it >= TC_STAGES &&
+                    !mbar_wait(&empty_bar[s], ((it / TC_STAGES) - 1) & 1, &abort_s)) {
+                    ok = false;
+                    break;
+                }
+                unsigned char *sp = stage_base + s * TC_STAGE_BYTES;
+                mbar_expect_tx(&full_bar[s], (uint32_t)stage_bytes);
+#pragma unroll
+                for (int p = 0; p < G::PARTS; p++) {
+                    unsigned char *sa = sp + p * G::A_BYTES;
+                    unsigned char *sb = sp + G::PARTS * G::A_BYTES + p * b_bytes;
+                    const int toff = p * g.mt;
+                    tma_load_4d(sa, &opmap, &full_bar[s], 0, kb * G::BK,
+                                i0 / G::MNBOX, m + toff);
+                    for (int c = 0; c < nb / TC_M; c++)
+                        tma_load_4d(sb + c * G::A_BYTES, &opmap, &full_bar[s], 0,
+                                    kb * G::BK, c * (TC_M / G::MNBOX), n + toff);
+                }
+            }
         }
     } else if (warp == 1 && lane == 0) {
         // ---------------- MMA issuer
         const uint32_t idesc = instr_desc(MODE, nb);
+        int it = 0;
         bool ok = true;
-        for (int kb = 0; kb < nkb && ok; kb++) {
-            int s = kb % TC_STAGES;
-            if (!mbar_wait(&full_bar[s], (kb / TC_STAGES) & 1, &abort_s)) {
-                ok = false;
+        for (int j = 0; j < nit && ok; j++) {
+            const int a = j & 1;
+            if (j >= 2 && !mbar_wait(&tempty_bar[a], ((j >> 1) - 1) & 1, &abort_s))
                 break;
-            }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            unsigned char *sa = stage_base + s * TC_STAGE_BYTES;
-            unsigned char *sbp = sa + a_bytes;
+            const uint32_t acc_t = tmem + (uint32_t)(a * nb);
+            for (int kb = 0; kb < nkb; kb++, it++) {
+                const int s = it % TC_STAGES;
+                if (!mbar_wait(&full_bar[s], (it / TC_STAGES) & 1, &abort_s)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                unsigned char *sp = stage_base + s * TC_STAGE_BYTES;
+                unsigned char *sa_hi = sp;
+                unsigned char *sb_hi = sp + G::PARTS * G::A_BYTES;
 #pragma unroll
-            for (int kk = 0; kk < BK / KI; kk++) {
-                constexpr uint32_t LAYOUT = MODE == MODE_TF32 ? 1u : 2u;
-                constexpr uint32_t SBO = MODE == MODE_TF32 ? 512u : 1024u;
-                uint64_t da = smem_desc(sa + kk * KI * 128, chunk_bytes, SBO, LAYOUT);
-                uint64_t db = smem_desc(sbp + kk * KI * 128, chunk_bytes, SBO, LAYOUT);
-                mma<MODE>(tmem, da, db, idesc, (kb | kk) != 0);
-            }
-            mma_commit(&empty_bar[s]);
-        }
-        mma_commit(&acc_bar);
-    } else if (warp >= 2) {
-        // ---------------- epilogue: warp -> TMEM lane quarter and column half
-        const int e = warp - 2;
-        const int q = warp & 3;                  // lanes 32q .. 32q+31
-        const int half = e / 4;                  // columns [half*nb/2, ...)
-        const bool ok = __all_sync(0xffffffffu, mbar_wait(&acc_bar, 0, &abort_s));
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        if (ok) {
-            const int row = i0 + 32 * q + lane;
-            const int rows = plasma_tile_mview(g.A, m);
-            const int cols = plasma_tile_mview(g.A, n);
-            const bool diag = m == n;
-            const int c0 = half * (nb / 2);
-            for (int cc = c0; cc < c0 + nb / 2; cc += 32) {
-                float v[32];
-                tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)cc, v);
-                if (row < rows) {
-                    float cv[32];
-#pragma unroll
-                    for (int j = 0; j < 32; j++) {
-                        int col = cc + j;
-                        cv[j] = (col < cols && (!diag || row >= col))
-                                    ? C[(size_t)col * ldc + row] : 0.f;
-                    }
-#pragma unroll
-                    for (int j = 0; j < 32; j++) {
-                        int col = cc + j;
-                        if (col < cols && (!diag || row >= col))
-                            C[(size_t)col * ldc + row] = cv[j] - v[j];
+                for (int kk = 0; kk < G::BK / G::KI; kk++) {
+                    const uint32_t acc_on = (kb | kk) != 0;
+                    uint64_t da = smem_desc(sa_hi + kk * G::KI * 128, G::CHUNK, G::SBO,
+                                            G::LAYOUT);
+                    uint64_t db = smem_desc(sb_hi + kk * G::KI * 128, G::CHUNK, G::SBO,
+                                            G::LAYOUT);
+                    if (MODE == MODE_TF32X3) {
+                        unsigned char *sa_lo = sp + G::A_BYTES;
+                        unsigned char *sb_lo = sb_hi + b_bytes;
+                        uint64_t dal = smem_desc(sa_lo + kk * G::KI * 128, G::CHUNK, G::SBO,
+                                                 G::LAYOUT);
+                        uint64_t dbl = smem_desc(sb_lo + kk * G::KI * 128, G::CHUNK, G::SBO,
+                                                 G::LAYOUT);
+                        // small terms first
+                        mma<MODE>(acc_t, dal, db, idesc, acc_on);
+                        mma<MODE>(acc_t, da, dbl, idesc, 1u);
+                        mma<MODE>(acc_t, da, db, idesc, 1u);
+                    } else {
+                        mma<MODE>(acc_t, da, db, idesc, acc_on);
                     }
                 }
+                mma_commit(&empty_bar[s]);
             }
+            if (ok) mma_commit(&tfull_bar[a]);
         }
+    } else if (warp >= TC_EPI_WARP0) {
+        // ---------------- epilogue: warp -> TMEM lane quarter and column half
+        const int e = warp - TC_EPI_WARP0;
+        const int q = warp & 3;                  // lanes 32q .. 32q+31
+        const int half = e / 4;                  // columns [half*nb/2, ...)
+        float *stage_epi = (float *)(stage_base + TC_STAGES * TC_STAGE_BYTES) +
+                           (size_t)e * TC_EPI_BUFS * (TC_EPI_BUF_BYTES / 4);
+        int nchunk = 0;
+        for (int j = 0; j < nit; j++) {
+            const int a = j & 1;
+            const bool ok = __all_sync(0xffffffffu,
+                                       mbar_wait(&tfull_bar[a], (j >> 1) & 1, &abort_s));
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            int m, n, si;
+            tc_item(g, first + j, m, n, si);
+            const int tile = (int)(((const char *)plasma_tile_addr(g.A, m, n) -
+                                    (const char *)g.A.matrix) / ((size_t)nb * nb * 4));
+            const int r0 = si * TC_M + 32 * q;   // first row of this warp
+            const int row = r0 + lane;
+            const bool diag = m == n;
+            const int c0 = half * (nb / 2);
+            for (int cc = c0; cc < c0 + nb / 2; cc += 32, nchunk++) {
+                float v[32];
+                tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(a * nb + cc), v);
+                float *buf = stage_epi + (nchunk % TC_EPI_BUFS) * (TC_EPI_BUF_BYTES / 4);
+                // the reduction that last read this buffer must be done with it
+                if (nchunk >= TC_EPI_BUFS && lane == 0) bulk_wait_read<TC_EPI_BUFS - 1>();
+                __syncwarp();
+#pragma unroll
+                for (int jj = 0; jj < 32; jj++) {
+                    const int col = cc + jj;
+                    buf[jj * 32 + lane] = (!diag || row >= col) ? -v[jj] : 0.f;
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) {
+                    tma_reduce_add_3d(&cmap, buf, r0, cc, tile);
+                    bulk_commit();
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty_bar[a]);
+        }
+        if (lane == 0) bulk_wait_all();
+        __syncwarp();
     }
     // ---------------- teardown
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -318,34 +419,25 @@ k_update_tc(const __grid_constant__ CUtensorMap opmap, TcArgs g,
     if (abort_s) {
         if (tid == 0) {
             plasma_fail(st, PlasmaErrorInternal, 0);
-            // Give the MMAs (the accumulator barrier) and the TMA copies that
-            // were issued a bounded time to land before TMEM and shared
-            // memory are released.
+            // Give the MMAs and the TMA copies that were issued a bounded time
+            // to land before tensor and shared memory are released.
             long long t0 = clock64();
-            while (!mbar_try(&acc_bar, 0) && clock64() - t0 < 400000000LL) {}
-            t0 = clock64();
-            while (clock64() - t0 < 100000000LL) {}
+            while (clock64() - t0 < 200000000LL) {}
         }
         __syncthreads();
     }
-    if (warp == 0) {
+    if (warp == 2) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
-                     :: "r"(tmem), "r"(256));
+                     :: "r"(tmem), "r"(tmem_cols));
     }
 }
 
 // ---------------------------------------------------------------------------
-// host side: tensor maps over column-major tile arrays
+// host side
 // ---------------------------------------------------------------------------
-bool encode_tile_map(CUtensorMap *map, void *base, CUtensorMapDataType dt,
-                     int esz, int nb, long long ntiles, int box_mn, int box_k,
-                     CUtensorMapSwizzle swz)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 {
-    cuuint64_t dims[3] = {(cuuint64_t)nb, (cuuint64_t)nb, (cuuint64_t)ntiles};
-    cuuint64_t strides[2] = {(cuuint64_t)nb * esz, (cuuint64_t)nb * nb * esz};
-    cuuint32_t box[3] = {(cuuint32_t)box_mn, (cuuint32_t)box_k, 1};
-    cuuint32_t estr[3] = {1, 1, 1};
     // resolved through the runtime so that the library does not link the
     // driver library directly (it must load on machines without a GPU)
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
@@ -353,23 +445,71 @@ bool encode_tile_map(CUtensorMap *map, void *base, CUtensorMapDataType dt,
         cudaDriverEntryPointQueryResult q;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void **)&encode,
                                     cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess) {
+            q != cudaDriverEntryPointSuccess)
             encode = nullptr;
-            return false;
-        }
     }
-    CUresult r = encode(map, dt, 3, base, dims, strides, box, estr,
-                                        CU_TENSOR_MAP_INTERLEAVE_NONE,
-                                        swz,
-                                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return encode;
+}
+
+// Operand map: 4-D over the column-major panel tiles
+//   dim 0: 128 bytes of a column (MN inner), dim 1: K (columns, stride nb),
+//   dim 2: 128-byte MN chunks (stride 128 bytes), dim 3: tiles
+// so one box {128 B, BK, 128 rows / chunk, 1} lands as consecutive MN chunks
+// of BK x 128 bytes, the layout the MMA descriptors describe.
+bool encode_tile_map(CUtensorMap *map, void *base, CUtensorMapDataType dt,
+                     int esz, int nb, long long ntiles, int bk, CUtensorMapSwizzle swz)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+    if (encode == nullptr) return false;
+    const int mnbox = 128 / esz;
+    cuuint64_t dims[4] = {(cuuint64_t)mnbox, (cuuint64_t)nb, (cuuint64_t)(nb / mnbox),
+                          (cuuint64_t)ntiles};
+    cuuint64_t strides[3] = {(cuuint64_t)nb * esz, 128, (cuuint64_t)nb * nb * esz};
+    cuuint32_t box[4] = {(cuuint32_t)mnbox, (cuuint32_t)bk, (cuuint32_t)(TC_M / mnbox), 1};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = encode(map, dt, 4, base, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
+}
+
+// C map: the FP32 tiles of the descriptor, {rows, columns, tile}, box 32 x 32.
+bool encode_c_map(CUtensorMap *map, const plasma_desc_t &A)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+    if (encode == nullptr) return false;
+    const size_t tile_bytes = (size_t)A.mb * A.nb * 4;
+    const long long ntiles = (long long)(plasma_desc_storage_bytes(A) / tile_bytes);
+    if (ntiles <= 0) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)A.mb, (cuuint64_t)A.nb, (cuuint64_t)ntiles};
+    cuuint64_t strides[2] = {(cuuint64_t)A.mb * 4, (cuuint64_t)tile_bytes};
+    cuuint32_t box[3] = {32, 32, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, A.matrix, dims, strides,
+                        box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+template <int MODE>
+void launch_update(cudaStream_t s, const CUtensorMap &map, const CUtensorMap &cmap,
+                   const TcArgs &g, unsigned grid, plasma_devstat_t *st)
+{
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_update_tc<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             TC_SMEM);
+        attr = true;
+    }
+    k_update_tc<MODE><<<grid, TC_THREADS, TC_SMEM, s>>>(map, cmap, g, st);
 }
 
 }  // namespace
 
-// Eligibility of the tensor-core update for an FP32 descriptor: general
-// storage, lower, square tiles of 128 or 256 with no ragged tile.
+// Eligibility of the tensor-core update for an FP32 descriptor: general or
+// packed-lower storage, lower, square tiles of 128 or 256, no ragged tile.
 extern "C" int plasma_cuda_update_tc_ok(plasma_desc_t A, plasma_enum_t uplo)
 {
     return A.precision == PlasmaRealFloat &&
@@ -378,40 +518,70 @@ extern "C" int plasma_cuda_update_tc_ok(plasma_desc_t A, plasma_enum_t uplo)
            A.gm % A.mb == 0 && A.gn % A.nb == 0 && A.i == 0 && A.j == 0;
 }
 
-// The operands come from `panel`: the copy of panel k rounded to the product
-// precision (TF32 values in FP32 containers, or BF16), tile m at
-// panel + m*nb*nb elements, column-major, 1024-byte aligned.
+// Bytes of one operand copy of a panel (plasma_cuda_panel_round).
+extern "C" size_t plasma_cuda_panel_bytes(int mode, plasma_desc_t A)
+{
+    size_t tile = (size_t)A.mb * A.mb;
+    switch (mode) {
+    case PLASMA_TC_BF16: return (size_t)A.mt * tile * 2;
+    case PLASMA_TC_TF32: return (size_t)A.mt * tile * 4;
+    case PLASMA_TC_TF32X3: return 2 * (size_t)A.mt * tile * 4;
+    default: return 0;
+    }
+}
+
+// The operands come from `panel`: the copy of panel k made by
+// plasma_cuda_panel_round for the same mode, 1024-byte aligned.  Returns 0
+// (nothing launched) when the update is not eligible.
 extern "C" int plasma_cuda_update_tc(cudaStream_t s, plasma_devstat_t *st,
                                      int mode, plasma_desc_t A, int k, int nlo,
-                                     int nhi, const void *panel)
+                                     int nhi, const void *panel, int num_sms)
 {
     if (nhi <= nlo) return 1;
     const int nb = A.mb;
     long long pairs = 0;
     for (int n = nlo; n < nhi; n++) pairs += A.mt - n;
-    long long nitems = pairs * (nb / TC_M);
+    const long long nitems = pairs * (nb / TC_M);
     if (nitems <= 0) return 1;
+    if (panel == nullptr || ((uintptr_t)panel & 1023) != 0 ||
+        ((uintptr_t)A.matrix & 15) != 0)
+        return 0;
 
-    CUtensorMap map;
+    CUtensorMap map, cmap;
+    bool enc;
+    switch (mode) {
+    case PLASMA_TC_TF32:
+        enc = encode_tile_map(&map, (void *)panel, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, nb,
+                              A.mt, Geo<MODE_TF32>::BK, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B);
+        break;
+    case PLASMA_TC_TF32X3:
+        enc = encode_tile_map(&map, (void *)panel, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, nb,
+                              2LL * A.mt, Geo<MODE_TF32X3>::BK,
+                              CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B);
+        break;
+    case PLASMA_TC_BF16:
+        enc = encode_tile_map(&map, (void *)panel, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, nb,
+                              A.mt, Geo<MODE_BF16>::BK, CU_TENSOR_MAP_SWIZZLE_128B);
+        break;
+    default:
+        return 0;
+    }
+    if (!enc || !encode_c_map(&cmap, A))
+        return 0;
+
     TcArgs g;
     g.A = A;
     g.k = k;
     g.nlo = nlo;
     g.nhi = nhi;
-    if (panel == nullptr || ((uintptr_t)panel & 1023) != 0)
-        return 0;
-    if (mode == PlasmaFactorTF32) {
-        if (!encode_tile_map(&map, (void *)panel, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
-                             nb, A.mt, 32, 32, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B))
-            return 0;
-    } else {
-        if (!encode_tile_map(&map, (void *)panel, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
-                             nb, A.mt, 64, 64, CU_TENSOR_MAP_SWIZZLE_128B))
-            return 0;
-    }
-    g.op_base = 0;
-    g.op_stride = 1;
-    static bool attr[3] = {false, false, false};
+    g.mt = A.mt;
+    g.nitems = nitems;
+    // a few items per CTA: enough to overlap epilogue and MMAs, few enough
+    // that CTAs retire often (two waves or more of CTAs when possible)
+    long long ipc = nitems / (2LL * (num_sms > 0 ? num_sms : 148));
+    g.ipc = (int)(ipc < 1 ? 1 : ipc > 8 ? 8 : ipc);
+    const unsigned grid = (unsigned)((nitems + g.ipc - 1) / g.ipc);
+
     PLASMA_COUNT_LAUNCH();
     double flops = 0.0, bytes = 0.0;
     for (int n = nlo; n < nhi; n++) {
@@ -423,46 +593,54 @@ extern "C" int plasma_cuda_update_tc(cudaStream_t s, plasma_devstat_t *st,
         }
     }
     int prof = plasma_prof_begin(s);
-    if (mode == PlasmaFactorTF32) {
-        if (!attr[1]) {
-            cudaFuncSetAttribute(k_update_tc<MODE_TF32>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
-            attr[1] = true;
-        }
-        k_update_tc<MODE_TF32><<<(unsigned)nitems, TC_THREADS, TC_SMEM, s>>>(map, g, st);
-    } else {
-        if (!attr[2]) {
-            cudaFuncSetAttribute(k_update_tc<MODE_BF16>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
-            attr[2] = true;
-        }
-        k_update_tc<MODE_BF16><<<(unsigned)nitems, TC_THREADS, TC_SMEM, s>>>(map, g, st);
+    switch (mode) {
+    case PLASMA_TC_TF32: launch_update<MODE_TF32>(s, map, cmap, g, grid, st); break;
+    case PLASMA_TC_TF32X3: launch_update<MODE_TF32X3>(s, map, cmap, g, grid, st); break;
+    default: launch_update<MODE_BF16>(s, map, cmap, g, grid, st); break;
     }
     plasma_prof_end(prof, s, PLASMA_KCLASS_UPDATE, flops, bytes);
     return 1;
 }
 
 // Operand copy of panel k: panel tile m (m = k+1 .. mt-1) <- A(m,k) rounded
-// to the product precision (TF32: round to nearest, ties away, kept in an
-// FP32 container; BF16: round to nearest even), same column-major layout.
+// to the product precision, same column-major layout.  TF32: round to
+// nearest, ties away, kept in an FP32 container; BF16: round to nearest
+// even; TF32X3: hi = tf32(a) at tile m and lo = tf32(a - hi) at tile m + mt
+// (a - hi is exact in FP32).
 namespace {
-template <bool BF16>
+template <int MODE>
 __global__ void k_panel_round(plasma_desc_t A, int k, void *panel,
                               const plasma_devstat_t *st)
 {
     if (plasma_failed(st)) return;
     const int m = k + 1 + blockIdx.y;
     const int nb = A.mb;
-    const float *a = (const float *)plasma_tile_addr(A, m, k);
+    const float4 *a = (const float4 *)plasma_tile_addr(A, m, k);
     const size_t tot = (size_t)nb * nb;
-    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot / 4;
          e += (size_t)gridDim.x * blockDim.x) {
-        if (BF16) {
-            ((__nv_bfloat16 *)panel)[(size_t)m * tot + e] = __float2bfloat16_rn(a[e]);
+        const float4 x = a[e];
+        const float xs[4] = {x.x, x.y, x.z, x.w};
+        if (MODE == MODE_BF16) {
+            __nv_bfloat16 *o = (__nv_bfloat16 *)panel + (size_t)m * tot + 4 * e;
+#pragma unroll
+            for (int i = 0; i < 4; i++) o[i] = __float2bfloat16_rn(xs[i]);
         } else {
-            uint32_t r;
-            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(a[e]));
-            ((uint32_t *)panel)[(size_t)m * tot + e] = r;
+            uint32_t hi[4], lo[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi[i]) : "f"(xs[i]));
+                if (MODE == MODE_TF32X3) {
+                    float r = xs[i] - __uint_as_float(hi[i]);
+                    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo[i]) : "f"(r));
+                }
+            }
+            uint4 *o = (uint4 *)panel + ((size_t)m * tot) / 4 + e;
+            *o = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+            if (MODE == MODE_TF32X3) {
+                uint4 *ol = (uint4 *)panel + ((size_t)(m + A.mt) * tot) / 4 + e;
+                *ol = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+            }
         }
     }
 }
@@ -475,8 +653,10 @@ extern "C" void plasma_cuda_panel_round(cudaStream_t s, plasma_devstat_t *st,
     int rows = A.mt - k - 1;
     if (rows <= 0) return;
     PLASMA_COUNT_LAUNCH();
-    if (mode == PlasmaFactorBF16)
-        k_panel_round<true><<<dim3(16, rows), 256, 0, s>>>(A, k, panel, st);
-    else
-        k_panel_round<false><<<dim3(16, rows), 256, 0, s>>>(A, k, panel, st);
+    dim3 grid(16, rows);
+    switch (mode) {
+    case PLASMA_TC_BF16: k_panel_round<MODE_BF16><<<grid, 256, 0, s>>>(A, k, panel, st); break;
+    case PLASMA_TC_TF32X3: k_panel_round<MODE_TF32X3><<<grid, 256, 0, s>>>(A, k, panel, st); break;
+    default: k_panel_round<MODE_TF32><<<grid, 256, 0, s>>>(A, k, panel, st); break;
+    }
 }

@@ -180,15 +180,20 @@ void plasma_cuda_geadd(cudaStream_t s, plasma_devstat_t *st,
 void plasma_cuda_lacpy(cudaStream_t s, plasma_devstat_t *st,
                        plasma_desc_t A, plasma_desc_t B);
 
-/* Tensor-core (tcgen05) trailing update of FP32 factors with TF32 or BF16
- * products (cuda/update_tc.cu). */
+/* Tensor-core (tcgen05) trailing update of FP32 factors (cuda/update_tc.cu).
+ * Product precisions: */
+#define PLASMA_TC_TF32   1   /* one TF32 product                         */
+#define PLASMA_TC_BF16   2   /* one BF16 product                         */
+#define PLASMA_TC_TF32X3 3   /* lo*hi + hi*lo + hi*hi TF32 split (FP32)   */
 int plasma_cuda_update_tc_ok(plasma_desc_t A, plasma_enum_t uplo);
-int plasma_cuda_update_tc(cudaStream_t s, plasma_devstat_t *st, int mode,
+size_t plasma_cuda_panel_bytes(int tc_mode, plasma_desc_t A);
+int plasma_cuda_update_tc(cudaStream_t s, plasma_devstat_t *st, int tc_mode,
                           plasma_desc_t A, int k, int nlo, int nhi,
-                          const void *panel);
-/* Copy of panel k rounded to the product precision of mode (TF32 or BF16),
- * tile m at panel + m*nb*nb elements. */
-void plasma_cuda_panel_round(cudaStream_t s, plasma_devstat_t *st, int mode,
+                          const void *panel, int num_sms);
+/* Copy of panel k in the operand format of tc_mode (plasma_cuda_panel_bytes
+ * bytes, tile m at panel + m*nb*nb elements; TF32X3 adds the low parts at
+ * tile m + mt). */
+void plasma_cuda_panel_round(cudaStream_t s, plasma_devstat_t *st, int tc_mode,
                              plasma_desc_t A, int k, void *panel);
 /* FP32 panel kernels: 3 = FP32-accurate split TF32 products, 1 = TF32. */
 void plasma_cuda_panel_set_split(int split);
