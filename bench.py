@@ -341,30 +341,37 @@ def main():
                  "update_kernel_tflops": upd_tf, "backward_error": berr_d}
         del Aw, Bw
 
-    # end to end through host buffers (pageable numpy arrays)
+    # end to end through host buffers: page-locked host copies of A and b,
+    # the H2D upload of A's stored triangle and of b and the D2H of x inside
+    # the timed region, through the LAPACK-layout entry point
     e2e = None
     if not args.no_e2e and rank == 0:
-        ah = np.ascontiguousarray(A.cpu().numpy())     # symmetric: also column-major
-        bh = np.ascontiguousarray(B.cpu().numpy())     # nrhs x n = column-major n x nrhs
-        xh = np.zeros_like(bh)
-        L.plasma_dsposv_ex(pb.PlasmaLower, n, nrhs, ah.ctypes.data, n, bh.ctypes.data, n,
-                           xh.ctypes.data, n, ctypes.byref(it), None)
+        ah = torch.empty_like(A, device="cpu").pin_memory()
+        ah.copy_(A)                                   # symmetric: also column-major
+        bh = torch.empty_like(B, device="cpu").pin_memory()
+        bh.copy_(B)                                   # nrhs x n = column-major n x nrhs
+        xh = torch.zeros_like(bh).pin_memory()
+        L.plasma_dsposv_ex(pb.PlasmaLower, n, nrhs, ah.data_ptr(), n, bh.data_ptr(), n,
+                           xh.data_ptr(), n, ctypes.byref(it), None)
         torch.cuda.synchronize()
-        g0 = torch.cuda.Event(enable_timing=True)
-        g1 = torch.cuda.Event(enable_timing=True)
-        g0.record()
-        rc = L.plasma_dsposv_ex(pb.PlasmaLower, n, nrhs, ah.ctypes.data, n, bh.ctypes.data,
-                                n, xh.ctypes.data, n, ctypes.byref(it), None)
-        g1.record()
-        torch.cuda.synchronize()
-        assert rc == 0
-        ems = g0.elapsed_time(g1)
+        ets = []
+        for _ in range(2):
+            g0 = torch.cuda.Event(enable_timing=True)
+            g1 = torch.cuda.Event(enable_timing=True)
+            g0.record()
+            rc = L.plasma_dsposv_ex(pb.PlasmaLower, n, nrhs, ah.data_ptr(), n, bh.data_ptr(),
+                                    n, xh.data_ptr(), n, ctypes.byref(it), None)
+            g1.record()
+            torch.cuda.synchronize()
+            assert rc == 0
+            ets.append(g0.elapsed_time(g1))
+        ems = min(ets)
         nbv = L.plasma_tuning_get_potrf_nb(pb.PlasmaRealFloat, n) if args.nb == 0 else args.nb
         h2d = sum((n - c0) * min(nbv, n - c0) for c0 in range(0, n, nbv)) * 8 + n * nrhs * 8
         e2e = {"value": flops_of(n, nrhs) / ems / 1e6, "unit": "GFLOP/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(n * nrhs * 8),
-               "ms_per_step": ems}
-        del ah
+               "ms_per_step": ems, "host_memory": "page-locked"}
+        del ah, bh, xh
 
     cpu = None
     if not args.no_cpu and rank == 0:
@@ -379,10 +386,13 @@ def main():
         return 0
 
     upd = prof["update"]
-    mode_peak = {"fp32": ("fp32", peaks.get("fp32")), "tf32": ("tf32", peaks.get("tf32")),
-                 "bf16": ("bf16", peaks.get("bf16")), "auto": ("bf16", peaks.get("bf16"))}
-    pk_name, pk = mode_peak[args.mode]
-    achieved = upd["flops"] / upd["ms"] / 1e9 if upd["ms"] > 0 else None
+    # all factor modes run the trailing update on the tcgen05 tensor cores;
+    # fp32 forms every FP32 product as three TF32 products (lo*hi + hi*lo +
+    # hi*hi), so its tensor work is three times the algorithmic flops
+    mode_peak = {"fp32": ("tf32", peaks.get("tf32"), 3), "tf32": ("tf32", peaks.get("tf32"), 1),
+                 "bf16": ("bf16", peaks.get("bf16"), 1), "auto": ("bf16", peaks.get("bf16"), 1)}
+    pk_name, pk, passes = mode_peak[args.mode]
+    achieved = passes * upd["flops"] / upd["ms"] / 1e9 if upd["ms"] > 0 else None
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "update_traffic.json")
     if os.path.exists(tpath):
@@ -408,14 +418,17 @@ def main():
         "backward_error_target": 50 * n * 2.0 ** -53,
         "dposv": dposv,
         "speedup_vs_dposv": (dposv["ms"] / ms) if dposv else None,
-        "roofline": {"bound": "tensor" if args.mode != "fp32" else "fp32-simt",
-                     "kernel": "trailing update (SYRK+GEMM)",
+        "roofline": {"bound": "tensor",
+                     "kernel": "k_update_tc trailing update (SYRK+GEMM)",
                      "achieved": achieved, "peak": pk, "unit": "TFLOP/s",
                      "frac": (achieved / pk) if achieved and pk else None,
-                     "peak_source": f"{pk_name} cuBLAS GEMM measured live"
-                     if pk_name != "bf16" else "MEASURED_PEAKS.json bf16_tflops",
+                     "tensor_products_per_flop": passes,
+                     "achieved_algorithmic": (achieved / passes) if achieved else None,
+                     "peak_source": f"{pk_name} cuBLAS GEMM measured live (of measured)"
+                     if pk_name != "bf16" else "MEASURED_PEAKS.json bf16_tflops (of measured)",
                      "traffic": traffic,
-                     "launches": upd["launches"], "avg_launch_ms": upd["ms"] / max(1, upd["launches"])},
+                     "launches": upd["launches"],
+                     "avg_launch_ms": upd["ms"] / max(1, upd["launches"])},
         "phases_ms_per_step": {k: v["ms"] / args.steps for k, v in prof.items()},
         "peaks_tflops": peaks,
         "e2e": e2e,

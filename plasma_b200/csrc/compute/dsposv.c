@@ -249,8 +249,12 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
     int nrhs = B.n;
     *iter = 0;
 
+    /* the small device buffers at their full size from the start, so that
+     * the slot never grows (and moves) during the solve */
     double *d_small = (double *)plasma_scratch(plasma, PLASMA_SLOT_SMALL,
-                                               sizeof(double) * (2 * nrhs + 8));
+                                               sizeof(double) * (2 * nrhs + 8) +
+                                               sizeof(double) * (GMRES_RESTART + 8) +
+                                               plasma_cuda_dots_work(GMRES_RESTART + 2));
     const int fast_sweep = plasma_sweep_reserve(plasma, As);
     size_t wtiles = (size_t)As.mt * As.mb * As.mb * sizeof(float);
     size_t wblocks = plasma_cuda_trsv_w_bytes(As);
@@ -273,7 +277,9 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
 
     int call = plasma_call_begin(plasma, sequence, request);
     double Anorm = 0.0;
-    plasma_cuda_lansy_inf(S, st, uplo, A, d_anorm, NULL);
+    double *sw = (double *)plasma_scratch(plasma, PLASMA_SLOT_SYMV,
+                                          plasma_cuda_symv_work(A));
+    plasma_cuda_lansy_inf(S, st, uplo, A, d_anorm, sw);
     cudaMemcpyAsync(&Anorm, d_anorm, sizeof(double), cudaMemcpyDeviceToHost, S);
 
     /* ------------------------------------------------------------------
@@ -310,12 +316,7 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
     size_t need = sizeof(double) * (size_t)n * (6 + mres + 1) +
                   sizeof(double) * npad + sizeof(float) * npad + 4096;
     char *wk = (char *)plasma_scratch(plasma, PLASMA_SLOT_REFINE, need);
-    double *small = (double *)plasma_scratch(plasma, PLASMA_SLOT_SMALL,
-                                             sizeof(double) * (2 * nrhs + 8) +
-                                             sizeof(double) * (mres + 8) +
-                                             plasma_cuda_dots_work(mres + 2));
-    double *sw = (double *)plasma_scratch(plasma, PLASMA_SLOT_SYMV,
-                                          plasma_cuda_symv_work(A));
+    double *small = d_small;
     if (wk == NULL || small == NULL || sw == NULL) {
         plasma_request_fail(sequence, request, PlasmaErrorOutOfMemory);
         return;

@@ -146,7 +146,9 @@ extern "C" void plasma_cuda_lansy_inf(cudaStream_t s, plasma_devstat_t *st,
                                       plasma_enum_t uplo, plasma_desc_t A,
                                       double *dnorm, double *work)
 {
-    (void)work;
+    /* with a workspace: one pass over the stored tiles (symv.cu) */
+    if (work != nullptr && plasma_cuda_lansy_tiles(s, st, uplo, A, dnorm, work))
+        return;
     cudaMemsetAsync(dnorm, 0, sizeof(double), s);
     if (A.mt == 0) return;
     PLASMA_COUNT_LAUNCH();

@@ -11,6 +11,10 @@
 // across lanes by a 31-shuffle butterfly.  The per-tile partial vectors go to
 // a workspace and a second kernel sums them in a fixed order, so results are
 // bit-reproducible.
+//
+// The same pass with |a| and x = 1 gives the row sums of |A|, whose maximum
+// is ||A||_inf (plasma_pdlansy, compute/pzlansy.c:83-131): one read of the
+// stored triangle.
 #include "common.cuh"
 
 namespace {
@@ -46,6 +50,7 @@ __device__ __forceinline__ void stored_tile(int t, int mt, int uplo, int &p, int
     }
 }
 
+template <bool ABS>
 __global__ void __launch_bounds__(SV_THREADS, 2)
 k_symv_tiles(plasma_desc_t A, int uplo, const double *x, double *part,
              const plasma_devstat_t *st)
@@ -65,8 +70,8 @@ k_symv_tiles(plasma_desc_t A, int uplo, const double *x, double *part,
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
     for (int i = tid; i < nb; i += SV_THREADS) {
-        xp_s[i] = i < rows ? x[(size_t)p * nb + i] : 0.0;
-        xq_s[i] = i < cols ? x[(size_t)q * nb + i] : 0.0;
+        xp_s[i] = i < rows ? (ABS ? 1.0 : x[(size_t)p * nb + i]) : 0.0;
+        xq_s[i] = i < cols ? (ABS ? 1.0 : x[(size_t)q * nb + i]) : 0.0;
     }
     for (int i = tid; i < 8 * 512; i += SV_THREADS) (&ypart[0][0])[i] = 0.0;
     __syncthreads();
@@ -86,6 +91,7 @@ k_symv_tiles(plasma_desc_t A, int uplo, const double *x, double *part,
                 const int col = cb * 32 + c;
                 double a = (row < rows && col < cols)
                                ? S[(size_t)col * ld + row] : 0.0;
+                if (ABS) a = fabs(a);
                 // the part of a diagonal tile outside the stored triangle is
                 // not referenced
                 double a_dir = a, a_tr = a;
@@ -137,8 +143,8 @@ k_symv_reduce(plasma_desc_t A, const double *part, const double *b,
         for (int q = 0; q < mt; q++) s += part[((size_t)m * mt + q) * nb + i];
         size_t gi = (size_t)m * nb + i;
         double v = (b ? b[gi] : 0.0) - s;
-        r[gi] = b ? v : s;
-        xm = fmax(xm, fabs(x[gi]));
+        if (r) r[gi] = b ? v : s;
+        if (x) xm = fmax(xm, fabs(x[gi]));
         rm = fmax(rm, fabs(v));
     }
     for (int off = 16; off > 0; off >>= 1) {
@@ -175,10 +181,35 @@ extern "C" int plasma_cuda_symv(cudaStream_t s, plasma_devstat_t *st,
     const long long ntiles = (long long)mt * (mt + 1) / 2;
     PLASMA_COUNT_LAUNCH();
     int prof = plasma_prof_begin(s);
-    k_symv_tiles<<<(unsigned)ntiles, SV_THREADS, 0, s>>>(A, uplo, x, work, st);
+    k_symv_tiles<false><<<(unsigned)ntiles, SV_THREADS, 0, s>>>(A, uplo, x, work, st);
     PLASMA_COUNT_LAUNCH();
     k_symv_reduce<<<mt, SV_THREADS, 0, s>>>(A, work, b, x, r, xnorm, rnorm, st);
     double n = A.m;
     plasma_prof_end(prof, s, PLASMA_KCLASS_AUX, 2.0 * n * n, 8.0 * n * (n + 1) / 2.0);
+    return 1;
+}
+
+// ||A||_inf of symmetric A (uplo triangle) into *norm (device): the maximum
+// row sum of |A| from one pass over the stored tiles.  work:
+// plasma_cuda_symv_work bytes.  Returns 0 (nothing launched) when A is not
+// an FP64 descriptor with square tiles of at most 512.
+extern "C" int plasma_cuda_lansy_tiles(cudaStream_t s, plasma_devstat_t *st,
+                                       plasma_enum_t uplo, plasma_desc_t A,
+                                       double *norm, double *work)
+{
+    if (A.precision != PlasmaRealDouble || A.mb != A.nb || A.mb > 512)
+        return 0;
+    cudaMemsetAsync(norm, 0, sizeof(double), s);
+    if (A.mt == 0) return 1;
+    const int mt = A.mt;
+    const long long ntiles = (long long)mt * (mt + 1) / 2;
+    PLASMA_COUNT_LAUNCH();
+    int prof = plasma_prof_begin(s);
+    k_symv_tiles<true><<<(unsigned)ntiles, SV_THREADS, 0, s>>>(A, uplo, nullptr, work, st);
+    PLASMA_COUNT_LAUNCH();
+    k_symv_reduce<<<mt, SV_THREADS, 0, s>>>(A, work, nullptr, nullptr, nullptr, nullptr,
+                                            norm, st);
+    double n = A.m;
+    plasma_prof_end(prof, s, PLASMA_KCLASS_AUX, n * n, 8.0 * n * (n + 1) / 2.0);
     return 1;
 }

@@ -158,7 +158,12 @@ void plasma_cuda_update(cudaStream_t s, plasma_devstat_t *st,
                         int nlo, int nhi, int num_sms);
 
 /* dsposv helpers. */
-/* Infinity norm of symmetric A (uplo triangle) into *dnorm (device). */
+/* Infinity norm of symmetric A (uplo triangle) into *dnorm (device); work
+ * (plasma_cuda_symv_work bytes, or NULL for the slow row-per-thread kernel)
+ * selects the one-pass tile kernel. */
+int plasma_cuda_lansy_tiles(cudaStream_t s, plasma_devstat_t *st,
+                            plasma_enum_t uplo, plasma_desc_t A, double *norm,
+                            double *work);
 void plasma_cuda_lansy_inf(cudaStream_t s, plasma_devstat_t *st,
                            plasma_enum_t uplo, plasma_desc_t A,
                            double *dnorm, double *work);

@@ -470,3 +470,21 @@ def test_single_rhs_sweeps(L, uplo, n, nb):
     x32 = np.asfortranarray(b.astype(np.float32))
     assert L.plasma_sposv(uplo, n, 1, a32.ctypes.data, n, x32.ctypes.data, n) == 0
     assert solve_residual(a, x32.astype(np.float64), b) < TOL * SEPS
+
+
+@pytest.mark.parametrize("uplo", [LO, UP])
+@pytest.mark.parametrize("n,nb", [(1000, 256), (777, 128), (64, 64)])
+def test_dsposv_anorm_tile_pass(L, uplo, n, nb):
+    """||A||_inf from the one-pass tile kernel (|a| row sums of the stored
+    triangle and its mirror) equals the dense row-sum maximum."""
+    set_nb(L, nb)
+    a, b = gen.diag_dominant(n, 1, seed=1500 + n)
+    x = np.zeros_like(b, order="F")
+    it = ctypes.c_int()
+    info = pb.plasma_dsposv_info_t()
+    assert L.plasma_dsposv_ex(uplo, n, 1, np.asfortranarray(a).ctypes.data, n,
+                              np.asfortranarray(b).ctypes.data, n, x.ctypes.data, n,
+                              ctypes.byref(it), ctypes.byref(info)) == 0
+    ref = np.abs(a).sum(axis=1).max()
+    assert abs(info.anorm - ref) <= 1e-13 * ref
+    assert solve_residual(a, x, b) < TOL * EPS
