@@ -54,6 +54,7 @@ def parse():
 
 
 MODES = {"fp32": 0, "tf32": 1, "bf16": 2, "auto": 3}
+UPDATE_DRAM_BYTES_PER_TILE = {"fp32": 393846}
 REFINE = {"ir": 0, "gmres": 1, "auto": 2}
 
 
@@ -393,13 +394,16 @@ def main():
                  "bf16": ("bf16", peaks.get("bf16"), 1), "auto": ("bf16", peaks.get("bf16"), 1)}
     pk_name, pk, passes = mode_peak[args.mode]
     achieved = passes * upd["flops"] / upd["ms"] / 1e9 if upd["ms"] > 0 else None
+    # DRAM bytes per 256 x 256 tile-update of k_update_tc, read + write, from
+    # one ncu capture (profiles/k_update_tc_tf32x3_n8192.md: a bulk launch of
+    # 325 tile-updates); a launch's traffic grows with the tiles it updates
+    # (the algorithmic C read + write is 524288 bytes per tile-update)
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "update_traffic.json")
-    if os.path.exists(tpath):
-        try:
-            traffic = json.load(open(tpath)).get(args.mode)
-        except Exception:
-            traffic = None
+    dram_per_tile = UPDATE_DRAM_BYTES_PER_TILE.get(args.mode)
+    nbv = args.nb or L.plasma_tuning_get_potrf_nb(pb.PlasmaRealFloat, n)
+    if dram_per_tile and nbv == 256 and upd["launches"] > 0:
+        tiles = upd["bytes"] / (8.0 * nbv * nbv)           # FP32 C read + write
+        traffic = dram_per_tile * tiles / upd["launches"]
     value = world * flops_of(n, nrhs) / ms / 1e6
     line = {
         "metric": "dsposv FP64-equivalent throughput to FP64 backward error "
@@ -426,7 +430,7 @@ def main():
                      "achieved_algorithmic": (achieved / passes) if achieved else None,
                      "peak_source": f"{pk_name} cuBLAS GEMM measured live (of measured)"
                      if pk_name != "bf16" else "MEASURED_PEAKS.json bf16_tflops (of measured)",
-                     "traffic": traffic,
+                     "traffic": traffic, "traffic_unit": "bytes per launch",
                      "launches": upd["launches"],
                      "avg_launch_ms": upd["ms"] / max(1, upd["launches"])},
         "phases_ms_per_step": {k: v["ms"] / args.steps for k, v in prof.items()},

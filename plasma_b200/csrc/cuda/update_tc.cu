@@ -576,10 +576,21 @@ extern "C" int plasma_cuda_update_tc(cudaStream_t s, plasma_devstat_t *st,
     g.nhi = nhi;
     g.mt = A.mt;
     g.nitems = nitems;
-    // a few items per CTA: enough to overlap epilogue and MMAs, few enough
-    // that CTAs retire often (two waves or more of CTAs when possible)
-    long long ipc = nitems / (2LL * (num_sms > 0 ? num_sms : 148));
-    g.ipc = (int)(ipc < 1 ? 1 : ipc > 8 ? 8 : ipc);
+    // Items per CTA (one CTA per SM): the smallest estimated makespan,
+    // waves * (ipc + 1/2) items -- a CTA's pipeline fill and its last,
+    // unoverlapped epilogue cost about half an item -- ties to the larger
+    // ipc (the SMs left over serve the panel stream).
+    const long long sms = num_sms > 0 ? num_sms : 148;
+    long long best_ipc = 1, best_cost = -1;
+    for (long long ipc = 1; ipc <= 8; ipc++) {
+        const long long ctas = (nitems + ipc - 1) / ipc;
+        const long long cost = ((ctas + sms - 1) / sms) * (2 * ipc + 1);
+        if (best_cost < 0 || cost <= best_cost) {
+            best_cost = cost;
+            best_ipc = ipc;
+        }
+    }
+    g.ipc = (int)best_ipc;
     const unsigned grid = (unsigned)((nitems + g.ipc - 1) / g.ipc);
 
     PLASMA_COUNT_LAUNCH();
