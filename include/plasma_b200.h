@@ -95,6 +95,49 @@ void plasma_omp_dpotrs_noalloc(plasma_enum_t uplo, plasma_desc_t A,
                                plasma_desc_t B, plasma_sequence_t *sequence,
                                plasma_request_t *request);
 
+/*
+ * Reverse mode of the Cholesky factor and solve.  No reference counterpart
+ * (PLASMA computes no derivatives).  A = L L^T (uplo = PlasmaLower) or
+ * A = U^T U (PlasmaUpper, L = U^T).
+ *
+ * plasma_?potrf_adjoint: on entry the uplo triangle of Lbar holds the
+ * cotangent of the factor; on exit Lbar holds the full symmetric cotangent of
+ * A, sym(L^-T Phi(L^T Lbar) L^-1) with Phi the lower triangle and half the
+ * diagonal (both triangles written).  Returns -1/-2/-4/-6 for an illegal
+ * uplo/n/ldl/ldlbar.
+ *
+ * plasma_?potrs_adjoint: X = A^-1 B was computed with the factor in L.  On
+ * entry Xbar is the cotangent of X, on exit the cotangent of B (A^-1 Xbar);
+ * the uplo triangle of Lbar is decreased by the factor cotangent of the
+ * solve, tril((Bbar X^T + X Bbar^T) L) (its transpose for upper storage), so
+ * that the cotangents of several uses of L accumulate in Lbar before one
+ * plasma_?potrf_adjoint.  Returns -1/-2/-3/-5/-7/-9/-11 for an illegal
+ * uplo/n/nrhs/ldl/ldx/ldxbar/ldlbar.
+ *
+ * Pointers may be host or device memory.  The omp forms take general
+ * descriptors (Lbar general for potrf_adjoint) and report through sequence.
+ */
+int plasma_dpotrf_adjoint(plasma_enum_t uplo, int n, const double *pL, int ldl,
+                          double *pLbar, int ldlbar);
+int plasma_spotrf_adjoint(plasma_enum_t uplo, int n, const float *pL, int ldl,
+                          float *pLbar, int ldlbar);
+int plasma_dpotrs_adjoint(plasma_enum_t uplo, int n, int nrhs, const double *pL, int ldl,
+                          const double *pX, int ldx, double *pXbar, int ldxbar,
+                          double *pLbar, int ldlbar);
+int plasma_spotrs_adjoint(plasma_enum_t uplo, int n, int nrhs, const float *pL, int ldl,
+                          const float *pX, int ldx, float *pXbar, int ldxbar,
+                          float *pLbar, int ldlbar);
+void plasma_omp_dpotrf_adjoint(plasma_enum_t uplo, plasma_desc_t L, plasma_desc_t Lbar,
+                               plasma_sequence_t *sequence, plasma_request_t *request);
+void plasma_omp_spotrf_adjoint(plasma_enum_t uplo, plasma_desc_t L, plasma_desc_t Lbar,
+                               plasma_sequence_t *sequence, plasma_request_t *request);
+void plasma_omp_dpotrs_adjoint(plasma_enum_t uplo, plasma_desc_t L, plasma_desc_t X,
+                               plasma_desc_t Xbar, plasma_desc_t Lbar,
+                               plasma_sequence_t *sequence, plasma_request_t *request);
+void plasma_omp_spotrs_adjoint(plasma_enum_t uplo, plasma_desc_t L, plasma_desc_t X,
+                               plasma_desc_t Xbar, plasma_desc_t Lbar,
+                               plasma_sequence_t *sequence, plasma_request_t *request);
+
 /* Human-readable name of a return code. */
 const char *plasma_strerror(int code);
 

@@ -119,6 +119,16 @@ _SIGNATURES = [
     ("plasma_omp_spotrf", None, [c_int, _DESC, _SEQ, _REQ]),
     ("plasma_omp_dpotrs", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
     ("plasma_omp_dpotrs_noalloc", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
+    ("plasma_dpotrf_adjoint", c_int, [c_int, c_int, c_void_p, c_int, c_void_p, c_int]),
+    ("plasma_spotrf_adjoint", c_int, [c_int, c_int, c_void_p, c_int, c_void_p, c_int]),
+    ("plasma_dpotrs_adjoint", c_int, [c_int, c_int, c_int, c_void_p, c_int, c_void_p,
+                                      c_int, c_void_p, c_int, c_void_p, c_int]),
+    ("plasma_spotrs_adjoint", c_int, [c_int, c_int, c_int, c_void_p, c_int, c_void_p,
+                                      c_int, c_void_p, c_int, c_void_p, c_int]),
+    ("plasma_omp_dpotrf_adjoint", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
+    ("plasma_omp_spotrf_adjoint", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
+    ("plasma_omp_dpotrs_adjoint", None, [c_int, _DESC, _DESC, _DESC, _DESC, _SEQ, _REQ]),
+    ("plasma_omp_spotrs_adjoint", None, [c_int, _DESC, _DESC, _DESC, _DESC, _SEQ, _REQ]),
     ("plasma_omp_spotrs", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
     ("plasma_omp_dposv", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
     ("plasma_omp_sposv", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),

@@ -35,7 +35,7 @@ typedef struct {
 
 #define PLASMA_MAX_PENDING_CALLS 4096
 #define PLASMA_NUM_STREAMS 4
-#define PLASMA_SCRATCH_SLOTS 6
+#define PLASMA_SCRATCH_SLOTS 7
 
 /* scratch slots */
 enum {
@@ -44,7 +44,8 @@ enum {
     PLASMA_SLOT_SMALL   = 2,   /* norms and other vectors                     */
     PLASMA_SLOT_MIXED   = 3,   /* low-precision operand copies (dsposv)       */
     PLASMA_SLOT_REFINE  = 4,   /* refinement vectors and Krylov basis         */
-    PLASMA_SLOT_SYMV    = 5    /* per-tile partial products of the residual   */
+    PLASMA_SLOT_SYMV    = 5,   /* per-tile partial products of the residual   */
+    PLASMA_SLOT_ADJOINT = 6    /* n x n work matrices of the adjoints         */
 };
 
 typedef struct {
@@ -205,6 +206,31 @@ void plasma_cuda_panel_set_split(int split);
 /* A(i,i) = value for i in [i0, i1) (identity padding of FP32 factors). */
 void plasma_cuda_set_diag(cudaStream_t s, plasma_desc_t A, int i0, int i1,
                           double value);
+
+/* A view of a tile descriptor for the adjoint kernels (cuda/adjoint.cu):
+ * logical element (i, j) is D(r0 + i, c0 + j), or D(r0 + j, c0 + i) when
+ * trans; tri = 1 (2) reads entries above (below) the diagonal of the
+ * untransposed view as zero; diag_scale = 1 halves its diagonal. */
+typedef struct {
+    plasma_desc_t D;
+    int r0, c0;
+    int trans;
+    int tri;
+    int diag_scale;
+} plasma_view_t;
+
+/* C = beta C + alpha op(A) op(B) (M x N, inner K); C is written inside the
+ * mask ctri (0 all, 1 i >= j, 2 i <= j), outside it zeroed when czero. */
+void plasma_cuda_gemm_view(cudaStream_t s, plasma_devstat_t *st, int M, int N,
+                           int K, double alpha, plasma_view_t A, plasma_view_t B,
+                           double beta, plasma_view_t C, int ctri, int czero);
+/* dst(i,j) = op(src)(i,j) (masks and diagonal scale of src applied),
+ * i < M, j < N. */
+void plasma_cuda_copy_view(cudaStream_t s, plasma_devstat_t *st, int M, int N,
+                           plasma_view_t src, plasma_view_t dst);
+/* dst(i,j) = (src(i,j) + src(j,i)) / 2 for the n x n views. */
+void plasma_cuda_symmetrize(cudaStream_t s, plasma_devstat_t *st, int n,
+                            plasma_view_t src, plasma_view_t dst);
 
 /* Refinement kernels (cuda/symv.cu, trsv.cu, vec.cu). */
 size_t plasma_cuda_symv_work(plasma_desc_t A);

@@ -200,3 +200,18 @@ def test_lapack_constants():
     assert L.plasma_norm_const(b"I") == 175
     assert L.plasma_side_const(b"R") == 142
     assert L.plasma_diag_const(b"U") == 132
+
+
+def test_adjoint_argument_codes(hostonly):
+    """Illegal arguments of the adjoint entry points are rejected before any
+    device work, with LAPACK-style negative codes."""
+    L = hostonly
+    assert L.plasma_dpotrf_adjoint(0, 4, None, 4, None, 4) == -1
+    assert L.plasma_dpotrf_adjoint(pb.PlasmaLower, -1, None, 4, None, 4) == -2
+    assert L.plasma_dpotrf_adjoint(pb.PlasmaLower, 4, None, 3, None, 4) == -4
+    assert L.plasma_dpotrf_adjoint(pb.PlasmaLower, 4, None, 4, None, 3) == -6
+    assert L.plasma_dpotrf_adjoint(pb.PlasmaLower, 0, None, 1, None, 1) == 0
+    assert L.plasma_spotrs_adjoint(7, 4, 1, None, 4, None, 4, None, 4, None, 4) == -1
+    assert L.plasma_dpotrs_adjoint(pb.PlasmaUpper, 4, -2, None, 4, None, 4, None, 4, None, 4) == -3
+    assert L.plasma_dpotrs_adjoint(pb.PlasmaUpper, 4, 1, None, 4, None, 2, None, 4, None, 4) == -7
+    assert L.plasma_dpotrs_adjoint(pb.PlasmaUpper, 4, 1, None, 4, None, 4, None, 4, None, 1) == -11
