@@ -50,6 +50,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-dposv", action="store_true")
+    p.add_argument("--workload", default="dsposv", choices=["dsposv", "adjoint", "batched"],
+                   help="dsposv: the headline; adjoint / batched: the differentiation "
+                        "and batched-solve configurations, one JSON line each")
     return p.parse_args()
 
 
@@ -235,8 +238,66 @@ def run_reference(args):
     return 0
 
 
+def run_adjoint(args):
+    """Forward (potrf + potrs) and backward (the two adjoints) of
+    logdet(A) + trace(B^T A^-1 B) through plasma_b200.autograd, A = G G^T/n + I
+    (G ~ N(0,1), seed 3), B ~ N(0,1), nrhs = 8, n in {4096, 8192}, FP64 and
+    FP32.  Device memory: the peak of (total - free) over the step, above the
+    level before it (the library allocates with cudaMalloc, outside torch)."""
+    import torch
+    import plasma_b200 as pb
+    import plasma_b200.autograd as ag
+    L = pb.lib()
+    assert L.plasma_init() == 0
+    rows = []
+    for n in (4096, 8192):
+        for dt in (torch.float64, torch.float32):
+            g = torch.Generator(device="cuda").manual_seed(3)
+            G = torch.randn(n, n, generator=g, device="cuda", dtype=torch.float64)
+            A0 = (G @ G.T / n + torch.eye(n, device="cuda", dtype=torch.float64)).to(dt)
+            B0 = torch.randn(n, 8, generator=g, device="cuda", dtype=torch.float64).to(dt)
+            del G
+            fwd, bwd, peak = [], [], 0
+            for rep in range(args.warmup + args.steps):
+                A = A0.clone().requires_grad_(True)
+                B = B0.clone().requires_grad_(True)
+                torch.cuda.synchronize()
+                free0, total = torch.cuda.mem_get_info()
+                e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+                e[0].record()
+                f = ag.gaussian_nll(A, B)
+                e[1].record()
+                torch.cuda.synchronize()
+                free1, _ = torch.cuda.mem_get_info()
+                f.backward()
+                e[2].record()
+                torch.cuda.synchronize()
+                free2, _ = torch.cuda.mem_get_info()
+                if rep >= args.warmup:
+                    fwd.append(e[0].elapsed_time(e[1]))
+                    bwd.append(e[1].elapsed_time(e[2]))
+                    peak = max(peak, free0 - min(free1, free2))
+                del A, B, f
+            flops_f = n ** 3 / 3 + 2 * n * n * 8
+            flops_b = 4 * n ** 3 / 3 + 6 * n * n * 8
+            rows.append({"n": n, "dtype": "f64" if dt == torch.float64 else "f32",
+                         "forward_ms": min(fwd), "backward_ms": min(bwd),
+                         "forward_gflops": flops_f / min(fwd) / 1e6,
+                         "backward_gflops": flops_b / min(bwd) / 1e6,
+                         "device_memory_gb": peak / 1e9})
+    print(json.dumps({"workload": "adjoint", "metric": "forward + backward time of "
+                      "logdet(A) + tr(B^T A^-1 B)", "unit": "ms", "steps": args.steps,
+                      "warmup": args.warmup, "nrhs": 8, "results": rows}), flush=True)
+    L.plasma_finalize()
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "adjoint":
+        return run_adjoint(args)
+    if args.workload == "batched":
+        return run_batched(args)
     if args.impl == "reference":
         return run_reference(args)
 

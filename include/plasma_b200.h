@@ -54,6 +54,9 @@ long long plasma_kernel_launches(void);
  * autotuner. */
 int plasma_tuning_get_potrf_nb(int dtyp, int n);
 int plasma_tuning_set_potrf_nb(int dtyp, int n, int nb);
+/* Block width (16 or 32) of the batched kernels for matrices of order n. */
+int plasma_tuning_get_batched_nb(int dtyp, int n);
+int plasma_tuning_set_batched_nb(int dtyp, int n, int nb);
 
 /* Kernel classes of the opt-in profiler. */
 enum {
@@ -137,6 +140,50 @@ void plasma_omp_dpotrs_adjoint(plasma_enum_t uplo, plasma_desc_t L, plasma_desc_
 void plasma_omp_spotrs_adjoint(plasma_enum_t uplo, plasma_desc_t L, plasma_desc_t X,
                                plasma_desc_t Xbar, plasma_desc_t Lbar,
                                plasma_sequence_t *sequence, plasma_request_t *request);
+
+/*
+ * Batched SPD systems of uneven order (0 <= n_i <= 512).  No reference
+ * counterpart (PLASMA factors one matrix at a time).  A plan fixes the
+ * orders: matrix i is column-major n_i x n_i (ld n_i) at element offset
+ * off_a[i] of one device array, its vector (one right-hand side) at off_b[i]
+ * of another (plasma_batch_offsets; plasma_batch_matrix_elems /
+ * plasma_batch_vector_elems give the array lengths).  Each operation is one
+ * persistent kernel launch on the context stream (device pointers, returns
+ * at once); the plan orders the matrices largest first and takes the block
+ * width of each size bucket from the tuning table.  With
+ * plasma_batch_set_graph(plan, 1) the launch is captured once into a CUDA
+ * graph held by the plan and replayed by later calls with the same
+ * pointers.
+ *   posv    : A <- L (lower triangle), B <- A^-1 B, info[i] as LAPACK dpotrf
+ *             (the solve is skipped for a matrix with info != 0)
+ *   potrf   : A <- L, info
+ *   potrs   : B <- A^-1 B with the factor in L
+ *   potrf_adjoint : Lbar (cotangent of L in the lower triangle) <- the
+ *             symmetric cotangent of A, both triangles
+ *   potrs_adjoint : Xbar <- A^-1 Xbar, lower triangle of Lbar -=
+ *             tril((Bbar X^T + X Bbar^T) L)
+ * Returns 0, PlasmaErrorNotInitialized, or a negative argument position.
+ */
+typedef struct plasma_batch_s plasma_batch_t;
+int plasma_batch_create(plasma_enum_t precision, int batch, const int *n,
+                        plasma_batch_t **plan);
+void plasma_batch_destroy(plasma_batch_t *plan);
+long long plasma_batch_matrix_elems(const plasma_batch_t *plan);
+long long plasma_batch_vector_elems(const plasma_batch_t *plan);
+int plasma_batch_offsets(const plasma_batch_t *plan, long long *off_a, long long *off_b);
+int plasma_batch_set_graph(plasma_batch_t *plan, int on);
+int plasma_dposv_batched(plasma_batch_t *plan, double *A, double *B, int *info);
+int plasma_sposv_batched(plasma_batch_t *plan, float *A, float *B, int *info);
+int plasma_dpotrf_batched(plasma_batch_t *plan, double *A, int *info);
+int plasma_spotrf_batched(plasma_batch_t *plan, float *A, int *info);
+int plasma_dpotrs_batched(plasma_batch_t *plan, const double *L, double *B);
+int plasma_spotrs_batched(plasma_batch_t *plan, const float *L, float *B);
+int plasma_dpotrf_adjoint_batched(plasma_batch_t *plan, const double *L, double *Lbar);
+int plasma_spotrf_adjoint_batched(plasma_batch_t *plan, const float *L, float *Lbar);
+int plasma_dpotrs_adjoint_batched(plasma_batch_t *plan, const double *L, const double *X,
+                                  double *Xbar, double *Lbar);
+int plasma_spotrs_adjoint_batched(plasma_batch_t *plan, const float *L, const float *X,
+                                  float *Xbar, float *Lbar);
 
 /* Human-readable name of a return code. */
 const char *plasma_strerror(int code);

@@ -119,6 +119,24 @@ _SIGNATURES = [
     ("plasma_omp_spotrf", None, [c_int, _DESC, _SEQ, _REQ]),
     ("plasma_omp_dpotrs", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
     ("plasma_omp_dpotrs_noalloc", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
+    ("plasma_batch_create", c_int, [c_int, c_int, c_void_p, POINTER(c_void_p)]),
+    ("plasma_batch_destroy", None, [c_void_p]),
+    ("plasma_batch_matrix_elems", c_longlong, [c_void_p]),
+    ("plasma_batch_vector_elems", c_longlong, [c_void_p]),
+    ("plasma_batch_offsets", c_int, [c_void_p, c_void_p, c_void_p]),
+    ("plasma_batch_set_graph", c_int, [c_void_p, c_int]),
+    ("plasma_dposv_batched", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("plasma_sposv_batched", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("plasma_dpotrf_batched", c_int, [c_void_p, c_void_p, c_void_p]),
+    ("plasma_spotrf_batched", c_int, [c_void_p, c_void_p, c_void_p]),
+    ("plasma_dpotrs_batched", c_int, [c_void_p, c_void_p, c_void_p]),
+    ("plasma_spotrs_batched", c_int, [c_void_p, c_void_p, c_void_p]),
+    ("plasma_dpotrf_adjoint_batched", c_int, [c_void_p, c_void_p, c_void_p]),
+    ("plasma_spotrf_adjoint_batched", c_int, [c_void_p, c_void_p, c_void_p]),
+    ("plasma_dpotrs_adjoint_batched", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("plasma_spotrs_adjoint_batched", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("plasma_tuning_get_batched_nb", c_int, [c_int, c_int]),
+    ("plasma_tuning_set_batched_nb", c_int, [c_int, c_int, c_int]),
     ("plasma_dpotrf_adjoint", c_int, [c_int, c_int, c_void_p, c_int, c_void_p, c_int]),
     ("plasma_spotrf_adjoint", c_int, [c_int, c_int, c_void_p, c_int, c_void_p, c_int]),
     ("plasma_dpotrs_adjoint", c_int, [c_int, c_int, c_int, c_void_p, c_int, c_void_p,

@@ -70,3 +70,33 @@ int plasma_tuning_get_potrf_nb(int dtyp, int n)
 {
     return potrf_table[prec_index(dtyp)][bucket_of(n)];
 }
+
+/* Block width of the batched kernels (16 or 32) per size bucket of the
+ * matrix order: buckets n <= 32, 64, 128, 256, 512.  [0] FP64, [1] FP32. */
+#define NBBUCKETS 5
+static int batched_table[2][NBBUCKETS] = {
+    /* <=32 <=64 <=128 <=256 <=512 */
+    {  32,  16,  32,   32,   32 },
+    {  32,  16,  32,   32,   32 },
+};
+
+static int batched_bucket(int n)
+{
+    int b = 0;
+    while (b < NBBUCKETS - 1 && n > (32 << b))
+        b++;
+    return b;
+}
+
+int plasma_tuning_get_batched_nb(int dtyp, int n)
+{
+    return batched_table[prec_index(dtyp)][batched_bucket(n)];
+}
+
+int plasma_tuning_set_batched_nb(int dtyp, int n, int nb)
+{
+    if (nb != 16 && nb != 32)
+        return PlasmaErrorIllegalValue;
+    batched_table[prec_index(dtyp)][batched_bucket(n)] = nb;
+    return PlasmaSuccess;
+}

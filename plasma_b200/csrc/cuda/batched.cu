@@ -1,0 +1,693 @@
+// batched.cu -- thousands of independent SPD systems of uneven size in one
+// persistent launch: Cholesky factor (potrf), solve (potrs, one right-hand
+// side) and their adjoints.  No reference counterpart (PLASMA factors one
+// matrix at a time); the per-matrix algorithm is the reference's blocked
+// right-looking Cholesky (compute/pzpotrf.c:37-80 at the scale of one CTA).
+//
+// Layout: matrix i is column-major n_i x n_i (ld = n_i) at A + off_a[i];
+// its right-hand side / solution at B + off_b[i].  A plan (host side) sorts
+// the matrices by decreasing size (longest processing time first) and picks
+// the block width NB of each size bucket from a measured table.
+//
+// One CTA per SM, 256 threads, takes the next matrix from an atomic counter
+// until the list is exhausted, so large and small matrices balance across
+// SMs.  Per matrix, for each block column j0:
+//   (a) one warp factors the NB x NB diagonal block, lane r holding row r,
+//       pivots broadcast by shuffles (LAPACK's info on a non-positive or NaN
+//       pivot, and the matrix is abandoned);
+//   (b) every thread solves one row of the panel below, x D^T = a, with D
+//       in shared memory; the panel is kept in shared memory;
+//   (c) the trailing lower triangle is updated, A22 -= P P^T, by warps on
+//       32 x 32 blocks with DMMA (FP64) or the three-product TF32 split
+//       (FP32, FP32-accurate), C read and written in global memory (L2).
+// The solve follows in the same CTA while the factor is in L2: forward by
+// block (diagonal block by one warp, the rows below by all threads),
+// backward by block (column dot products by warps, then the diagonal block).
+#include "common.cuh"
+#include "mma.cuh"
+
+#include <stdlib.h>
+#include <string.h>
+
+namespace {
+
+constexpr int BT = 256;               // threads per CTA
+constexpr int NMAX = 512;             // largest matrix of the batched path
+constexpr int NBMAXB = 32;            // largest block width
+
+template <typename T> constexpr int ps_ld() { return NBMAXB + Pad<T>::v; }
+// shared memory: panel [NMAX][ps_ld], two 32 x 33 blocks, a vector of NMAX,
+// 32 reciprocal pivots
+template <typename T> constexpr int batched_smem()
+{
+    return (NMAX * ps_ld<T>() + 2 * NBMAXB * (NBMAXB + 1) + NMAX + NBMAXB) * (int)sizeof(T);
+}
+
+enum { OP_POSV = 0, OP_POTRF = 1, OP_POTRS = 2, OP_POTRF_ADJ = 3, OP_POTRS_ADJ = 4 };
+
+struct BatchArgs {
+    int batch;
+    const int *n;               // [batch]
+    const long long *off_a;     // [batch] element offsets of the matrices
+    const long long *off_b;     // [batch] element offsets of the vectors
+    const int *order;           // processing order (largest first)
+    const unsigned char *nbsel; // [batch] block width of each matrix (16 or 32)
+    void *A;                    // matrices (the factor for solves and adjoints)
+    void *B;                    // right-hand sides / solutions (X for the adjoint)
+    void *C;                    // Xbar -> Bbar (potrs adjoint)
+    void *D;                    // Lbar (adjoints)
+    int *info;                  // [batch] (factorisations)
+    int *counter;               // zeroed before the launch
+    int op;
+};
+
+// ------------------------------------------------------------------ factor
+template <typename T, int SPLIT, int NB>
+__device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag)
+{
+    constexpr int PLD = ps_ld<T>();
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    for (int j0 = 0; j0 < n; j0 += NB) {
+        const int jb = min(NB, n - j0);
+        const int m2 = n - j0 - jb;
+        // (a) diagonal block
+        if (warp == 0) {
+            T v[NB];
+#pragma unroll
+            for (int c = 0; c < NB; c++)
+                v[c] = (lane < jb && c < jb && lane >= c) ? A[(size_t)(j0 + c) * n + j0 + lane]
+                                                          : T(0);
+            int bad = 0;
+            T myrd = T(1);
+#pragma unroll
+            for (int c = 0; c < NB; c++) {
+                if (c < jb) {
+                    T d = __shfl_sync(0xffffffffu, v[c], c);
+                    bool ok = d > T(0);
+                    if (!ok && bad == 0) bad = c + 1;
+                    T sd = ok ? sqrt(d) : T(1);
+                    T rd = T(1) / sd;
+                    if (lane == c) myrd = rd;
+                    if (lane >= c) v[c] = (lane == c) ? sd : v[c] * rd;
+#pragma unroll
+                    for (int c2 = c + 1; c2 < NB; c2++) {
+                        T l = __shfl_sync(0xffffffffu, v[c], c2);
+                        if (c2 < jb && lane >= c2) v[c2] -= v[c] * l;
+                    }
+                }
+            }
+            if (lane < jb) {
+#pragma unroll
+                for (int c = 0; c < NB; c++)
+                    if (c < jb && lane >= c) {
+                        A[(size_t)(j0 + c) * n + j0 + lane] = v[c];
+                        Ds[c * (NBMAXB + 1) + lane] = v[c];
+                    }
+                rdiag[lane] = myrd;
+            }
+            if (lane == 0) *flag = bad;
+        }
+        __syncthreads();
+        const int bad = *flag;
+        if (bad) return j0 + bad;
+        // (b) panel rows below: x D^T = a, one thread per row
+        for (int r = tid; r < m2; r += BT) {
+            const int row = j0 + jb + r;
+            T x[NB];
+#pragma unroll
+            for (int c = 0; c < NB; c++) x[c] = c < jb ? A[(size_t)(j0 + c) * n + row] : T(0);
+#pragma unroll
+            for (int c = 0; c < NB; c++) {
+                if (c < jb) {
+                    T s = x[c];
+#pragma unroll
+                    for (int c2 = 0; c2 < c; c2++) s -= x[c2] * Ds[c2 * (NBMAXB + 1) + c];
+                    x[c] = s * rdiag[c];
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < NB; c++) {
+                if (c < jb) A[(size_t)(j0 + c) * n + row] = x[c];
+                Ps[r * PLD + c] = x[c];            // zero beyond jb
+            }
+        }
+        __syncthreads();
+        // (c) trailing lower triangle, 32 x 32 blocks, K = NB (zero padded)
+        const int nbk = (m2 + 31) / 32;
+        const int npairs = nbk * (nbk + 1) / 2;
+        for (int p = warp; p < npairs; p += BT / 32) {
+            int bj = 0, q = p;
+            while (q >= nbk - bj) { q -= nbk - bj; bj++; }
+            const int bi = bj + q;
+            const int r0 = bi * 32, c0 = bj * 32;
+            T acc[2][4][4];
+#pragma unroll
+            for (int a = 0; a < 2; a++)
+#pragma unroll
+                for (int b = 0; b < 4; b++)
+#pragma unroll
+                    for (int c = 0; c < 4; c++) acc[a][b][c] = T(0);
+#pragma unroll
+            for (int k8 = 0; k8 < NB; k8 += 8) {
+                T bf[4][2];
+#pragma unroll
+                for (int ni = 0; ni < 4; ni++) {
+                    const int cr = c0 + ni * 8 + g;
+                    bf[ni][0] = cr < m2 ? Ps[cr * PLD + k8 + t] : T(0);
+                    bf[ni][1] = cr < m2 ? Ps[cr * PLD + k8 + t + 4] : T(0);
+                }
+#pragma unroll
+                for (int mi = 0; mi < 2; mi++) {
+                    const int ra = r0 + mi * 16 + g;
+                    T af[4];
+                    af[0] = ra < m2 ? Ps[ra * PLD + k8 + t] : T(0);
+                    af[1] = ra + 8 < m2 ? Ps[(ra + 8) * PLD + k8 + t] : T(0);
+                    af[2] = ra < m2 ? Ps[ra * PLD + k8 + t + 4] : T(0);
+                    af[3] = ra + 8 < m2 ? Ps[(ra + 8) * PLD + k8 + t + 4] : T(0);
+#pragma unroll
+                    for (int ni = 0; ni < 4; ni++) mma8<SPLIT>(acc[mi][ni], af, bf[ni]);
+                }
+            }
+            T *C = A + (size_t)(j0 + jb) * n + (j0 + jb);   // A22(0,0)
+#pragma unroll
+            for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+                for (int ni = 0; ni < 4; ni++)
+#pragma unroll
+                    for (int h = 0; h < 2; h++)
+#pragma unroll
+                        for (int e = 0; e < 2; e++) {
+                            const int r = r0 + mi * 16 + g + 8 * h;
+                            const int c = c0 + ni * 8 + 2 * t + e;
+                            if (r < m2 && c < m2 && r >= c)
+                                C[(size_t)c * n + r] -= acc[mi][ni][2 * h + e];
+                        }
+        }
+        __syncthreads();
+    }
+    return 0;
+}
+
+// ------------------------------------------------------------------- solve
+// b <- A^-1 b with the factor L in the lower triangle of A (n x n, ld n).
+template <typename T>
+__device__ void solve_one(const T *A, int n, T *b, T *Ys)
+{
+    constexpr int NB = 32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = tid; i < n; i += BT) Ys[i] = b[i];
+    __syncthreads();
+    // forward: L y = b
+    for (int j0 = 0; j0 < n; j0 += NB) {
+        const int jb = min(NB, n - j0);
+        if (warp == 0) {
+            T y = lane < jb ? Ys[j0 + lane] : T(0);
+            for (int c = 0; c < jb; c++) {
+                if (lane == c) y = y / A[(size_t)(j0 + c) * n + j0 + c];
+                const T yc = __shfl_sync(0xffffffffu, y, c);
+                if (lane > c && lane < jb) y -= A[(size_t)(j0 + c) * n + j0 + lane] * yc;
+            }
+            if (lane < jb) Ys[j0 + lane] = y;
+        }
+        __syncthreads();
+        for (int r = j0 + jb + tid; r < n; r += BT) {
+            T s = Ys[r];
+            for (int c = 0; c < jb; c++) s -= A[(size_t)(j0 + c) * n + r] * Ys[j0 + c];
+            Ys[r] = s;
+        }
+        __syncthreads();
+    }
+    // backward: L^T x = y
+    for (int j0 = ((n - 1) / NB) * NB; j0 >= 0; j0 -= NB) {
+        const int jb = min(NB, n - j0);
+        for (int c = warp; c < jb; c += BT / 32) {
+            T s = T(0);
+            for (int i = j0 + jb + lane; i < n; i += 32) s += A[(size_t)(j0 + c) * n + i] * Ys[i];
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+            if (lane == 0) Ys[j0 + c] -= s;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            T x = lane < jb ? Ys[j0 + lane] : T(0);
+            for (int c = jb - 1; c >= 0; c--) {
+                if (lane == c) x = x / A[(size_t)(j0 + c) * n + j0 + c];
+                const T xc = __shfl_sync(0xffffffffu, x, c);
+                if (lane < c) x -= A[(size_t)(j0 + lane) * n + j0 + c] * xc;
+            }
+            if (lane < jb) Ys[j0 + lane] = x;
+        }
+        __syncthreads();
+    }
+    for (int i = tid; i < n; i += BT) b[i] = Ys[i];
+    __syncthreads();
+}
+
+// ------------------------------------------------------------ potrs adjoint
+// xbar <- A^-1 xbar (= bbar); Lbar -= tril(bbar (L^T x)^T + x (L^T bbar)^T)
+template <typename T>
+__device__ void solve_adjoint_one(const T *Lf, int n, const T *x, T *xbar, T *Lbar, T *Ys,
+                                  T *U)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    solve_one<T>(Lf, n, xbar, Ys);                 // Ys keeps bbar
+    T *u1 = U, *u2 = U + NMAX;                     // L^T x, L^T bbar
+    for (int c = warp; c < n; c += BT / 32) {
+        T s1 = T(0), s2 = T(0);
+        for (int r = c + lane; r < n; r += 32) {
+            const T l = Lf[(size_t)c * n + r];
+            s1 += l * x[r];
+            s2 += l * Ys[r];
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            s1 += __shfl_xor_sync(0xffffffffu, s1, off);
+            s2 += __shfl_xor_sync(0xffffffffu, s2, off);
+        }
+        if (lane == 0) { u1[c] = s1; u2[c] = s2; }
+    }
+    __syncthreads();
+    for (int c = warp; c < n; c += BT / 32)
+        for (int r = c + lane; r < n; r += 32)
+            Lbar[(size_t)c * n + r] -= Ys[r] * u1[c] + x[r] * u2[c];
+    __syncthreads();
+}
+
+// ------------------------------------------------------------ potrf adjoint
+// Blocked reverse mode of the Cholesky factor, walking block columns from the
+// last to the first and recomputing from the factor L (lower triangle of Lf):
+//   Cbar <- Cbar D^-1;  Bbar -= Cbar R;  Dbar <- tril(Dbar) - tril(Cbar^T C);
+//   Dbar <- unblocked reverse of the diagonal block;
+//   Rbar -= Cbar^T B + (Dbar + Dbar^T) R
+// (R, D, B, C: the blocks left of, on, below-left of and below the diagonal
+// block; bars the same blocks of Lbar).  The result Abar is lower triangular
+// and the symmetric cotangent is (Abar + Abar^T)/2 with Abar's own diagonal,
+// written into both triangles of Lbar at the end.
+template <typename T>
+__device__ void factor_adjoint_one(const T *Lf, int n, T *Lb, T *Cs, T *Ds, T *Dbs)
+{
+    constexpr int NB = 32, CLD = NB + 1;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int k = n; k > 0; k -= NB) {
+        const int j = max(0, k - NB), jb = k - j, m2 = n - k;
+        for (int e = tid; e < NB * NB; e += BT) {
+            const int r = e % NB, c = e / NB;
+            const bool in = r < jb && c < jb && r >= c;
+            Ds[c * CLD + r] = in ? Lf[(size_t)(j + c) * n + j + r] : T(0);
+            Dbs[c * CLD + r] = in ? Lb[(size_t)(j + c) * n + j + r] : T(0);
+        }
+        __syncthreads();
+        // (1) Cbar <- Cbar D^-1, one thread per row
+        for (int r = tid; r < m2; r += BT) {
+            T x[NB];
+#pragma unroll
+            for (int c = 0; c < NB; c++) x[c] = c < jb ? Lb[(size_t)(j + c) * n + k + r] : T(0);
+#pragma unroll
+            for (int c = NB - 1; c >= 0; c--) {
+                if (c < jb) {
+                    T s = x[c];
+#pragma unroll
+                    for (int c2 = c + 1; c2 < NB; c2++)
+                        if (c2 < jb) s -= x[c2] * Ds[c * CLD + c2];
+                    x[c] = s / Ds[c * CLD + c];
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < NB; c++) {
+                if (c < jb) Lb[(size_t)(j + c) * n + k + r] = x[c];
+                Cs[r * CLD + c] = x[c];
+            }
+        }
+        __syncthreads();
+        // (2) Bbar -= Cbar R   (rows k.., columns 0..j)
+        for (int e = tid; e < m2 * j; e += BT) {
+            const int r = e % m2, col = e / m2;
+            const T *Rc = Lf + (size_t)col * n + j;
+            T s = T(0);
+            for (int c = 0; c < jb; c++) s += Cs[r * CLD + c] * Rc[c];
+            Lb[(size_t)col * n + k + r] -= s;
+        }
+        // (3) Dbar -= tril(Cbar^T C)
+        for (int e = tid; e < jb * jb; e += BT) {
+            const int i = e % jb, c = e / jb;
+            if (i < c) continue;
+            const T *Cc = Lf + (size_t)(j + c) * n + k;
+            T s = T(0);
+            for (int r = 0; r < m2; r++) s += Cs[r * CLD + i] * Cc[r];
+            Dbs[c * CLD + i] -= s;
+        }
+        __syncthreads();
+        // (4) unblocked reverse on the diagonal block, one warp, lane = column
+        if (warp == 0) {
+            for (int jj = jb - 1; jj >= 0; jj--) {
+                const T djj = Ds[jj * CLD + jj];
+                T p = (lane > jj && lane < jb) ? Ds[jj * CLD + lane] * Dbs[jj * CLD + lane] : T(0);
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) p += __shfl_xor_sync(0xffffffffu, p, off);
+                if (lane == 0) Dbs[jj * CLD + jj] -= p / djj;
+                __syncwarp();
+                if (lane >= jj && lane < jb) Dbs[jj * CLD + lane] /= djj;
+                __syncwarp();
+                if (lane < jj) {
+                    T s = T(0);
+                    for (int r = jj; r < jb; r++) s += Dbs[jj * CLD + r] * Ds[lane * CLD + r];
+                    Dbs[lane * CLD + jj] -= s;
+                    const T ljc = Ds[lane * CLD + jj];
+                    for (int r = jj + 1; r < jb; r++) Dbs[lane * CLD + r] -= Dbs[jj * CLD + r] * ljc;
+                }
+                __syncwarp();
+                if (lane == 0) Dbs[jj * CLD + jj] *= T(0.5);
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        // (5) Rbar -= Cbar^T B + (Dbar + Dbar^T) R   (rows j..k, columns 0..j)
+        for (int e = tid; e < jb * j; e += BT) {
+            const int i = e % jb, col = e / jb;
+            const T *Bc = Lf + (size_t)col * n + k;
+            const T *Rc = Lf + (size_t)col * n + j;
+            T s = T(0);
+            for (int r = 0; r < m2; r++) s += Cs[r * CLD + i] * Bc[r];
+            for (int c = 0; c < jb; c++)
+                s += (Dbs[c * CLD + i] + Dbs[i * CLD + c]) * Rc[c];
+            Lb[(size_t)col * n + j + i] -= s;
+        }
+        for (int e = tid; e < jb * jb; e += BT) {
+            const int r = e % jb, c = e / jb;
+            if (r >= c) Lb[(size_t)(j + c) * n + j + r] = Dbs[c * CLD + r];
+        }
+        __syncthreads();
+    }
+    // symmetric cotangent in both triangles
+    for (size_t e = tid; e < (size_t)n * n; e += BT) {
+        const int r = (int)(e % n), c = (int)(e / n);
+        if (r > c) {
+            const T v = T(0.5) * Lb[(size_t)c * n + r];
+            Lb[(size_t)c * n + r] = v;
+            Lb[(size_t)r * n + c] = v;
+        }
+    }
+    __syncthreads();
+}
+
+// ------------------------------------------------------------------ kernel
+template <typename T, int SPLIT>
+__global__ void __launch_bounds__(BT, 1)
+k_batched(BatchArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *Ps = reinterpret_cast<T *>(smem_raw);        // [NMAX][ps_ld]
+    T *Ds = Ps + NMAX * ps_ld<T>();                 // [32][33]
+    T *D2 = Ds + NBMAXB * (NBMAXB + 1);             // [32][33]
+    T *Ys = D2 + NBMAXB * (NBMAXB + 1);             // [NMAX]
+    T *rdiag = Ys + NMAX;                           // [32]
+    __shared__ int idx_s, flag_s;
+    const int tid = threadIdx.x;
+    for (;;) {
+        if (tid == 0) idx_s = atomicAdd(a.counter, 1);
+        __syncthreads();
+        const int idx = idx_s;
+        __syncthreads();
+        if (idx >= a.batch) break;
+        const int m = a.order[idx];
+        const int n = a.n[m];
+        T *A = (T *)a.A + a.off_a[m];
+        if (a.op == OP_POSV || a.op == OP_POTRF) {
+            const int info = a.nbsel[m] == 16 ? factor_one<T, SPLIT, 16>(A, n, Ps, Ds, rdiag, &flag_s)
+                                              : factor_one<T, SPLIT, 32>(A, n, Ps, Ds, rdiag, &flag_s);
+            if (tid == 0) a.info[m] = info;
+            __syncthreads();
+            if (info == 0 && a.op == OP_POSV) solve_one<T>(A, n, (T *)a.B + a.off_b[m], Ys);
+        } else if (a.op == OP_POTRS) {
+            solve_one<T>(A, n, (T *)a.B + a.off_b[m], Ys);
+        } else if (a.op == OP_POTRS_ADJ) {
+            solve_adjoint_one<T>(A, n, (const T *)a.B + a.off_b[m], (T *)a.C + a.off_b[m],
+                                 (T *)a.D + a.off_a[m], Ys, Ps);
+        } else {
+            factor_adjoint_one<T>(A, n, (T *)a.D + a.off_a[m], Ps, Ds, D2);
+        }
+    }
+}
+
+template <typename T, int SPLIT>
+void launch_batched(cudaStream_t s, const BatchArgs &a, int grid)
+{
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_batched<T, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             batched_smem<T>());
+        attr = true;
+    }
+    k_batched<T, SPLIT><<<grid, BT, batched_smem<T>(), s>>>(a);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------- plans
+struct plasma_batch_s {
+    int batch;
+    int precision;
+    int *d_n;
+    long long *d_off_a, *d_off_b;
+    int *d_order;
+    unsigned char *d_nbsel;
+    int *d_counter;
+    long long *h_off_a, *h_off_b;
+    long long elems_a, elems_b;
+    int device;
+    int graph;                  // replay launches from a cached CUDA graph
+    cudaGraphExec_t exec;
+    int g_op;
+    void *g_ptr[5];
+};
+
+static void batch_free(plasma_batch_t *p)
+{
+    if (p == NULL) return;
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    cudaFree(p->d_n);
+    cudaFree(p->d_off_a);
+    cudaFree(p->d_off_b);
+    cudaFree(p->d_order);
+    cudaFree(p->d_nbsel);
+    cudaFree(p->d_counter);
+    free(p->h_off_a);
+    free(p->h_off_b);
+    free(p);
+}
+
+extern "C" int plasma_batch_create(plasma_enum_t precision, int batch, const int *n,
+                                   plasma_batch_t **plan)
+{
+    plasma_context_t *plasma = plasma_context_self();
+    if (plasma == NULL) return PlasmaErrorNotInitialized;
+    if (precision != PlasmaRealDouble && precision != PlasmaRealFloat) return -1;
+    if (batch < 0) return -2;
+    if (n == NULL && batch > 0) return -3;
+    if (plan == NULL) return -4;
+    for (int i = 0; i < batch; i++)
+        if (n[i] < 0 || n[i] > NMAX) {
+            plasma_error("plasma_batch_create: matrix orders must lie in [0, 512]");
+            return -3;
+        }
+    if (plasma->device < 0) return PlasmaErrorEnvironment;
+    plasma_batch_t *p = (plasma_batch_t *)calloc(1, sizeof(plasma_batch_t));
+    if (p == NULL) return PlasmaErrorOutOfMemory;
+    p->batch = batch;
+    p->precision = precision;
+    p->device = plasma->device;
+    const int cnt = batch > 0 ? batch : 1;
+    p->h_off_a = (long long *)malloc(sizeof(long long) * cnt);
+    p->h_off_b = (long long *)malloc(sizeof(long long) * cnt);
+    int *order = (int *)malloc(sizeof(int) * cnt);
+    unsigned char *nbsel = (unsigned char *)malloc(cnt);
+    if (!p->h_off_a || !p->h_off_b || !order || !nbsel) {
+        free(order); free(nbsel); batch_free(p);
+        return PlasmaErrorOutOfMemory;
+    }
+    // packed column-major matrices and vectors, each start 32-element aligned
+    long long oa = 0, ob = 0;
+    for (int i = 0; i < batch; i++) {
+        p->h_off_a[i] = oa;
+        p->h_off_b[i] = ob;
+        oa += ((long long)n[i] * n[i] + 31) / 32 * 32;
+        ob += ((long long)n[i] + 31) / 32 * 32;
+        order[i] = i;
+        nbsel[i] = (unsigned char)plasma_tuning_get_batched_nb(precision, n[i]);
+    }
+    p->elems_a = oa;
+    p->elems_b = ob;
+    // longest processing time first: decreasing n (stable)
+    int *tmp = (int *)malloc(sizeof(int) * cnt);
+    if (tmp == NULL) {
+        free(order); free(nbsel); batch_free(p);
+        return PlasmaErrorOutOfMemory;
+    }
+    {
+        // counting sort by n, largest first
+        int hist[NMAX + 2] = {0};
+        for (int i = 0; i < batch; i++) hist[NMAX - n[i]]++;
+        int acc = 0;
+        for (int v = 0; v <= NMAX + 1; v++) { int c = hist[v]; hist[v] = acc; acc += c; }
+        for (int i = 0; i < batch; i++) tmp[hist[NMAX - n[i]]++] = i;
+        memcpy(order, tmp, sizeof(int) * cnt);
+    }
+    free(tmp);
+    bool ok = cudaMalloc(&p->d_n, sizeof(int) * cnt) == cudaSuccess &&
+              cudaMalloc(&p->d_off_a, sizeof(long long) * cnt) == cudaSuccess &&
+              cudaMalloc(&p->d_off_b, sizeof(long long) * cnt) == cudaSuccess &&
+              cudaMalloc(&p->d_order, sizeof(int) * cnt) == cudaSuccess &&
+              cudaMalloc(&p->d_nbsel, cnt) == cudaSuccess &&
+              cudaMalloc(&p->d_counter, sizeof(int)) == cudaSuccess;
+    if (ok && batch > 0) {
+        ok = cudaMemcpy(p->d_n, n, sizeof(int) * batch, cudaMemcpyHostToDevice) == cudaSuccess &&
+             cudaMemcpy(p->d_off_a, p->h_off_a, sizeof(long long) * batch,
+                        cudaMemcpyHostToDevice) == cudaSuccess &&
+             cudaMemcpy(p->d_off_b, p->h_off_b, sizeof(long long) * batch,
+                        cudaMemcpyHostToDevice) == cudaSuccess &&
+             cudaMemcpy(p->d_order, order, sizeof(int) * batch, cudaMemcpyHostToDevice) ==
+                 cudaSuccess &&
+             cudaMemcpy(p->d_nbsel, nbsel, batch, cudaMemcpyHostToDevice) == cudaSuccess;
+    }
+    free(order);
+    free(nbsel);
+    if (!ok) {
+        cudaGetLastError();
+        batch_free(p);
+        return PlasmaErrorOutOfMemory;
+    }
+    *plan = p;
+    return PlasmaSuccess;
+}
+
+extern "C" void plasma_batch_destroy(plasma_batch_t *plan)
+{
+    if (plan) cudaDeviceSynchronize();
+    batch_free(plan);
+}
+
+extern "C" long long plasma_batch_matrix_elems(const plasma_batch_t *plan)
+{
+    return plan ? plan->elems_a : 0;
+}
+
+extern "C" long long plasma_batch_vector_elems(const plasma_batch_t *plan)
+{
+    return plan ? plan->elems_b : 0;
+}
+
+extern "C" int plasma_batch_offsets(const plasma_batch_t *plan, long long *off_a,
+                                    long long *off_b)
+{
+    if (plan == NULL) return -1;
+    if (off_a) memcpy(off_a, plan->h_off_a, sizeof(long long) * plan->batch);
+    if (off_b) memcpy(off_b, plan->h_off_b, sizeof(long long) * plan->batch);
+    return PlasmaSuccess;
+}
+
+extern "C" int plasma_batch_set_graph(plasma_batch_t *plan, int on)
+{
+    if (plan == NULL) return -1;
+    plan->graph = on != 0;
+    return PlasmaSuccess;
+}
+
+// One batched operation: the counter reset and one persistent launch on the
+// context stream, or the replay of the CUDA graph that holds both.
+static int batch_run(plasma_batch_t *p, int prec, int op, void *A, void *B, void *C, void *D,
+                     int *info)
+{
+    plasma_context_t *plasma = plasma_context_self();
+    if (plasma == NULL) return PlasmaErrorNotInitialized;
+    if (p == NULL) return -1;
+    if (p->precision != prec) {
+        plasma_error("batched call: precision differs from the plan's");
+        return -1;
+    }
+    if (p->batch == 0) return PlasmaSuccess;
+    if (A == NULL || ((op == OP_POSV || op == OP_POTRF) && info == NULL) ||
+        ((op == OP_POSV || op == OP_POTRS || op == OP_POTRS_ADJ) && B == NULL) ||
+        (op == OP_POTRS_ADJ && C == NULL) ||
+        ((op == OP_POTRF_ADJ || op == OP_POTRS_ADJ) && D == NULL))
+        return -2;
+    BatchArgs a;
+    a.batch = p->batch;
+    a.n = p->d_n;
+    a.off_a = p->d_off_a;
+    a.off_b = p->d_off_b;
+    a.order = p->d_order;
+    a.nbsel = p->d_nbsel;
+    a.A = A;
+    a.B = B;
+    a.C = C;
+    a.D = D;
+    a.info = info;
+    a.counter = p->d_counter;
+    a.op = op;
+    int grid = plasma->num_sms;          // one CTA per SM (registers, shared memory)
+    if (grid > p->batch) grid = p->batch;
+    cudaStream_t s = plasma->stream;
+
+    void *key[5] = {A, B, C, D, (void *)info};
+    if (p->graph) {
+        if (p->exec == NULL || p->g_op != op || memcmp(p->g_ptr, key, sizeof(key)) != 0) {
+            if (p->exec) {
+                cudaGraphExecDestroy(p->exec);
+                p->exec = NULL;
+            }
+            cudaStream_t cap;
+            if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess)
+                return PlasmaErrorEnvironment;
+            cudaGraph_t g = NULL;
+            cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+            cudaMemsetAsync(p->d_counter, 0, sizeof(int), cap);
+            if (prec == PlasmaRealDouble) launch_batched<double, 1>(cap, a, grid);
+            else launch_batched<float, 3>(cap, a, grid);
+            cudaError_t rc = cudaStreamEndCapture(cap, &g);
+            if (rc == cudaSuccess)
+                rc = cudaGraphInstantiate(&p->exec, g, 0);
+            if (g) cudaGraphDestroy(g);
+            cudaStreamDestroy(cap);
+            if (rc != cudaSuccess) {
+                cudaGetLastError();
+                p->exec = NULL;
+                return PlasmaErrorEnvironment;
+            }
+            p->g_op = op;
+            memcpy(p->g_ptr, key, sizeof(key));
+        }
+        PLASMA_COUNT_LAUNCH();
+        return cudaGraphLaunch(p->exec, s) == cudaSuccess ? PlasmaSuccess : PlasmaErrorEnvironment;
+    }
+    cudaMemsetAsync(p->d_counter, 0, sizeof(int), s);
+    PLASMA_COUNT_LAUNCH();
+    if (prec == PlasmaRealDouble) launch_batched<double, 1>(s, a, grid);
+    else launch_batched<float, 3>(s, a, grid);
+    return PlasmaSuccess;
+}
+
+extern "C" int plasma_dposv_batched(plasma_batch_t *plan, double *A, double *B, int *info)
+{ return batch_run(plan, PlasmaRealDouble, OP_POSV, A, B, NULL, NULL, info); }
+extern "C" int plasma_sposv_batched(plasma_batch_t *plan, float *A, float *B, int *info)
+{ return batch_run(plan, PlasmaRealFloat, OP_POSV, A, B, NULL, NULL, info); }
+extern "C" int plasma_dpotrf_batched(plasma_batch_t *plan, double *A, int *info)
+{ return batch_run(plan, PlasmaRealDouble, OP_POTRF, A, NULL, NULL, NULL, info); }
+extern "C" int plasma_spotrf_batched(plasma_batch_t *plan, float *A, int *info)
+{ return batch_run(plan, PlasmaRealFloat, OP_POTRF, A, NULL, NULL, NULL, info); }
+extern "C" int plasma_dpotrs_batched(plasma_batch_t *plan, const double *L, double *B)
+{ return batch_run(plan, PlasmaRealDouble, OP_POTRS, (void *)L, B, NULL, NULL, NULL); }
+extern "C" int plasma_spotrs_batched(plasma_batch_t *plan, const float *L, float *B)
+{ return batch_run(plan, PlasmaRealFloat, OP_POTRS, (void *)L, B, NULL, NULL, NULL); }
+extern "C" int plasma_dpotrf_adjoint_batched(plasma_batch_t *plan, const double *L,
+                                             double *Lbar)
+{ return batch_run(plan, PlasmaRealDouble, OP_POTRF_ADJ, (void *)L, NULL, NULL, Lbar, NULL); }
+extern "C" int plasma_spotrf_adjoint_batched(plasma_batch_t *plan, const float *L,
+                                             float *Lbar)
+{ return batch_run(plan, PlasmaRealFloat, OP_POTRF_ADJ, (void *)L, NULL, NULL, Lbar, NULL); }
+extern "C" int plasma_dpotrs_adjoint_batched(plasma_batch_t *plan, const double *L,
+                                             const double *X, double *Xbar, double *Lbar)
+{ return batch_run(plan, PlasmaRealDouble, OP_POTRS_ADJ, (void *)L, (void *)X, Xbar, Lbar, NULL); }
+extern "C" int plasma_spotrs_adjoint_batched(plasma_batch_t *plan, const float *L,
+                                             const float *X, float *Xbar, float *Lbar)
+{ return batch_run(plan, PlasmaRealFloat, OP_POTRS_ADJ, (void *)L, (void *)X, Xbar, Lbar, NULL); }
