@@ -242,8 +242,9 @@ def run_adjoint(args):
     """Forward (potrf + potrs) and backward (the two adjoints) of
     logdet(A) + trace(B^T A^-1 B) through plasma_b200.autograd, A = G G^T/n + I
     (G ~ N(0,1), seed 3), B ~ N(0,1), nrhs = 8, n in {4096, 8192}, FP64 and
-    FP32.  Device memory: the peak of (total - free) over the step, above the
-    level before it (the library allocates with cudaMalloc, outside torch)."""
+    FP32.  Device memory: the most held at the phase boundaries (inputs,
+    autograd state, the library's workspace, which it keeps between calls),
+    above the level before the inputs were made."""
     import torch
     import plasma_b200 as pb
     import plasma_b200.autograd as ag
@@ -252,12 +253,14 @@ def run_adjoint(args):
     rows = []
     for n in (4096, 8192):
         for dt in (torch.float64, torch.float32):
+            torch.cuda.synchronize()
+            free_base, total = torch.cuda.mem_get_info()
             g = torch.Generator(device="cuda").manual_seed(3)
             G = torch.randn(n, n, generator=g, device="cuda", dtype=torch.float64)
             A0 = (G @ G.T / n + torch.eye(n, device="cuda", dtype=torch.float64)).to(dt)
             B0 = torch.randn(n, 8, generator=g, device="cuda", dtype=torch.float64).to(dt)
             del G
-            fwd, bwd, peak = [], [], 0
+            fwd, bwd, peak = [], [], 0          # bytes above free_base
             for rep in range(args.warmup + args.steps):
                 A = A0.clone().requires_grad_(True)
                 B = B0.clone().requires_grad_(True)
@@ -273,10 +276,10 @@ def run_adjoint(args):
                 e[2].record()
                 torch.cuda.synchronize()
                 free2, _ = torch.cuda.mem_get_info()
+                peak = max(peak, free_base - min(free0, free1, free2))
                 if rep >= args.warmup:
                     fwd.append(e[0].elapsed_time(e[1]))
                     bwd.append(e[1].elapsed_time(e[2]))
-                    peak = max(peak, free0 - min(free1, free2))
                 del A, B, f
             flops_f = n ** 3 / 3 + 2 * n * n * 8
             flops_b = 4 * n ** 3 / 3 + 6 * n * n * 8
@@ -288,6 +291,87 @@ def run_adjoint(args):
     print(json.dumps({"workload": "adjoint", "metric": "forward + backward time of "
                       "logdet(A) + tr(B^T A^-1 B)", "unit": "ms", "steps": args.steps,
                       "warmup": args.warmup, "nrhs": 8, "results": rows}), flush=True)
+    L.plasma_finalize()
+    return 0
+
+
+def run_batched(args):
+    """4096 SPD systems, n uniform in [16, 512] (seed 5), A = G G^T / n + 0.1 I,
+    b ~ N(0,1), FP64 and FP32: one batched posv (factor + solve) launch per
+    step and the batched adjoints (potrs then potrf) of logdet(A) + b^T A^-1 b;
+    systems/s and p50/p99 per-batch latency (CUDA events, one event pair per
+    batch, CUDA-graph replay).  Beside it the plain path, plasma_dposv per
+    matrix on device pointers, on the first 256 matrices (scaled to the
+    batch)."""
+    import torch
+    import plasma_b200 as pb
+    from plasma_b200.batched import Batch
+    L = pb.lib()
+    assert L.plasma_init() == 0
+    rng = np.random.default_rng(5)
+    sizes = rng.integers(16, 513, 4096)
+    out = {"workload": "batched", "metric": "batched SPD solves (uneven n in [16, 512])",
+           "unit": "systems/s", "batch": len(sizes), "steps": args.steps,
+           "warmup": args.warmup, "flops_per_batch": float(np.sum(sizes.astype(float) ** 3) / 3),
+           "results": []}
+    for dt in (torch.float64, torch.float32):
+        b = Batch(sizes, dt, graph=True)
+        g = torch.Generator(device="cuda").manual_seed(5)
+        A0 = torch.zeros(b.matrix_elems, dtype=dt, device="cuda")
+        B0 = torch.zeros(b.vector_elems, dtype=dt, device="cuda")
+        for i, n in enumerate(sizes):
+            n = int(n)
+            G = torch.randn(n, n, generator=g, device="cuda", dtype=torch.float64)
+            a = G @ G.T / n + 0.1 * torch.eye(n, device="cuda", dtype=torch.float64)
+            A0[b.off_a[i]:b.off_a[i] + n * n] = a.reshape(-1).to(dt)
+            B0[b.off_b[i]:b.off_b[i] + n] = torch.randn(n, generator=g, device="cuda",
+                                                       dtype=torch.float64).to(dt)
+        A, B, info = A0.clone(), B0.clone(), b.info_buffer()
+        times, adj = [], []
+        for rep in range(args.warmup + args.steps):
+            A.copy_(A0)
+            B.copy_(B0)
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            e[0].record()
+            b.posv(A, B, info)
+            e[1].record()
+            Lbar = torch.zeros_like(A)
+            Xbar = B0.clone()
+            e[1].synchronize()
+            e2 = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            e2[0].record()
+            b.potrs_adjoint(A, B, Xbar, Lbar)
+            b.potrf_adjoint(A, Lbar)
+            e2[1].record()
+            torch.cuda.synchronize()
+            if rep >= args.warmup:
+                times.append(e[0].elapsed_time(e[1]))
+                adj.append(e2[0].elapsed_time(e2[1]))
+        assert not info.any()
+        t = np.array(times)
+        row = {"dtype": "f64" if dt == torch.float64 else "f32",
+               "systems_per_s": len(sizes) / (np.median(t) / 1e3),
+               "posv_ms_p50": float(np.percentile(t, 50)),
+               "posv_ms_p99": float(np.percentile(t, 99)),
+               "gflops": out["flops_per_batch"] / np.median(t) / 1e6,
+               "adjoint_ms_p50": float(np.median(adj))}
+        # the plain path, one matrix at a time (device pointers)
+        nloop = 256
+        f = L.plasma_dposv if dt == torch.float64 else L.plasma_sposv
+        As = [A0[b.off_a[i]:b.off_a[i] + int(n) ** 2].clone() for i, n in enumerate(sizes[:nloop])]
+        Bs = [B0[b.off_b[i]:b.off_b[i] + int(n)].clone() for i, n in enumerate(sizes[:nloop])]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i, n in enumerate(sizes[:nloop]):
+            n = int(n)
+            assert f(pb.PlasmaLower, n, 1, As[i].data_ptr(), n, Bs[i].data_ptr(), n) == 0
+        torch.cuda.synchronize()
+        loop_s = (time.perf_counter() - t0) * len(sizes) / nloop
+        row["per_matrix_loop_ms"] = loop_s * 1e3
+        row["speedup_vs_loop"] = loop_s * 1e3 / np.median(t)
+        out["results"].append(row)
+        b.close()
+    print(json.dumps(out), flush=True)
     L.plasma_finalize()
     return 0
 

@@ -54,6 +54,16 @@ long long plasma_kernel_launches(void);
  * autotuner. */
 int plasma_tuning_get_potrf_nb(int dtyp, int n);
 int plasma_tuning_set_potrf_nb(int dtyp, int n, int nb);
+/* Measured autotuning of the tables above (no reference counterpart: the
+ * reference reads nb from a Lua script).  plasma_autotune_potrf times the
+ * tile factorization of a synthetic SPD matrix of order n for nb in
+ * {128, 256, 384, 512}, stores the fastest for n's size bucket and returns
+ * it (its time in *best_ms when not NULL).  plasma_autotune_batched times
+ * batches of `count` matrices of each bucket's largest order with block
+ * widths 16 and 32 and stores the faster per bucket.  Negative returns:
+ * argument position or PlasmaError*. */
+int plasma_autotune_potrf(plasma_enum_t dtyp, int n, double *best_ms);
+int plasma_autotune_batched(plasma_enum_t dtyp, int count);
 /* Block width (16 or 32) of the batched kernels for matrices of order n. */
 int plasma_tuning_get_batched_nb(int dtyp, int n);
 int plasma_tuning_set_batched_nb(int dtyp, int n, int nb);

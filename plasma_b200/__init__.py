@@ -136,6 +136,8 @@ _SIGNATURES = [
     ("plasma_dpotrs_adjoint_batched", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("plasma_spotrs_adjoint_batched", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("plasma_tuning_get_batched_nb", c_int, [c_int, c_int]),
+    ("plasma_autotune_potrf", c_int, [c_int, c_int, POINTER(c_double)]),
+    ("plasma_autotune_batched", c_int, [c_int, c_int]),
     ("plasma_tuning_set_batched_nb", c_int, [c_int, c_int, c_int]),
     ("plasma_dpotrf_adjoint", c_int, [c_int, c_int, c_void_p, c_int, c_void_p, c_int]),
     ("plasma_spotrf_adjoint", c_int, [c_int, c_int, c_void_p, c_int, c_void_p, c_int]),

@@ -6,11 +6,11 @@
  * tuning/default.lua:125-127) and, like here, writes the answer into the
  * context's nb.  Without a script nb stays at the plasma_set value.
  *
- * The GPU build keeps a small table of tile sizes per (precision, size
- * bucket).  It starts from built-in defaults measured on B200 and can be
- * refreshed at run time by plasma_autotune_potrf(), which times the candidate
- * tile sizes {128, 256, 384, 512} on a synthetic SPD matrix and stores the
- * fastest one for that bucket.
+ * The GPU build keeps small tables of tile sizes per (precision, size
+ * bucket): nb of the tile factorization and the block width of the batched
+ * kernels.  They start from built-in defaults and are refreshed at run time
+ * by the measured autotuner (cuda/autotune.cu: plasma_autotune_potrf,
+ * plasma_autotune_batched).
  */
 #include "../internal.h"
 

@@ -456,16 +456,16 @@ struct plasma_batch_s {
     long long *h_off_a, *h_off_b;
     long long elems_a, elems_b;
     int device;
-    int graph;                  // replay launches from a cached CUDA graph
-    cudaGraphExec_t exec;
-    int g_op;
-    void *g_ptr[5];
+    int graph;                  // replay launches from cached CUDA graphs
+    cudaGraphExec_t exec[5];    // one per operation
+    void *g_ptr[5][5];          // the pointers each graph was captured with
 };
 
 static void batch_free(plasma_batch_t *p)
 {
     if (p == NULL) return;
-    if (p->exec) cudaGraphExecDestroy(p->exec);
+    for (int i = 0; i < 5; i++)
+        if (p->exec[i]) cudaGraphExecDestroy(p->exec[i]);
     cudaFree(p->d_n);
     cudaFree(p->d_off_a);
     cudaFree(p->d_off_b);
@@ -631,10 +631,10 @@ static int batch_run(plasma_batch_t *p, int prec, int op, void *A, void *B, void
 
     void *key[5] = {A, B, C, D, (void *)info};
     if (p->graph) {
-        if (p->exec == NULL || p->g_op != op || memcmp(p->g_ptr, key, sizeof(key)) != 0) {
-            if (p->exec) {
-                cudaGraphExecDestroy(p->exec);
-                p->exec = NULL;
+        if (p->exec[op] == NULL || memcmp(p->g_ptr[op], key, sizeof(key)) != 0) {
+            if (p->exec[op]) {
+                cudaGraphExecDestroy(p->exec[op]);
+                p->exec[op] = NULL;
             }
             cudaStream_t cap;
             if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess)
@@ -646,19 +646,19 @@ static int batch_run(plasma_batch_t *p, int prec, int op, void *A, void *B, void
             else launch_batched<float, 3>(cap, a, grid);
             cudaError_t rc = cudaStreamEndCapture(cap, &g);
             if (rc == cudaSuccess)
-                rc = cudaGraphInstantiate(&p->exec, g, 0);
+                rc = cudaGraphInstantiate(&p->exec[op], g, 0);
             if (g) cudaGraphDestroy(g);
             cudaStreamDestroy(cap);
             if (rc != cudaSuccess) {
                 cudaGetLastError();
-                p->exec = NULL;
+                p->exec[op] = NULL;
                 return PlasmaErrorEnvironment;
             }
-            p->g_op = op;
-            memcpy(p->g_ptr, key, sizeof(key));
+            memcpy(p->g_ptr[op], key, sizeof(key));
         }
         PLASMA_COUNT_LAUNCH();
-        return cudaGraphLaunch(p->exec, s) == cudaSuccess ? PlasmaSuccess : PlasmaErrorEnvironment;
+        return cudaGraphLaunch(p->exec[op], s) == cudaSuccess ? PlasmaSuccess
+                                                               : PlasmaErrorEnvironment;
     }
     cudaMemsetAsync(p->d_counter, 0, sizeof(int), s);
     PLASMA_COUNT_LAUNCH();

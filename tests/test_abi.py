@@ -215,3 +215,11 @@ def test_adjoint_argument_codes(hostonly):
     assert L.plasma_dpotrs_adjoint(pb.PlasmaUpper, 4, -2, None, 4, None, 4, None, 4, None, 4) == -3
     assert L.plasma_dpotrs_adjoint(pb.PlasmaUpper, 4, 1, None, 4, None, 2, None, 4, None, 4) == -7
     assert L.plasma_dpotrs_adjoint(pb.PlasmaUpper, 4, 1, None, 4, None, 4, None, 4, None, 1) == -11
+
+
+def test_autotune_argument_codes(hostonly):
+    L = hostonly
+    assert L.plasma_autotune_potrf(0, 100, None) == -1
+    assert L.plasma_autotune_potrf(pb.PlasmaRealDouble, 0, None) == -2
+    assert L.plasma_autotune_batched(pb.PlasmaRealFloat, 0) == -2
+    assert L.plasma_autotune_potrf(pb.PlasmaRealDouble, 100, None) == pb.PlasmaErrorEnvironment
