@@ -480,6 +480,8 @@ extern "C" int plasma_cuda_potrf_diag_fast(cudaStream_t s, plasma_devstat_t *st,
     int prof = plasma_prof_begin(s);
     if (A.precision == PlasmaRealDouble)
         launch_diag<double, 1>(s, st, call, A, k, iinfo);
+    else if (plasma_cuda_potrf_diag_smem(s, st, call, uplo, A, k, iinfo, g_fp32_split))
+        ;   // FP32 tile held in shared memory (potrf_smem.cu)
     else if (g_fp32_split == 1)
         launch_diag<float, 1>(s, st, call, A, k, iinfo);
     else

@@ -201,6 +201,11 @@ int plasma_cuda_update_tc(cudaStream_t s, plasma_devstat_t *st, int tc_mode,
  * tile m + mt). */
 void plasma_cuda_panel_round(cudaStream_t s, plasma_devstat_t *st, int tc_mode,
                              plasma_desc_t A, int k, void *panel);
+/* FP32 diagonal tile held in shared memory (order a multiple of 32, at most
+ * 256); 0 when not applicable. */
+int plasma_cuda_potrf_diag_smem(cudaStream_t s, plasma_devstat_t *st, int call,
+                                plasma_enum_t uplo, plasma_desc_t A, int k,
+                                int iinfo, int split);
 /* FP32 panel kernels: 3 = FP32-accurate split TF32 products, 1 = TF32. */
 void plasma_cuda_panel_set_split(int split);
 /* A(i,i) = value for i in [i0, i1) (identity padding of FP32 factors). */
