@@ -18,7 +18,8 @@
 // B operand in L2):
 //   warp 0     : TMA producer -- 4-D tensor maps over the column-major panel
 //                tiles (128-byte swizzle; 32-byte swizzle atoms for TF32, the
-//                only MN-major TF32 layout), a 3-stage ring of 48 KB stages;
+//                only MN-major TF32 layout), a ring of 48 KB stages (4 for
+//                TF32X3, 3 otherwise);
 //   warp 1     : MMA issuer -- one thread issues tcgen05.mma (M = 128, N = nb,
 //                MN-major A and B), tcgen05.commit frees a stage and, after
 //                the last k-step of an item, publishes its accumulator;
@@ -48,11 +49,7 @@ constexpr int TC_THREADS = 384;          // 12 warps
 constexpr int TC_EPI_WARP0 = 4;
 constexpr int TC_EPI_WARPS = 8;
 constexpr int TC_STAGE_BYTES = 48 * 1024;
-constexpr int TC_STAGES = 3;
-constexpr int TC_EPI_BUFS = 2;           // staging buffers per epilogue warp
 constexpr int TC_EPI_BUF_BYTES = 32 * 32 * 4;
-constexpr int TC_SMEM = TC_STAGES * TC_STAGE_BYTES +
-                        TC_EPI_WARPS * TC_EPI_BUFS * TC_EPI_BUF_BYTES + 1024;
 
 enum { MODE_TF32 = PLASMA_TC_TF32, MODE_BF16 = PLASMA_TC_BF16,
        MODE_TF32X3 = PLASMA_TC_TF32X3 };
@@ -68,6 +65,12 @@ struct Geo {
     static constexpr uint32_t SBO = MODE == MODE_BF16 ? 1024u : 512u;
     static constexpr int CHUNK = BK * 128;            // one MN chunk of a stage
     static constexpr int A_BYTES = (TC_M / MNBOX) * CHUNK;
+    // TF32X3 moves twice the operand bytes per product: a deeper ring (more
+    // bytes in flight against the L2 latency), one epilogue buffer per warp
+    static constexpr int STAGES = MODE == MODE_TF32X3 ? 4 : 3;
+    static constexpr int EPI_BUFS = MODE == MODE_TF32X3 ? 1 : 2;
+    static constexpr int SMEM = STAGES * TC_STAGE_BYTES +
+                                TC_EPI_WARPS * EPI_BUFS * TC_EPI_BUF_BYTES + 1024;
 };
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar, int count)
@@ -247,6 +250,8 @@ k_update_tc(const __grid_constant__ CUtensorMap opmap,
 {
     using G = Geo<MODE>;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
+    constexpr int TC_STAGES = G::STAGES;
+    constexpr int TC_EPI_BUFS = G::EPI_BUFS;
     __shared__ uint64_t full_bar[TC_STAGES], empty_bar[TC_STAGES];
     __shared__ uint64_t tfull_bar[2], tempty_bar[2];
     __shared__ uint32_t tmem_base_s;
@@ -500,10 +505,10 @@ void launch_update(cudaStream_t s, const CUtensorMap &map, const CUtensorMap &cm
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_update_tc<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             TC_SMEM);
+                             Geo<MODE>::SMEM);
         attr = true;
     }
-    k_update_tc<MODE><<<grid, TC_THREADS, TC_SMEM, s>>>(map, cmap, g, st);
+    k_update_tc<MODE><<<grid, TC_THREADS, Geo<MODE>::SMEM, s>>>(map, cmap, g, st);
 }
 
 }  // namespace
