@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-dposv", action="store_true")
+    p.add_argument("--batch-count", type=int, default=4096,
+                   help="matrices of the batched workload")
     p.add_argument("--workload", default="dsposv", choices=["dsposv", "adjoint", "batched"],
                    help="dsposv: the headline; adjoint / batched: the differentiation "
                         "and batched-solve configurations, one JSON line each")
@@ -309,7 +311,7 @@ def run_batched(args):
     L = pb.lib()
     assert L.plasma_init() == 0
     rng = np.random.default_rng(5)
-    sizes = rng.integers(16, 513, 4096)
+    sizes = rng.integers(16, 513, args.batch_count)
     out = {"workload": "batched", "metric": "batched SPD solves (uneven n in [16, 512])",
            "unit": "systems/s", "batch": len(sizes), "steps": args.steps,
            "warmup": args.warmup, "flops_per_batch": float(np.sum(sizes.astype(float) ** 3) / 3),
@@ -356,7 +358,7 @@ def run_batched(args):
                "gflops": out["flops_per_batch"] / np.median(t) / 1e6,
                "adjoint_ms_p50": float(np.median(adj))}
         # the plain path, one matrix at a time (device pointers)
-        nloop = 256
+        nloop = min(256, len(sizes))
         f = L.plasma_dposv if dt == torch.float64 else L.plasma_sposv
         As = [A0[b.off_a[i]:b.off_a[i] + int(n) ** 2].clone() for i, n in enumerate(sizes[:nloop])]
         Bs = [B0[b.off_b[i]:b.off_b[i] + int(n)].clone() for i, n in enumerate(sizes[:nloop])]

@@ -191,28 +191,35 @@ __device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag)
 
 // ------------------------------------------------------------------- solve
 // b <- A^-1 b with the factor L in the lower triangle of A (n x n, ld n).
+// Each 32 x 32 diagonal block is first staged in shared memory (one parallel
+// load), so the warp's substitution reads shared memory only.
 template <typename T>
-__device__ void solve_one(const T *A, int n, T *b, T *Ys)
+__device__ void solve_one(const T *A, int n, T *b, T *Ys, T *Db)
 {
-    constexpr int NB = 32;
+    constexpr int NB = 32, DLD = NB + 1;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int i = tid; i < n; i += BT) Ys[i] = b[i];
-    __syncthreads();
     // forward: L y = b
     for (int j0 = 0; j0 < n; j0 += NB) {
         const int jb = min(NB, n - j0);
+        for (int e = tid; e < NB * NB; e += BT) {
+            const int r = e % NB, c = e / NB;
+            Db[c * DLD + r] = (r < jb && c < jb && r >= c) ? A[(size_t)(j0 + c) * n + j0 + r] : T(0);
+        }
+        __syncthreads();
         if (warp == 0) {
             T y = lane < jb ? Ys[j0 + lane] : T(0);
             for (int c = 0; c < jb; c++) {
-                if (lane == c) y = y / A[(size_t)(j0 + c) * n + j0 + c];
+                if (lane == c) y = y / Db[c * DLD + c];
                 const T yc = __shfl_sync(0xffffffffu, y, c);
-                if (lane > c && lane < jb) y -= A[(size_t)(j0 + c) * n + j0 + lane] * yc;
+                if (lane > c && lane < jb) y -= Db[c * DLD + lane] * yc;
             }
             if (lane < jb) Ys[j0 + lane] = y;
         }
         __syncthreads();
         for (int r = j0 + jb + tid; r < n; r += BT) {
             T s = Ys[r];
+#pragma unroll 8
             for (int c = 0; c < jb; c++) s -= A[(size_t)(j0 + c) * n + r] * Ys[j0 + c];
             Ys[r] = s;
         }
@@ -221,6 +228,10 @@ __device__ void solve_one(const T *A, int n, T *b, T *Ys)
     // backward: L^T x = y
     for (int j0 = ((n - 1) / NB) * NB; j0 >= 0; j0 -= NB) {
         const int jb = min(NB, n - j0);
+        for (int e = tid; e < NB * NB; e += BT) {
+            const int r = e % NB, c = e / NB;
+            Db[c * DLD + r] = (r < jb && c < jb && r >= c) ? A[(size_t)(j0 + c) * n + j0 + r] : T(0);
+        }
         for (int c = warp; c < jb; c += BT / 32) {
             T s = T(0);
             for (int i = j0 + jb + lane; i < n; i += 32) s += A[(size_t)(j0 + c) * n + i] * Ys[i];
@@ -232,9 +243,9 @@ __device__ void solve_one(const T *A, int n, T *b, T *Ys)
         if (warp == 0) {
             T x = lane < jb ? Ys[j0 + lane] : T(0);
             for (int c = jb - 1; c >= 0; c--) {
-                if (lane == c) x = x / A[(size_t)(j0 + c) * n + j0 + c];
+                if (lane == c) x = x / Db[c * DLD + c];
                 const T xc = __shfl_sync(0xffffffffu, x, c);
-                if (lane < c) x -= A[(size_t)(j0 + lane) * n + j0 + c] * xc;
+                if (lane < c) x -= Db[lane * DLD + c] * xc;
             }
             if (lane < jb) Ys[j0 + lane] = x;
         }
@@ -248,10 +259,10 @@ __device__ void solve_one(const T *A, int n, T *b, T *Ys)
 // xbar <- A^-1 xbar (= bbar); Lbar -= tril(bbar (L^T x)^T + x (L^T bbar)^T)
 template <typename T>
 __device__ void solve_adjoint_one(const T *Lf, int n, const T *x, T *xbar, T *Lbar, T *Ys,
-                                  T *U)
+                                  T *U, T *Db)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    solve_one<T>(Lf, n, xbar, Ys);                 // Ys keeps bbar
+    solve_one<T>(Lf, n, xbar, Ys, Db);             // Ys keeps bbar
     T *u1 = U, *u2 = U + NMAX;                     // L^T x, L^T bbar
     for (int c = warp; c < n; c += BT / 32) {
         T s1 = T(0), s2 = T(0);
@@ -418,12 +429,12 @@ k_batched(BatchArgs a)
                                               : factor_one<T, SPLIT, 32>(A, n, Ps, Ds, rdiag, &flag_s);
             if (tid == 0) a.info[m] = info;
             __syncthreads();
-            if (info == 0 && a.op == OP_POSV) solve_one<T>(A, n, (T *)a.B + a.off_b[m], Ys);
+            if (info == 0 && a.op == OP_POSV) solve_one<T>(A, n, (T *)a.B + a.off_b[m], Ys, D2);
         } else if (a.op == OP_POTRS) {
-            solve_one<T>(A, n, (T *)a.B + a.off_b[m], Ys);
+            solve_one<T>(A, n, (T *)a.B + a.off_b[m], Ys, D2);
         } else if (a.op == OP_POTRS_ADJ) {
             solve_adjoint_one<T>(A, n, (const T *)a.B + a.off_b[m], (T *)a.C + a.off_b[m],
-                                 (T *)a.D + a.off_a[m], Ys, Ps);
+                                 (T *)a.D + a.off_a[m], Ys, Ps, D2);
         } else {
             factor_adjoint_one<T>(A, n, (T *)a.D + a.off_a[m], Ps, Ds, D2);
         }
