@@ -86,8 +86,9 @@ __device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag)
                     T d = __shfl_sync(0xffffffffu, v[c], c);
                     bool ok = d > T(0);
                     if (!ok && bad == 0) bad = c + 1;
-                    T sd = ok ? sqrt(d) : T(1);
-                    T rd = T(1) / sd;
+                    // one reciprocal square root per pivot: 1/sqrt(d), sqrt(d) = d/sqrt(d)
+                    T rd = ok ? rsqrt(d) : T(1);
+                    T sd = ok ? d * rd : T(1);
                     if (lane == c) myrd = rd;
                     if (lane >= c) v[c] = (lane == c) ? sd : v[c] * rd;
 #pragma unroll
@@ -194,7 +195,7 @@ __device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag)
 // Each 32 x 32 diagonal block is first staged in shared memory (one parallel
 // load), so the warp's substitution reads shared memory only.
 template <typename T>
-__device__ void solve_one(const T *A, int n, T *b, T *Ys, T *Db)
+__device__ void solve_one(const T *A, int n, T *b, T *Ys, T *Db, T *Dr)
 {
     constexpr int NB = 32, DLD = NB + 1;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -206,11 +207,12 @@ __device__ void solve_one(const T *A, int n, T *b, T *Ys, T *Db)
             const int r = e % NB, c = e / NB;
             Db[c * DLD + r] = (r < jb && c < jb && r >= c) ? A[(size_t)(j0 + c) * n + j0 + r] : T(0);
         }
+        if (tid < jb) Dr[tid] = T(1) / A[(size_t)(j0 + tid) * n + j0 + tid];
         __syncthreads();
         if (warp == 0) {
             T y = lane < jb ? Ys[j0 + lane] : T(0);
             for (int c = 0; c < jb; c++) {
-                if (lane == c) y = y / Db[c * DLD + c];
+                if (lane == c) y = y * Dr[c];
                 const T yc = __shfl_sync(0xffffffffu, y, c);
                 if (lane > c && lane < jb) y -= Db[c * DLD + lane] * yc;
             }
@@ -232,6 +234,7 @@ __device__ void solve_one(const T *A, int n, T *b, T *Ys, T *Db)
             const int r = e % NB, c = e / NB;
             Db[c * DLD + r] = (r < jb && c < jb && r >= c) ? A[(size_t)(j0 + c) * n + j0 + r] : T(0);
         }
+        if (tid < jb) Dr[tid] = T(1) / A[(size_t)(j0 + tid) * n + j0 + tid];
         for (int c = warp; c < jb; c += BT / 32) {
             T s = T(0);
             for (int i = j0 + jb + lane; i < n; i += 32) s += A[(size_t)(j0 + c) * n + i] * Ys[i];
@@ -243,7 +246,7 @@ __device__ void solve_one(const T *A, int n, T *b, T *Ys, T *Db)
         if (warp == 0) {
             T x = lane < jb ? Ys[j0 + lane] : T(0);
             for (int c = jb - 1; c >= 0; c--) {
-                if (lane == c) x = x / Db[c * DLD + c];
+                if (lane == c) x = x * Dr[c];
                 const T xc = __shfl_sync(0xffffffffu, x, c);
                 if (lane < c) x -= Db[lane * DLD + c] * xc;
             }
@@ -259,10 +262,10 @@ __device__ void solve_one(const T *A, int n, T *b, T *Ys, T *Db)
 // xbar <- A^-1 xbar (= bbar); Lbar -= tril(bbar (L^T x)^T + x (L^T bbar)^T)
 template <typename T>
 __device__ void solve_adjoint_one(const T *Lf, int n, const T *x, T *xbar, T *Lbar, T *Ys,
-                                  T *U, T *Db)
+                                  T *U, T *Db, T *Dr)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    solve_one<T>(Lf, n, xbar, Ys, Db);             // Ys keeps bbar
+    solve_one<T>(Lf, n, xbar, Ys, Db, Dr);         // Ys keeps bbar
     T *u1 = U, *u2 = U + NMAX;                     // L^T x, L^T bbar
     for (int c = warp; c < n; c += BT / 32) {
         T s1 = T(0), s2 = T(0);
@@ -429,12 +432,12 @@ k_batched(BatchArgs a)
                                               : factor_one<T, SPLIT, 32>(A, n, Ps, Ds, rdiag, &flag_s);
             if (tid == 0) a.info[m] = info;
             __syncthreads();
-            if (info == 0 && a.op == OP_POSV) solve_one<T>(A, n, (T *)a.B + a.off_b[m], Ys, D2);
+            if (info == 0 && a.op == OP_POSV) solve_one<T>(A, n, (T *)a.B + a.off_b[m], Ys, D2, rdiag);
         } else if (a.op == OP_POTRS) {
-            solve_one<T>(A, n, (T *)a.B + a.off_b[m], Ys, D2);
+            solve_one<T>(A, n, (T *)a.B + a.off_b[m], Ys, D2, rdiag);
         } else if (a.op == OP_POTRS_ADJ) {
             solve_adjoint_one<T>(A, n, (const T *)a.B + a.off_b[m], (T *)a.C + a.off_b[m],
-                                 (T *)a.D + a.off_a[m], Ys, Ps, D2);
+                                 (T *)a.D + a.off_a[m], Ys, Ps, D2, rdiag);
         } else {
             factor_adjoint_one<T>(A, n, (T *)a.D + a.off_a[m], Ps, Ds, D2);
         }
