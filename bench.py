@@ -433,12 +433,16 @@ def main():
     l0 = pb.launches()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     e0.record()
-    for _ in range(args.steps):
+    marks[0].record()
+    for i in range(args.steps):
         dsposv()
+        marks[i + 1].record()
     e1.record()
     barrier()
     ms = e0.elapsed_time(e1) / args.steps
+    step_ms = [marks[i].elapsed_time(marks[i + 1]) for i in range(args.steps)]
     launches = pb.launches() - l0
     prof = {k: pb.profile_query(k) for k in pb.KCLASS}
     pb.profile_enable(False)
@@ -565,6 +569,7 @@ def main():
                    "nb": args.nb or L.plasma_tuning_get_potrf_nb(pb.PlasmaRealFloat, n),
                    "l2": "inputs larger than L2 (A is 8.6 GB)",
                    "parallelism": f"replicas x{world}"},
+        "step_ms": step_ms,
         "iter": iters, "backward_error": berr, "forward_error": ferr,
         "backward_error_target": 50 * n * 2.0 ** -53,
         "dposv": dposv,

@@ -41,6 +41,7 @@
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
+#include <stdlib.h>
 
 namespace {
 
@@ -585,9 +586,17 @@ extern "C" int plasma_cuda_update_tc(cudaStream_t s, plasma_devstat_t *st,
     // waves * (ipc + 1/2) items -- a CTA's pipeline fill and its last,
     // unoverlapped epilogue cost about half an item -- ties to the larger
     // ipc (the SMs left over serve the panel stream).
+    // PLASMA_UPDATE_MAX_ITEMS caps the items per CTA (default 8): shorter
+    // CTAs hand SMs back to the panel stream sooner
+    static int max_items = -1;
+    if (max_items < 0) {
+        const char *env = getenv("PLASMA_UPDATE_MAX_ITEMS");
+        max_items = env ? atoi(env) : 8;
+        if (max_items < 1 || max_items > 64) max_items = 8;
+    }
     const long long sms = num_sms > 0 ? num_sms : 148;
     long long best_ipc = 1, best_cost = -1;
-    for (long long ipc = 1; ipc <= 8; ipc++) {
+    for (long long ipc = 1; ipc <= max_items; ipc++) {
         const long long ctas = (nitems + ipc - 1) / ipc;
         const long long cost = ((ctas + sms - 1) / sms) * (2 * ipc + 1);
         if (best_cost < 0 || cost <= best_cost) {
