@@ -51,6 +51,25 @@ __device__ __forceinline__ T *out_ptr(const View &v, int i, int j)
     return t + (size_t)(gc - tn * v.D.nb) * plasma_tile_mmain(v.D, tm) + (gr - tm * v.D.mb);
 }
 
+// A block of op(V) at (i0, k0) spanning si x sk elements: when it lies in one
+// storage tile, element (ii, kk) is base[ii * di + kk * dk] (returns true).
+template <typename T>
+__device__ __forceinline__ bool block_base(const View &v, int i0, int k0, int si, int sk,
+                                           const T *&base, int &di, int &dk)
+{
+    // block of D: rows [r, r + sr), columns [c, c + sc)
+    const int r = v.r0 + (v.trans ? k0 : i0), c = v.c0 + (v.trans ? i0 : k0);
+    const int sr = v.trans ? sk : si, sc = v.trans ? si : sk;
+    const int tm = r / v.D.mb, tn = c / v.D.nb;
+    const int rr = r - tm * v.D.mb, cc = c - tn * v.D.nb;
+    if (rr + sr > v.D.mb || cc + sc > v.D.nb) return false;
+    const int ld = plasma_tile_mmain(v.D, tm);
+    base = (const T *)plasma_tile_addr(v.D, tm, tn) + (size_t)cc * ld + rr;
+    di = v.trans ? ld : 1;
+    dk = v.trans ? 1 : ld;
+    return true;
+}
+
 // K range [kb, ke) in which op(A)(i, k) op(B)(k, j) can be non-zero for
 // i in [i0, i1), j in [j0, j1)
 __device__ __forceinline__ void k_range(const View &a, const View &b, int K, int i0,
@@ -95,30 +114,50 @@ k_gemm_view(int M, int N, int K, T alpha, View A, View B, T beta, View C,
     int kb, ke;
     k_range(A, B, K, i0, i1, j0, j1, kb, ke);
     if (all_out) ke = kb;
+    // masks in the coordinates of the untransposed view
+    auto masked = [](const View &v, int i, int k) {
+        const int r = v.trans ? k : i, c = v.trans ? i : k;
+        return (v.tri == 1 && r < c) || (v.tri == 2 && r > c);
+    };
+    auto halved = [](const View &v, int i, int k) { return v.diag_scale && i == k; };
     auto stage = [&](int k0, int buf) {
+        const T *ba, *bb;
+        int dia, dka, dib, dkb;
+        const bool fa = block_base<T>(A, i0, k0, GM, GK, ba, dia, dka);
+        // op(B)(k, j): first index k, second j
+        const bool fb = block_base<T>(B, k0, j0, GK, GN, bb, dib, dkb);
         for (int e = tid; e < GK * GM; e += GTHREADS) {
             const int ii = e % GM, kk = e / GM;
             const int i = i0 + ii, k = k0 + kk;
-            bool zero = true, half = false;
-            const T *p = (i < M && k < ke) ? view_ptr<T>(A, i, k, zero, half) : nullptr;
-            if (p == nullptr) zero = true;
-            if (half && !zero) {
-                As[buf][kk][ii] = T(0.5) * *p;
-            } else {
-                cp_async_el(&As[buf][kk][ii], zero ? (const T *)A.D.matrix : p, !zero);
+            const bool in = i < M && k < ke && !masked(A, i, k);
+            const T *p = (const T *)A.D.matrix;
+            if (in) {
+                if (fa) {
+                    p = ba + (size_t)ii * dia + (size_t)kk * dka;
+                } else {
+                    bool z, h;
+                    p = view_ptr<T>(A, i, k, z, h);
+                }
             }
+            if (in && halved(A, i, k)) As[buf][kk][ii] = T(0.5) * *p;
+            else cp_async_el(&As[buf][kk][ii], p, in);
         }
         for (int e = tid; e < GK * GN; e += GTHREADS) {
             const int jj = e % GN, kk = e / GN;
             const int j = j0 + jj, k = k0 + kk;
-            bool zero = true, half = false;
-            const T *p = (j < N && k < ke) ? view_ptr<T>(B, k, j, zero, half) : nullptr;
-            if (p == nullptr) zero = true;
-            if (half && !zero) {
-                Bs[buf][kk][jj] = T(0.5) * *p;
-            } else {
-                cp_async_el(&Bs[buf][kk][jj], zero ? (const T *)B.D.matrix : p, !zero);
+            // op(B)(k, j): the view's "row" index is k
+            const bool in = j < N && k < ke && !masked(B, k, j);
+            const T *p = (const T *)B.D.matrix;
+            if (in) {
+                if (fb) {
+                    p = bb + (size_t)kk * dib + (size_t)jj * dkb;
+                } else {
+                    bool z, h;
+                    p = view_ptr<T>(B, k, j, z, h);
+                }
             }
+            if (in && halved(B, k, j)) Bs[buf][kk][jj] = T(0.5) * *p;
+            else cp_async_el(&Bs[buf][kk][jj], p, in);
         }
         cp_async_commit();
     };
@@ -257,10 +296,13 @@ extern "C" void plasma_cuda_copy_view(cudaStream_t s, plasma_devstat_t *st, int 
     if (M <= 0 || N <= 0) return;
     dim3 grid((N + 31) / 32, (M + 31) / 32);
     PLASMA_COUNT_LAUNCH();
+    int prof = plasma_prof_begin(s);
     if (dst.D.precision == PlasmaRealDouble)
         k_copy_view<double><<<grid, 256, 0, s>>>(M, N, src, dst, st);
     else
         k_copy_view<float><<<grid, 256, 0, s>>>(M, N, src, dst, st);
+    plasma_prof_end(prof, s, PLASMA_KCLASS_AUX, 0.0,
+                    2.0 * M * N * plasma_element_size(dst.D.precision));
 }
 
 extern "C" void plasma_cuda_symmetrize(cudaStream_t s, plasma_devstat_t *st, int n,
@@ -269,8 +311,11 @@ extern "C" void plasma_cuda_symmetrize(cudaStream_t s, plasma_devstat_t *st, int
     if (n <= 0) return;
     dim3 grid((n + 31) / 32, (n + 31) / 32);
     PLASMA_COUNT_LAUNCH();
+    int prof = plasma_prof_begin(s);
     if (dst.D.precision == PlasmaRealDouble)
         k_symmetrize<double><<<grid, 256, 0, s>>>(n, src, dst, st);
     else
         k_symmetrize<float><<<grid, 256, 0, s>>>(n, src, dst, st);
+    plasma_prof_end(prof, s, PLASMA_KCLASS_AUX, 0.0,
+                    3.0 * (double)n * n * plasma_element_size(dst.D.precision));
 }

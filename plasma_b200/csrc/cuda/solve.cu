@@ -13,6 +13,8 @@
 // The sweeps are HBM bound: each reads the triangle of the factor once.
 #include "common.cuh"
 
+#include <string.h>
+
 namespace {
 
 constexpr int kCols = 16;        // right-hand sides per CTA
@@ -115,6 +117,9 @@ void sweep(cudaStream_t s, plasma_devstat_t *st, int uplo, int trans,
                              200 * 1024);
         attr_set = true;
     }
+    // many right-hand sides: the update of a step is one tensor-core GEMM on
+    // views of the factor and of B (cuda/adjoint.cu, k_gemm_view)
+    const bool gemm = B.n >= 64 && A.mb == B.mb;
     for (int step = 0; step < mt; step++) {
         int k = trans ? mt - 1 - step : step;
         PLASMA_COUNT_LAUNCH();
@@ -122,7 +127,32 @@ void sweep(cudaStream_t s, plasma_devstat_t *st, int uplo, int trans,
             B, k, W, nbw, trans, st);
         int mlo = trans ? 0 : k + 1;
         int mhi = trans ? k : mt;
-        if (mhi > mlo) {
+        if (gemm && mhi > mlo) {
+            const int mb = B.mb, kr = plasma_tile_mview(B, k);
+            plasma_view_t lv, bv, cv;
+            memset(&lv, 0, sizeof(lv));
+            memset(&bv, 0, sizeof(bv));
+            memset(&cv, 0, sizeof(cv));
+            lv.D = A;
+            bv.D = B;
+            bv.r0 = k * mb;
+            cv.D = B;
+            int M;
+            if (!trans) {
+                // B(k+1.., :) -= L(k+1.., k) B(k, :)
+                M = B.m - (k + 1) * mb;
+                cv.r0 = (k + 1) * mb;
+                if (uplo == PlasmaLower) { lv.r0 = (k + 1) * mb; lv.c0 = k * mb; lv.trans = 0; }
+                else { lv.r0 = k * mb; lv.c0 = (k + 1) * mb; lv.trans = 1; }
+            } else {
+                // B(0..k, :) -= L(k, 0..k)^T B(k, :)
+                M = k * mb;
+                cv.r0 = 0;
+                if (uplo == PlasmaLower) { lv.r0 = k * mb; lv.c0 = 0; lv.trans = 1; }
+                else { lv.r0 = 0; lv.c0 = k * mb; lv.trans = 0; }
+            }
+            plasma_cuda_gemm_view(s, st, M, B.n, kr, -1.0, lv, bv, 1.0, cv, 0, 0);
+        } else if (mhi > mlo) {
             PLASMA_COUNT_LAUNCH();
             k_solve_update<T><<<dim3(mhi - mlo, B.nt, chunks), kThreads, smem, s>>>(
                 A, uplo, B, k, mlo, trans, st);

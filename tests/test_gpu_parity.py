@@ -488,3 +488,19 @@ def test_dsposv_anorm_tile_pass(L, uplo, n, nb):
     ref = np.abs(a).sum(axis=1).max()
     assert abs(info.anorm - ref) <= 1e-13 * ref
     assert solve_residual(a, x, b) < TOL * EPS
+
+
+@pytest.mark.parametrize("uplo", [LO, UP])
+def test_dposv_many_rhs(L, uplo):
+    """nrhs >= 64: the sweeps' tile updates run as tensor-core GEMMs on views
+    of the factor; compare with the oracle and check the tester's residual."""
+    set_nb(L, 128)
+    n, nrhs = 700, 100
+    a, b = gen.diag_dominant(n, nrhs, seed=1700)
+    x = np.asfortranarray(b.copy())
+    assert L.plasma_dposv(uplo, n, nrhs, np.asfortranarray(a.copy()).ctypes.data, n,
+                          x.ctypes.data, n) == 0
+    assert solve_residual(a, x, b) < TOL * EPS
+    xo = np.asfortranarray(b.copy())
+    assert oracle.posv(uplo, np.asfortranarray(a.copy()), xo, 128) == 0
+    np.testing.assert_allclose(x, xo, rtol=1e-11, atol=1e-14)
