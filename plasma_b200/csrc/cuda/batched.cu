@@ -91,10 +91,13 @@ __device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag)
                     T sd = ok ? d * rd : T(1);
                     if (lane == c) myrd = rd;
                     if (lane >= c) v[c] = (lane == c) ? sd : v[c] * rd;
+                    // a fixed trip count keeps v[] in registers (full unroll)
 #pragma unroll
-                    for (int c2 = c + 1; c2 < NB; c2++) {
-                        T l = __shfl_sync(0xffffffffu, v[c], c2);
-                        if (c2 < jb && lane >= c2) v[c2] -= v[c] * l;
+                    for (int c2 = 0; c2 < NB; c2++) {
+                        if (c2 > c) {
+                            T l = __shfl_sync(0xffffffffu, v[c], c2);
+                            if (c2 < jb && lane >= c2) v[c2] -= v[c] * l;
+                        }
                     }
                 }
             }

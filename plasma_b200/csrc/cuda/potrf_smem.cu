@@ -81,10 +81,13 @@ k_potrf_diag_smem(plasma_desc_t A, int k, int iinfo, plasma_devstat_t *st, int c
                 const float rd = 1.f / sd;
                 if (lane == c) myrd = rd;
                 if (lane >= c) v[c] = lane == c ? sd : v[c] * rd;
+                // a fixed trip count keeps v[] in registers (full unroll)
 #pragma unroll
-                for (int c2 = c + 1; c2 < 32; c2++) {
-                    const float l = __shfl_sync(0xffffffffu, v[c], c2);
-                    if (lane >= c2) v[c2] -= v[c] * l;
+                for (int c2 = 0; c2 < 32; c2++) {
+                    if (c2 > c) {
+                        const float l = __shfl_sync(0xffffffffu, v[c], c2);
+                        if (lane >= c2) v[c2] -= v[c] * l;
+                    }
                 }
             }
 #pragma unroll
@@ -103,12 +106,13 @@ k_potrf_diag_smem(plasma_desc_t A, int k, int iinfo, plasma_devstat_t *st, int c
             float x[32];
 #pragma unroll
             for (int c = 0; c < 32; c++) x[c] = P[c * ld + rr];
+            // column-oriented substitution: x_c final, then its multiple of
+            // column c of the block leaves the later entries
 #pragma unroll
             for (int c = 0; c < 32; c++) {
-                float s = x[c];
+                x[c] *= rdiag[c];
 #pragma unroll
-                for (int c2 = 0; c2 < c; c2++) s -= x[c2] * P[c2 * ld + c];
-                x[c] = s * rdiag[c];
+                for (int c2 = c + 1; c2 < 32; c2++) x[c2] -= x[c] * P[c * ld + c2];
             }
 #pragma unroll
             for (int c = 0; c < 32; c++) P[c * ld + rr] = x[c];

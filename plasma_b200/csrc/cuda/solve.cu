@@ -53,8 +53,9 @@ k_diag_apply(plasma_desc_t B, int k, const T *W, int nbw, int trans,
 #pragma unroll
             for (int j = 0; j < kCols; j++) acc[j] += wv * Bs[c][j];
         }
-        for (int j = 0; j < cols; j++)
-            b[(size_t)(c0 + j) * ldb + i] = acc[j];
+#pragma unroll
+        for (int j = 0; j < kCols; j++)
+            if (j < cols) b[(size_t)(c0 + j) * ldb + i] = acc[j];
     }
 }
 
@@ -94,8 +95,9 @@ k_solve_update(plasma_desc_t A, int uplo, plasma_desc_t B, int k, int mlo,
 #pragma unroll
             for (int j = 0; j < kCols; j++) acc[j] += lv * Ys[c][j];
         }
-        for (int j = 0; j < cols; j++)
-            b[(size_t)(c0 + j) * ldb + i] -= acc[j];
+#pragma unroll
+        for (int j = 0; j < kCols; j++)
+            if (j < cols) b[(size_t)(c0 + j) * ldb + i] -= acc[j];
     }
 }
 

@@ -35,7 +35,7 @@ typedef struct {
 
 #define PLASMA_MAX_PENDING_CALLS 4096
 #define PLASMA_NUM_STREAMS 4
-#define PLASMA_SCRATCH_SLOTS 7
+#define PLASMA_SCRATCH_SLOTS 9
 
 /* scratch slots */
 enum {
@@ -45,7 +45,9 @@ enum {
     PLASMA_SLOT_MIXED   = 3,   /* low-precision operand copies (dsposv)       */
     PLASMA_SLOT_REFINE  = 4,   /* refinement vectors and Krylov basis         */
     PLASMA_SLOT_SYMV    = 5,   /* per-tile partial products of the residual   */
-    PLASMA_SLOT_ADJOINT = 6    /* n x n work matrices of the adjoints         */
+    PLASMA_SLOT_ADJOINT = 6,   /* n x n work matrices of the adjoints         */
+    PLASMA_SLOT_DESC_A  = 7,   /* dsposv's FP64 tile copy of A (kept)         */
+    PLASMA_SLOT_DESC_AS = 8    /* dsposv's FP32 tile copy of A (kept)         */
 };
 
 typedef struct {
