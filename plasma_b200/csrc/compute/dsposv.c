@@ -550,22 +550,11 @@ int plasma_dsposv_ex(plasma_enum_t uplo, int n, int nrhs,
      * neither allocates nor frees its two large tile copies; zeroed on the
      * stream (the padding of As and the unreferenced halves of diagonal
      * tiles must hold finite values) */
-    const size_t tiles_a = (size_t)((n + nb - 1) / nb) * ((n + nb - 1) / nb + 1) / 2;
-    const size_t tiles_as = (size_t)(npad / nb) * (npad / nb + 1) / 2;
-    void *buf_a = plasma_scratch(plasma, PLASMA_SLOT_DESC_A,
-                                 tiles_a * nb * nb * sizeof(double));
-    void *buf_as = plasma_scratch(plasma, PLASMA_SLOT_DESC_AS,
-                                  tiles_as * nb * nb * sizeof(float));
-    if (buf_a == NULL || buf_as == NULL)
-        return PlasmaErrorOutOfMemory;
-    plasma_desc_triangular_init(PlasmaRealDouble, uplo, buf_a, nb, nb, n, n, 0, 0, n, n, &A);
-    plasma_desc_triangular_init(PlasmaRealFloat, uplo, buf_as, nb, nb, npad, npad, 0, 0,
-                                npad, npad, &As);
-    if (plasma_desc_storage_bytes(A) > tiles_a * nb * nb * sizeof(double) ||
-        plasma_desc_storage_bytes(As) > tiles_as * nb * nb * sizeof(float))
-        return PlasmaErrorInternal;
-    cudaMemsetAsync(buf_a, 0, plasma_desc_storage_bytes(A), plasma->stream);
-    cudaMemsetAsync(buf_as, 0, plasma_desc_storage_bytes(As), plasma->stream);
+    if ((retval = plasma_desc_kept(plasma, PLASMA_SLOT_DESC_A, PlasmaRealDouble, uplo, nb, n,
+                                   n, &A)) != 0 ||
+        (retval = plasma_desc_kept(plasma, PLASMA_SLOT_DESC_AS, PlasmaRealFloat, uplo, nb,
+                                   npad, npad, &As)) != 0)
+        return retval;
     if ((retval = plasma_desc_general_create(PlasmaRealDouble, nb, nb, n, nrhs,
                                              0, 0, n, nrhs, &B)) != 0 ||
         (retval = plasma_desc_general_create(PlasmaRealDouble, nb, nb, n, nrhs,

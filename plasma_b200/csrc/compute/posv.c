@@ -159,14 +159,14 @@ static int Xpotrs(plasma_enum_t prec, plasma_enum_t uplo, int n, int nrhs,
     int nb = plasma->nb;
 
     plasma_desc_t A, B;
-    int retval = plasma_desc_general_create(prec, nb, nb, n, n, 0, 0, n, n, &A);
+    /* the tile copy of A lives in a slot the context keeps between calls */
+    int retval = plasma_desc_kept(plasma, PLASMA_SLOT_DESC_A, prec, PlasmaGeneral, nb, n, n,
+                                  &A);
     if (retval != PlasmaSuccess)
         return retval;
     retval = plasma_desc_general_create(prec, nb, nb, n, nrhs, 0, 0, n, nrhs, &B);
-    if (retval != PlasmaSuccess) {
-        plasma_desc_destroy(&A);
+    if (retval != PlasmaSuccess)
         return retval;
-    }
     plasma_sequence_t sequence;
     plasma_request_t request;
     plasma_sequence_init(&sequence);
@@ -180,7 +180,6 @@ static int Xpotrs(plasma_enum_t prec, plasma_enum_t uplo, int n, int nrhs,
     plasma_omp_Xdesc2lapack(B, pB, ldb, PlasmaGeneral, &sequence, &request);
     plasma_sequence_wait(&sequence);
 
-    plasma_desc_destroy(&A);
     plasma_desc_destroy(&B);
     return sequence.status;
 }
@@ -203,15 +202,13 @@ static int Xposv(plasma_enum_t prec, plasma_enum_t uplo, int n, int nrhs,
     int nb = plasma->nb;
 
     plasma_desc_t A, B;
-    int retval = plasma_desc_triangular_create(prec, uplo, nb, nb, n, n, 0, 0,
-                                               n, n, &A);
+    /* the tile copy of A lives in a slot the context keeps between calls */
+    int retval = plasma_desc_kept(plasma, PLASMA_SLOT_DESC_A, prec, uplo, nb, n, n, &A);
     if (retval != PlasmaSuccess)
         return retval;
     retval = plasma_desc_general_create(prec, nb, nb, n, nrhs, 0, 0, n, nrhs, &B);
-    if (retval != PlasmaSuccess) {
-        plasma_desc_destroy(&A);
+    if (retval != PlasmaSuccess)
         return retval;
-    }
     plasma_sequence_t sequence;
     plasma_request_t request;
     plasma_sequence_init(&sequence);
@@ -225,7 +222,6 @@ static int Xposv(plasma_enum_t prec, plasma_enum_t uplo, int n, int nrhs,
     plasma_omp_Xdesc2lapack(B, pB, ldb, PlasmaGeneral, &sequence, &request);
     plasma_sequence_wait(&sequence);
 
-    plasma_desc_destroy(&A);
     plasma_desc_destroy(&B);
     return sequence.status;
 }

@@ -91,10 +91,10 @@ static int Xpotrf(plasma_enum_t prec, plasma_enum_t uplo, int n, void *pA,
     int nb = plasma->nb;
 
     plasma_desc_t A;
-    int retval = plasma_desc_triangular_create(prec, uplo, nb, nb, n, n, 0, 0,
-                                               n, n, &A);
+    /* the tile copy lives in a slot the context keeps between calls */
+    int retval = plasma_desc_kept(plasma, PLASMA_SLOT_DESC_A, prec, uplo, nb, n, n, &A);
     if (retval != PlasmaSuccess) {
-        plasma_error("plasma_desc_triangular_create() failed");
+        plasma_error("tile copy of A failed");
         return retval;
     }
     plasma_sequence_t sequence;
@@ -109,8 +109,6 @@ static int Xpotrf(plasma_enum_t prec, plasma_enum_t uplo, int n, void *pA,
     plasma_sequence_wait(&sequence);
     plasma_omp_Xdesc2lapack(A, pA, lda, uplo, &sequence, &request);
     plasma_sequence_wait(&sequence);
-
-    plasma_desc_destroy(&A);
     return sequence.status;
 }
 

@@ -382,3 +382,32 @@ int plasma_sweep(plasma_context_t *c, plasma_enum_t uplo, int backward,
     return plasma_cuda_trsv(c->stream, c->dstat, uplo, backward, A, W, vec,
                             c->sweep_sync, c->sweep_epoch, c->num_sms);
 }
+
+/* A descriptor over a scratch slot that the context keeps between calls
+ * (the LAPACK-layout drivers' tile copies): no allocation once the slot is
+ * large enough, storage zeroed on the context stream.  type = PlasmaGeneral
+ * or the uplo of a packed triangle.  The descriptor must not be destroyed. */
+int plasma_desc_kept(plasma_context_t *c, int slot, plasma_enum_t precision,
+                     plasma_enum_t type, int nb, int m, int n, plasma_desc_t *A)
+{
+    if (c->device < 0) {
+        plasma_error("no CUDA device");
+        return PlasmaErrorEnvironment;
+    }
+    const size_t mt = (size_t)(m + nb - 1) / nb, nt = (size_t)(n + nb - 1) / nb;
+    const size_t tiles = type == PlasmaGeneral ? mt * nt : nt * (nt + 1) / 2;
+    const size_t bytes = tiles * nb * nb * plasma_element_size(precision);
+    void *buf = plasma_scratch(c, slot, bytes > 0 ? bytes : 16);
+    if (buf == NULL)
+        return PlasmaErrorOutOfMemory;
+    int rc = type == PlasmaGeneral
+                 ? plasma_desc_general_init(precision, buf, nb, nb, m, n, 0, 0, m, n, A)
+                 : plasma_desc_triangular_init(precision, type, buf, nb, nb, m, n, 0, 0,
+                                               m, n, A);
+    if (rc != PlasmaSuccess)
+        return rc;
+    if (plasma_desc_storage_bytes(*A) > bytes)
+        return PlasmaErrorInternal;
+    cudaMemsetAsync(buf, 0, plasma_desc_storage_bytes(*A), c->stream);
+    return PlasmaSuccess;
+}

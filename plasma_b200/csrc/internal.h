@@ -277,6 +277,8 @@ void plasma_cuda_column(cudaStream_t s, plasma_desc_t D, int j, void *v,
 /* One-launch sweep with the context's ready-flag buffer (W from
  * plasma_cuda_trtri_blocks); returns 0 when the factor is not eligible. */
 int plasma_sweep_reserve(plasma_context_t *plasma, plasma_desc_t A);
+int plasma_desc_kept(plasma_context_t *c, int slot, plasma_enum_t precision,
+                     plasma_enum_t type, int nb, int m, int n, plasma_desc_t *A);
 int plasma_sweep(plasma_context_t *plasma, plasma_enum_t uplo, int backward,
                  plasma_desc_t A, const void *W, void *vec);
 
