@@ -59,7 +59,7 @@ def parse():
 
 
 MODES = {"fp32": 0, "tf32": 1, "bf16": 2, "auto": 3}
-UPDATE_DRAM_BYTES_PER_TILE = {"fp32": 393846}
+UPDATE_DRAM_BYTES_PER_TILE = {"fp32": 389908}
 REFINE = {"ir": 0, "gmres": 1, "auto": 2}
 
 
