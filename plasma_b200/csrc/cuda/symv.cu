@@ -8,7 +8,8 @@
 // forms both contributions  S x_q  (to rows of block p)  and  S^T x_p  (to
 // rows of block q).  Lanes own rows, so every warp load is 32 consecutive
 // doubles of one column; the transposed product of a 32x32 block is reduced
-// across lanes by a 31-shuffle butterfly.  The per-tile partial vectors go to
+// across lanes by a butterfly (16 columns per warp pass; one CTA per SM
+// keeps the loop in registers).  The per-tile partial vectors go to
 // a workspace and a second kernel sums them in a fixed order, so results are
 // bit-reproducible.
 //
@@ -21,11 +22,14 @@ namespace {
 
 constexpr int SV_THREADS = 256;
 
-// lane c ends up with sum over lanes of v[c]
-__device__ __forceinline__ double butterfly32(double (&v)[32], int lane)
+// v[i] summed over the 32 lanes, for 16 columns: lane l (and l + 16) ends
+// up with the sum of column l & 15
+__device__ __forceinline__ double butterfly16(double (&v)[16], int lane)
 {
 #pragma unroll
-    for (int off = 16; off >= 1; off >>= 1) {
+    for (int i = 0; i < 16; i++) v[i] += __shfl_xor_sync(0xffffffffu, v[i], 16);
+#pragma unroll
+    for (int off = 8; off >= 1; off >>= 1) {
         const bool hi = (lane & off) != 0;
 #pragma unroll
         for (int i = 0; i < off; i++) {
@@ -51,7 +55,7 @@ __device__ __forceinline__ void stored_tile(int t, int mt, int uplo, int &p, int
 }
 
 template <bool ABS>
-__global__ void __launch_bounds__(SV_THREADS, 2)
+__global__ void __launch_bounds__(SV_THREADS, 1)
 k_symv_tiles(plasma_desc_t A, int uplo, const double *x, double *part,
              const plasma_devstat_t *st)
 {
@@ -77,18 +81,20 @@ k_symv_tiles(plasma_desc_t A, int uplo, const double *x, double *part,
     __syncthreads();
 
     double *yq_out = part + ((size_t)q * mt + p) * nb;     // S^T x_p -> block q
-    const int nbr = (rows + 31) / 32, nbc = (cols + 31) / 32;
+    // warps take 16-column groups (16 accumulators and 16 loads in flight
+    // per lane keep the loop in registers); lanes walk rows
+    const int nbr = (rows + 31) / 32, nbc = (cols + 15) / 16;
     for (int cb = warp; cb < nbc; cb += 8) {
-        double v[32];
+        double v[16];
 #pragma unroll
-        for (int c = 0; c < 32; c++) v[c] = 0.0;
+        for (int c = 0; c < 16; c++) v[c] = 0.0;
         for (int rb = 0; rb < nbr; rb++) {
             const int row = rb * 32 + lane;
             const double xr = xp_s[row];
             double yrow = 0.0;
 #pragma unroll
-            for (int c = 0; c < 32; c++) {
-                const int col = cb * 32 + c;
+            for (int c = 0; c < 16; c++) {
+                const int col = cb * 16 + c;
                 double a = (row < rows && col < cols)
                                ? S[(size_t)col * ld + row] : 0.0;
                 if (ABS) a = fabs(a);
@@ -105,12 +111,14 @@ k_symv_tiles(plasma_desc_t A, int uplo, const double *x, double *part,
             }
             ypart[warp][row] += yrow;
         }
-        double colsum = butterfly32(v, lane);
-        const int col = cb * 32 + lane;
-        if (diag) {
-            if (col < cols) ypart[warp][col] += colsum;
-        } else if (col < cols) {
-            yq_out[col] = colsum;
+        double colsum = butterfly16(v, lane);
+        const int col = cb * 16 + (lane & 15);
+        if (lane < 16) {
+            if (diag) {
+                if (col < cols) ypart[warp][col] += colsum;
+            } else if (col < cols) {
+                yq_out[col] = colsum;
+            }
         }
     }
     __syncthreads();
