@@ -20,7 +20,9 @@
  *    factorisation, as LAPACK's dsposv -- the reference tester's oracle -- does,
  *    and returns the FP64 info (iter = -31).
  *  - Only the uplo triangle of A is converted (the reference converts the full
- *    general matrix, with a "TODO: need zlat2c" note at zcposv.c:447).
+ *    general matrix, with a "TODO: need zlat2c" note at zcposv.c:447), and
+ *    into the LOWER triangle of As whatever uplo is (transposed tiles for
+ *    uplo = Upper), so that the FP32 factor is always the lower one.
  *  - Extended factor precisions and GMRES-IR are available through
  *    PlasmaMixedPrecisionMode / PlasmaRefinement (defaults match the
  *    reference: FP32 factor, classical IR).
@@ -67,7 +69,8 @@ static int take_status(plasma_context_t *plasma)
 
 typedef struct {
     plasma_context_t *plasma;
-    plasma_enum_t uplo;
+    plasma_enum_t uplo;               /* stored triangle of A            */
+    plasma_enum_t uplo_s;             /* stored triangle of As (factor)  */
     plasma_desc_t A, As;
     const void *W32;
     int call;
@@ -89,16 +92,16 @@ static void precond(refine_t *R, const double *in, double *out)
      * D A D (+ shift): M^{-1} v = D (L L^T)^{-1} D v */
     plasma_cuda_d2s(S, in, R->dscale, R->ws, R->n, R->npad, R->plasma->dstat, R->call);
     if (R->fast) {
-        plasma_sweep(R->plasma, R->uplo, 0, R->As, R->W32, R->ws);
-        plasma_sweep(R->plasma, R->uplo, 1, R->As, R->W32, R->ws);
+        plasma_sweep(R->plasma, R->uplo_s, 0, R->As, R->W32, R->ws);
+        plasma_sweep(R->plasma, R->uplo_s, 1, R->As, R->W32, R->ws);
     } else {
         /* the vector viewed as an npad x 1 tile descriptor */
         plasma_desc_t V;
         plasma_desc_general_init(PlasmaRealFloat, R->ws, R->As.mb, R->As.nb,
                                  (int)R->npad, 1, 0, 0, (int)R->npad, 1, &V);
-        plasma_cuda_trsm_sweep(S, R->plasma->dstat, R->uplo, PlasmaNoTrans,
+        plasma_cuda_trsm_sweep(S, R->plasma->dstat, R->uplo_s, PlasmaNoTrans,
                                R->As, V, (void *)R->W32, 1);
-        plasma_cuda_trsm_sweep(S, R->plasma->dstat, R->uplo, PlasmaTrans,
+        plasma_cuda_trsm_sweep(S, R->plasma->dstat, R->uplo_s, PlasmaTrans,
                                R->As, V, (void *)R->W32, 1);
     }
     plasma_cuda_s2d(S, R->ws, R->dscale, out, R->n);
@@ -248,6 +251,13 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
     plasma_devstat_t *st = plasma->dstat;
     int nrhs = B.n;
     *iter = 0;
+    /* The FP32 copy and its factor live in LOWER storage whatever triangle
+     * the caller stores A in (an upper-stored A is converted by transposed
+     * tiles): the tensor-core trailing update of the factorisation runs on
+     * lower tiles.  Only an As that is itself a packed upper triangle keeps
+     * the upper factor.  A keeps the caller's triangle (norm, residual and
+     * the FP64 fallback read it there). */
+    const plasma_enum_t uplo_s = As.type == PlasmaUpper ? PlasmaUpper : PlasmaLower;
 
     /* the small device buffers at their full size from the start, so that
      * the slot never grows (and moves) during the solve */
@@ -325,6 +335,7 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
     memset(&RF, 0, sizeof(RF));
     RF.plasma = plasma;
     RF.uplo = uplo;
+    RF.uplo_s = uplo_s;
     RF.A = A;
     RF.As = As;
     RF.W32 = W32;
@@ -351,7 +362,10 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
         attempts++;
         if (rep) rep->factor_mode = mode;
         if (a > 0 && rep) cudaEventRecord(e0, S);
-        plasma_cuda_lag2s(S, st, call, A, As, uplo);
+        if (uplo_s == uplo)
+            plasma_cuda_lag2s(S, st, call, A, As, uplo);
+        else
+            plasma_cuda_lag2s_upper_to_lower(S, st, call, A, As);
         /* As may be padded to whole tiles: identity on the padding */
         if (As.m > A.m)
             plasma_cuda_set_diag(S, As, A.m, As.m, 1.0);
@@ -362,10 +376,10 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
             double u = mode == PlasmaFactorBF16 ? 0x1p-8 :
                        mode == PlasmaFactorTF32 ? 0x1p-11 : 0x1p-24;
             plasma_cuda_diag_rsqrt(S, A, dvec, n, npad);
-            plasma_cuda_scale_shift(S, As, uplo, dvec, (float)(4.0 * u));
+            plasma_cuda_scale_shift(S, As, uplo_s, dvec, (float)(4.0 * u));
             RF.dscale = dvec;
         }
-        plasma_pXpotrf_mode(plasma, uplo, As, sequence, request, call, mode);
+        plasma_pXpotrf_mode(plasma, uplo_s, As, sequence, request, call, mode);
         factor_failed = take_status(plasma) != 0;
         if (rep)
             cudaEventRecord(e1, S);
@@ -375,9 +389,9 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
         cte = Anorm * eps * sqrt((double)A.n);
         /* inverses of the diagonal blocks of the factor, used by every sweep */
         if (fast_sweep)
-            plasma_cuda_trtri_blocks(S, st, uplo, As, W32);
+            plasma_cuda_trtri_blocks(S, st, uplo_s, As, W32);
         else
-            plasma_cuda_trtri_tiles(S, st, uplo, As, W32);
+            plasma_cuda_trtri_tiles(S, st, uplo_s, As, W32);
         converged = 1;
         int itmax = 0;
         for (int j = 0; j < nrhs; j++) {
@@ -456,6 +470,18 @@ static int check_descs(plasma_enum_t uplo, plasma_desc_t A, plasma_desc_t B,
             plasma_request_fail(sequence, request, PlasmaErrorIllegalValue);
             return 0;
         }
+    }
+    /* a packed triangle must hold the triangle the solve reads: A the
+     * uplo one; As lower (any uplo) or, for uplo = Upper only, upper */
+    if ((A.type == PlasmaLower || A.type == PlasmaUpper) && A.type != uplo) {
+        plasma_error("invalid A");
+        plasma_request_fail(sequence, request, PlasmaErrorIllegalValue);
+        return 0;
+    }
+    if (As.type == PlasmaUpper && uplo != PlasmaUpper) {
+        plasma_error("invalid As");
+        plasma_request_fail(sequence, request, PlasmaErrorIllegalValue);
+        return 0;
     }
     return 1;
 }
@@ -544,16 +570,17 @@ int plasma_dsposv_ex(plasma_enum_t uplo, int n, int nrhs,
     memset(&X, 0, sizeof(X)); memset(&R, 0, sizeof(R));
     memset(&As, 0, sizeof(As)); memset(&Xs, 0, sizeof(Xs));
     int retval;
-    /* A and As: packed uplo triangles (half the memory of general storage;
-     * every kernel of the solve reads the stored triangle only), held in
+    /* A: the packed uplo triangle, As: the packed lower triangle (half the
+     * memory of general storage; every kernel of the solve reads the stored
+     * triangle only), held in
      * scratch slots that the context keeps between calls, so a solve
      * neither allocates nor frees its two large tile copies; zeroed on the
      * stream (the padding of As and the unreferenced halves of diagonal
      * tiles must hold finite values) */
     if ((retval = plasma_desc_kept(plasma, PLASMA_SLOT_DESC_A, PlasmaRealDouble, uplo, nb, n,
                                    n, &A)) != 0 ||
-        (retval = plasma_desc_kept(plasma, PLASMA_SLOT_DESC_AS, PlasmaRealFloat, uplo, nb,
-                                   npad, npad, &As)) != 0)
+        (retval = plasma_desc_kept(plasma, PLASMA_SLOT_DESC_AS, PlasmaRealFloat, PlasmaLower,
+                                   nb, npad, npad, &As)) != 0)
         return retval;
     if ((retval = plasma_desc_general_create(PlasmaRealDouble, nb, nb, n, nrhs,
                                              0, 0, n, nrhs, &B)) != 0 ||

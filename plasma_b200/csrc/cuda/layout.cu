@@ -89,6 +89,51 @@ k_tile_copy(plasma_desc_t A, plasma_desc_t B, int uplo,
         plasma_fail(st, 1, call);
 }
 
+// B(m,n) <- A(n,m)^T for the lower tiles of B (m >= n) from the upper tiles
+// of A (same symmetric matrix in the other triangle), FP64 -> FP32 with the
+// overflow test; 32 x 32 blocks transposed through shared memory so that
+// both the read and the write run along tile columns.
+__global__ void __launch_bounds__(kThreads)
+k_tile_copy_t(plasma_desc_t A, plasma_desc_t B, plasma_devstat_t *st, int call)
+{
+    __shared__ float blk[32][33];
+    const int m = blockIdx.x, n = blockIdx.y;
+    // one answer for the whole block: the loop below holds barriers
+    if (m < n || __syncthreads_or(plasma_failed(st))) return;
+    const double *a = (const double *)plasma_tile_addr(A, n, m);
+    float *b = (float *)plasma_tile_addr(B, m, n);
+    const int lda = plasma_tile_mmain(A, n), ldb = plasma_tile_mmain(B, m);
+    // B(m,n) element (i, j) = A(n,m) element (j, i)
+    const int rows = min(plasma_tile_mview(B, m), plasma_tile_nview(A, m));
+    const int cols = min(plasma_tile_nview(B, n), plasma_tile_mview(A, n));
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    bool overflow = false;
+    for (int i0 = 0; i0 < rows; i0 += 32)
+        for (int j0 = 0; j0 < cols; j0 += 32) {
+            __syncthreads();
+            // read A(n,m)(j0 + tx, i0 + q): along A's columns
+            for (int q = ty; q < 32; q += kThreads / 32) {
+                const int j = j0 + tx, i = i0 + q;
+                float v = 0.f;
+                if (j < cols && i < rows && (m != n || i >= j)) {
+                    const double x = a[(size_t)i * lda + j];
+                    if (x > (double)FLT_MAX || x < -(double)FLT_MAX) overflow = true;
+                    v = (float)x;
+                }
+                blk[q][tx] = v;                       // blk[i - i0][j - j0]
+            }
+            __syncthreads();
+            // write B(m,n)(i0 + tx, j0 + q): along B's columns
+            for (int q = ty; q < 32; q += kThreads / 32) {
+                const int i = i0 + tx, j = j0 + q;
+                if (i < rows && j < cols && (m != n || i >= j))
+                    b[(size_t)j * ldb + i] = blk[tx][q];
+            }
+        }
+    if (__syncthreads_or(overflow) && threadIdx.x == 0)
+        plasma_fail(st, 1, call);
+}
+
 // X(m,n) += R(m,n)  (reference compute/pzgeadd.c:28-73 with alpha = beta = 1)
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
@@ -165,6 +210,17 @@ extern "C" void plasma_cuda_lacpy(cudaStream_t s, plasma_devstat_t *st,
     else
         k_tile_copy<float, float, false><<<tile_grid(A), kThreads, 0, s>>>(
             A, B, PlasmaGeneral, st, 0);
+}
+
+// As (lower tiles) <- A held in upper storage: the conversion of dsposv
+// when its FP32 factor is kept in lower storage for an upper-stored A.
+extern "C" void plasma_cuda_lag2s_upper_to_lower(cudaStream_t s, plasma_devstat_t *st,
+                                                 int call, plasma_desc_t A,
+                                                 plasma_desc_t As)
+{
+    if (A.mt == 0 || A.nt == 0) return;
+    PLASMA_COUNT_LAUNCH();
+    k_tile_copy_t<<<tile_grid(A), kThreads, 0, s>>>(A, As, st, call);
 }
 
 extern "C" void plasma_cuda_lag2s(cudaStream_t s, plasma_devstat_t *st, int call,

@@ -170,6 +170,9 @@ int plasma_cuda_lansy_tiles(cudaStream_t s, plasma_devstat_t *st,
 void plasma_cuda_lansy_inf(cudaStream_t s, plasma_devstat_t *st,
                            plasma_enum_t uplo, plasma_desc_t A,
                            double *dnorm, double *work);
+/* As (lower tiles) <- (float)A with A in upper storage (transposed tiles). */
+void plasma_cuda_lag2s_upper_to_lower(cudaStream_t s, plasma_devstat_t *st, int call,
+                                      plasma_desc_t A, plasma_desc_t As);
 /* As <- (float)A tile by tile; sets status 1 on overflow (dlag2s). */
 void plasma_cuda_lag2s(cudaStream_t s, plasma_devstat_t *st, int call,
                        plasma_desc_t A, plasma_desc_t As, plasma_enum_t uplo);

@@ -223,3 +223,44 @@ def test_autotune_argument_codes(hostonly):
     assert L.plasma_autotune_potrf(pb.PlasmaRealDouble, 0, None) == -2
     assert L.plasma_autotune_batched(pb.PlasmaRealFloat, 0) == -2
     assert L.plasma_autotune_potrf(pb.PlasmaRealDouble, 100, None) == pb.PlasmaErrorEnvironment
+
+
+def test_dsposv_descriptor_triangles(hostonly):
+    """plasma_omp_dsposv checks that packed triangles hold what the solve
+    reads: A the uplo triangle, As lower (for either uplo) or upper (for
+    uplo = Upper only); a mismatch fails the sequence with IllegalValue
+    before any device work, a match reaches the device check."""
+    L = hostonly
+    n, nb = 64, 32
+    buf = np.zeros(4 * n * n)
+    p = buf.ctypes.data
+
+    def tri(prec, uplo):
+        d = pb.plasma_desc_t()
+        assert L.plasma_desc_triangular_init(prec, uplo, p, nb, nb, n, n, 0, 0, n, n,
+                                             ctypes.byref(d)) == 0
+        return d
+
+    def gen(prec, m):
+        d = pb.plasma_desc_t()
+        assert L.plasma_desc_general_init(prec, p, nb, nb, n, m, 0, 0, n, m,
+                                          ctypes.byref(d)) == 0
+        return d
+
+    B, X, R = gen(pb.PlasmaRealDouble, 1), gen(pb.PlasmaRealDouble, 1), gen(pb.PlasmaRealDouble, 1)
+    Xs = gen(pb.PlasmaRealFloat, 1)
+    D, S = pb.PlasmaRealDouble, pb.PlasmaRealFloat
+    cases = [
+        (pb.PlasmaLower, tri(D, pb.PlasmaLower), tri(S, pb.PlasmaUpper), pb.PlasmaErrorIllegalValue),
+        (pb.PlasmaUpper, tri(D, pb.PlasmaLower), tri(S, pb.PlasmaLower), pb.PlasmaErrorIllegalValue),
+        (pb.PlasmaUpper, tri(D, pb.PlasmaUpper), tri(S, pb.PlasmaLower), pb.PlasmaErrorEnvironment),
+        (pb.PlasmaUpper, tri(D, pb.PlasmaUpper), tri(S, pb.PlasmaUpper), pb.PlasmaErrorEnvironment),
+        (pb.PlasmaLower, gen(D, n), gen(S, n), pb.PlasmaErrorEnvironment),
+    ]
+    for uplo, A, As, want in cases:
+        seq, req = pb.new_sequence()
+        it = ctypes.c_int(-5)
+        L.plasma_omp_dsposv(uplo, A, B, X, As, Xs, R, None, None, None, ctypes.byref(it),
+                            ctypes.byref(seq), ctypes.byref(req))
+        assert seq.status == want, (uplo, A.type, As.type)
+        assert it.value == 0

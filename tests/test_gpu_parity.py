@@ -383,6 +383,33 @@ def test_dsposv_tensor_core_factor(L, mode, n, nb):
         L.plasma_set(pb.PlasmaMixedPrecisionMode, pb.PlasmaFactorFP32)
 
 
+@pytest.mark.parametrize("mode", [pb.PlasmaFactorFP32, pb.PlasmaFactorTF32,
+                                  pb.PlasmaFactorBF16])
+@pytest.mark.parametrize("n,nb", [(1024, 256), (1000, 256), (777, 128)])
+def test_dsposv_upper_storage(L, mode, n, nb):
+    """uplo = Upper: the FP32 copy is built in lower storage from transposed
+    upper tiles (only the upper triangle of A is read: the strictly lower
+    part holds NaN), so the factor is the one of uplo = Lower; the answer
+    matches the oracle and the refinement takes the same number of steps."""
+    set_nb(L, nb)
+    L.plasma_set(pb.PlasmaMixedPrecisionMode, mode)
+    try:
+        a, b = gen.diag_dominant(n, 2, seed=900 + n)
+        au = np.asfortranarray(np.triu(a) + np.tril(np.full_like(a, np.nan), -1))
+        rc, it_up, x, info = dsposv_ex(L, UP, au, b)
+        assert rc == 0
+        assert info.factor_mode == mode
+        assert 0 <= it_up <= 30
+        assert solve_residual(a, x, b) < TOL * EPS
+        rc, it_lo, xl, _ = dsposv_ex(L, LO, np.asfortranarray(a.copy()), b)
+        assert rc == 0 and abs(it_up - it_lo) <= 1
+        xo = np.zeros_like(x, order="F")
+        assert oracle.dsposv(oracle.UPPER, np.asfortranarray(a.copy()), b, xo, nb)[0] == 0
+        np.testing.assert_allclose(x, xo, rtol=1e-12, atol=1e-15)
+    finally:
+        L.plasma_set(pb.PlasmaMixedPrecisionMode, pb.PlasmaFactorFP32)
+
+
 @pytest.mark.parametrize("mode", [pb.PlasmaFactorTF32, pb.PlasmaFactorBF16])
 def test_tensor_core_factor_quality(L, mode):
     """The low-precision factor itself: ||A - L L^T|| / ||A|| at the level of
