@@ -440,6 +440,348 @@ k_update_tc(const __grid_constant__ CUtensorMap opmap,
 }
 
 // ---------------------------------------------------------------------------
+// CTA-pair variant for nb = 256: one cluster of two CTAs (on two SMs) owns a
+// whole 256 x 256 output tile per item.  The MMA runs with cta_group::2,
+// M = 256 and N = 256: each CTA stages its own 128 rows of A(m,k) and its
+// own 128 rows of A(n,k) (half of the B operand), so a CTA moves 32 KB of
+// operands per k-step instead of 48 KB (TF32X3) -- a third less L2 traffic
+// per product, and a 6-deep ring in the same shared memory.  Tensor memory
+// of each CTA holds its 128 output rows (two accumulators of 256 columns).
+//   rank 0 (leader) : producer, MMA issuer, epilogue of rows 0..127;
+//   rank 1          : producer, epilogue of rows 128..255.
+// Both producers' TMA loads complete on the leader's full barrier (the
+// .cta_group::2 form of the load); the leader's commits arrive on the empty
+// and accumulator-full barriers of both CTAs (tcgen05.commit multicast);
+// both epilogues release an accumulator on the leader's barrier.  The pair
+// meets at cluster barriers after the barriers are initialised and before
+// tensor memory is freed; every loop in between ends (waits are bounded),
+// so both CTAs always reach them.
+// ---------------------------------------------------------------------------
+constexpr int PAIR_STAGE_BYTES = 32 * 1024;
+
+template <int MODE>
+struct PairGeo {
+    using G = Geo<MODE>;
+    static constexpr int EPI_BUFS = MODE == MODE_TF32X3 ? 1 : 2;
+    static constexpr int STAGES = MODE == MODE_TF32X3 ? 6 : 5;
+    static constexpr int SMEM = STAGES * PAIR_STAGE_BYTES +
+                                TC_EPI_WARPS * EPI_BUFS * TC_EPI_BUF_BYTES + 1024;
+};
+
+__device__ __forceinline__ uint32_t cluster_rank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+// shared::cluster address of the variable at `p` in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t peer_addr(const void *p, uint32_t rank)
+{
+    uint32_t a;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(smem_u32(p)), "r"(rank));
+    return a;
+}
+
+__device__ __forceinline__ void cluster_sync_all()
+{
+    asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr)
+{
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];"
+                 :: "r"(cluster_addr) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_cluster(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+
+// Bounded wait with cluster-scope acquire (barriers that CTAs of the pair
+// arrive on): false after ~2 s or when this CTA already gave up.
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t *bar, uint32_t parity,
+                                                  volatile int *abort_flag)
+{
+    long long t0 = clock64();
+    while (!mbar_try_cluster(bar, parity)) {
+        if (*abort_flag) return false;
+        if (clock64() - t0 > 4000000000LL) {
+            *abort_flag = 1;
+            return false;
+        }
+    }
+    return true;
+}
+
+// TMA load into this CTA's shared memory whose completion is counted on the
+// barrier at shared::cluster address `bar` (the leader's)
+__device__ __forceinline__ void tma_load_4d_pair(void *dst, const CUtensorMap *map,
+                                                 uint32_t bar, int c0, int c1, int c2,
+                                                 int c3)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5, %6}], [%2];"
+        :: "r"(smem_u32(dst)), "l"(map), "r"(bar), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+        : "memory");
+}
+
+template <int MODE>
+__device__ __forceinline__ void mma_pair(uint32_t tmem, uint64_t a, uint64_t b,
+                                         uint32_t idesc, uint32_t acc)
+{
+    const uint32_t z = 0;
+    if (MODE != MODE_BF16)
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, "
+            "{%5, %5, %5, %5, %5, %5, %5, %5}, p;\n\t}"
+            :: "r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(z));
+    else
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, "
+            "{%5, %5, %5, %5, %5, %5, %5, %5}, p;\n\t}"
+            :: "r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(z));
+}
+
+// arrive on the barrier at this offset in both CTAs of the pair once the
+// MMAs issued so far are complete
+__device__ __forceinline__ void mma_commit_pair(uint64_t *bar)
+{
+    const uint16_t mask = 0x3;
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
+        " [%0], %1;" :: "r"(smem_u32(bar)), "h"(mask) : "memory");
+}
+
+__device__ __forceinline__ uint32_t instr_desc_pair(int mode)
+{
+    uint32_t fmt = mode == MODE_BF16 ? 1u : 2u;
+    return (1u << 4) | (fmt << 7) | (fmt << 10) | (1u << 15) | (1u << 16) |
+           ((uint32_t)(256 >> 3) << 17) | ((uint32_t)(256 >> 4) << 24);
+}
+
+template <int MODE>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
+k_update_pair(const __grid_constant__ CUtensorMap opmap,
+              const __grid_constant__ CUtensorMap cmap, TcArgs g,
+              plasma_devstat_t *st)
+{
+    using G = Geo<MODE>;
+    using P = PairGeo<MODE>;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    constexpr int STAGES = P::STAGES;
+    constexpr int EPI_BUFS = P::EPI_BUFS;
+    constexpr int NB = 256;
+    __shared__ uint64_t full_bar[STAGES], empty_bar[STAGES];
+    __shared__ uint64_t tfull_bar[2], tempty_bar[2];
+    __shared__ uint32_t tmem_base_s;
+    __shared__ int go_s;
+    __shared__ volatile int abort_s;
+
+    const uint32_t rank = cluster_rank();
+    const bool leader = rank == 0;
+    // items: whole tiles; g.ipc tiles per pair, g.nitems tiles in all
+    const long long pair = blockIdx.x >> 1;
+    const long long first = pair * g.ipc;
+    if (first >= g.nitems) return;                 // the same for both CTAs
+    const int nit = (int)min((long long)g.ipc, g.nitems - first);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    unsigned char *stage_base =
+        (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    // per part: 128 rows of A(m,k) then 128 rows of A(n,k), BK columns each
+    constexpr int HALF = G::A_BYTES;
+    constexpr int STAGE_BYTES = G::PARTS * 2 * HALF;
+    static_assert(STAGE_BYTES == PAIR_STAGE_BYTES, "stage size");
+    constexpr int nkb = NB / G::BK;
+    constexpr uint32_t tmem_cols = 2 * NB;
+
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], 1);
+        }
+        for (int a = 0; a < 2; a++) {
+            mbar_init(&tfull_bar[a], 1);
+            mbar_init(&tempty_bar[a], 2 * TC_EPI_WARPS);
+        }
+        abort_s = 0;
+        go_s = !plasma_failed(st);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    cluster_sync_all();                            // barriers of both CTAs ready
+    // the leader's view of the device status decides for the pair
+    int go;
+    {
+        const uint32_t a = peer_addr((const void *)&go_s, 0);
+        asm volatile("ld.shared::cluster.s32 %0, [%1];" : "=r"(go) : "r"(a) : "memory");
+    }
+    if (warp == 2) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(&tmem_base_s)), "r"(tmem_cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base_s;
+    const uint32_t full_lead0 = peer_addr(&full_bar[0], 0);   // leader's full_bar[0]
+    const uint32_t tempty_lead0 = peer_addr(&tempty_bar[0], 0);
+
+    if (!go) {
+        // status already failed: no work, both CTAs go to the teardown
+    } else if (warp == 0 && lane == 0) {
+        // ---------------- producer (both CTAs)
+        int it = 0;
+        bool ok = true;
+        for (int j = 0; j < nit && ok; j++) {
+            int m, n, si;
+            tc_item(g, 2 * (first + j) + rank, m, n, si);
+            const int row0 = (int)rank * TC_M;   // this CTA's rows of both operands
+            for (int kb = 0; kb < nkb; kb++, it++) {
+                const int s = it % STAGES;
+                if (it >= STAGES &&
+                    !mbar_wait_cluster(&empty_bar[s], ((it / STAGES) - 1) & 1, &abort_s)) {
+                    ok = false;
+                    break;
+                }
+                unsigned char *sp = stage_base + s * PAIR_STAGE_BYTES;
+                const uint32_t fb = full_lead0 + (uint32_t)(s * sizeof(uint64_t));
+                if (leader) mbar_expect_tx(&full_bar[s], 2u * (uint32_t)STAGE_BYTES);
+#pragma unroll
+                for (int p = 0; p < G::PARTS; p++) {
+                    const int toff = p * g.mt;
+                    tma_load_4d_pair(sp + p * HALF, &opmap, fb, 0, kb * G::BK,
+                                     row0 / G::MNBOX, m + toff);
+                    tma_load_4d_pair(sp + (G::PARTS + p) * HALF, &opmap, fb, 0, kb * G::BK,
+                                     row0 / G::MNBOX, n + toff);
+                }
+            }
+        }
+    } else if (warp == 1 && lane == 0 && leader) {
+        // ---------------- MMA issuer (leader only)
+        const uint32_t idesc = instr_desc_pair(MODE);
+        int it = 0;
+        bool ok = true;
+        for (int j = 0; j < nit && ok; j++) {
+            const int a = j & 1;
+            if (j >= 2 && !mbar_wait_cluster(&tempty_bar[a], ((j >> 1) - 1) & 1, &abort_s))
+                break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t acc_t = tmem + (uint32_t)(a * NB);
+            for (int kb = 0; kb < nkb; kb++, it++) {
+                const int s = it % STAGES;
+                if (!mbar_wait_cluster(&full_bar[s], (it / STAGES) & 1, &abort_s)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                unsigned char *sp = stage_base + s * PAIR_STAGE_BYTES;
+                unsigned char *sa_hi = sp;
+                unsigned char *sb_hi = sp + G::PARTS * HALF;
+#pragma unroll
+                for (int kk = 0; kk < G::BK / G::KI; kk++) {
+                    const uint32_t acc_on = (kb | kk) != 0;
+                    uint64_t da = smem_desc(sa_hi + kk * G::KI * 128, G::CHUNK, G::SBO,
+                                            G::LAYOUT);
+                    uint64_t db = smem_desc(sb_hi + kk * G::KI * 128, G::CHUNK, G::SBO,
+                                            G::LAYOUT);
+                    if (MODE == MODE_TF32X3) {
+                        uint64_t dal = smem_desc(sa_hi + HALF + kk * G::KI * 128, G::CHUNK,
+                                                 G::SBO, G::LAYOUT);
+                        uint64_t dbl = smem_desc(sb_hi + HALF + kk * G::KI * 128, G::CHUNK,
+                                                 G::SBO, G::LAYOUT);
+                        mma_pair<MODE>(acc_t, dal, db, idesc, acc_on);
+                        mma_pair<MODE>(acc_t, da, dbl, idesc, 1u);
+                        mma_pair<MODE>(acc_t, da, db, idesc, 1u);
+                    } else {
+                        mma_pair<MODE>(acc_t, da, db, idesc, acc_on);
+                    }
+                }
+                mma_commit_pair(&empty_bar[s]);
+            }
+            if (ok) mma_commit_pair(&tfull_bar[a]);
+        }
+    } else if (warp >= TC_EPI_WARP0) {
+        // ---------------- epilogue (both CTAs): this CTA's 128 rows
+        const int e = warp - TC_EPI_WARP0;
+        const int q = warp & 3;
+        const int half = e / 4;
+        float *stage_epi = (float *)(stage_base + STAGES * PAIR_STAGE_BYTES) +
+                           (size_t)e * EPI_BUFS * (TC_EPI_BUF_BYTES / 4);
+        int nchunk = 0;
+        for (int j = 0; j < nit; j++) {
+            const int a = j & 1;
+            const bool ok = __all_sync(0xffffffffu,
+                                       mbar_wait_cluster(&tfull_bar[a], (j >> 1) & 1, &abort_s));
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            int m, n, si;
+            tc_item(g, 2 * (first + j) + rank, m, n, si);
+            const int tile = (int)(((const char *)plasma_tile_addr(g.A, m, n) -
+                                    (const char *)g.A.matrix) / ((size_t)NB * NB * 4));
+            const int r0 = si * TC_M + 32 * q;
+            const int row = r0 + lane;
+            const bool diag = m == n;
+            const int c0 = half * (NB / 2);
+            for (int cc = c0; cc < c0 + NB / 2; cc += 32, nchunk++) {
+                float v[32];
+                tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(a * NB + cc), v);
+                float *buf = stage_epi + (nchunk % EPI_BUFS) * (TC_EPI_BUF_BYTES / 4);
+                if (nchunk >= EPI_BUFS && lane == 0) bulk_wait_read<EPI_BUFS - 1>();
+                __syncwarp();
+#pragma unroll
+                for (int jj = 0; jj < 32; jj++) {
+                    const int col = cc + jj;
+                    buf[jj * 32 + lane] = (!diag || row >= col) ? -v[jj] : 0.f;
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) {
+                    tma_reduce_add_3d(&cmap, buf, r0, cc, tile);
+                    bulk_commit();
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive_remote(tempty_lead0 + (uint32_t)(a * sizeof(uint64_t)));
+        }
+        if (lane == 0) bulk_wait_all();
+        __syncwarp();
+    }
+    // ---------------- teardown
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (abort_s) {
+        if (tid == 0) {
+            plasma_fail(st, PlasmaErrorInternal, 0);
+            long long t0 = clock64();
+            while (clock64() - t0 < 200000000LL) {}
+        }
+        __syncthreads();
+    }
+    // neither CTA frees tensor memory or leaves while the pair's MMAs,
+    // commits or remote arrivals may still touch it
+    cluster_sync_all();
+    if (warp == 2) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;"
+                     :: "r"(tmem), "r"(tmem_cols));
+    }
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
@@ -512,6 +854,37 @@ void launch_update(cudaStream_t s, const CUtensorMap &map, const CUtensorMap &cm
     k_update_tc<MODE><<<grid, TC_THREADS, Geo<MODE>::SMEM, s>>>(map, cmap, g, st);
 }
 
+template <int MODE>
+void launch_pair(cudaStream_t s, const CUtensorMap &map, const CUtensorMap &cmap,
+                 const TcArgs &g, unsigned grid, plasma_devstat_t *st)
+{
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_update_pair<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             PairGeo<MODE>::SMEM);
+        attr = true;
+    }
+    k_update_pair<MODE><<<grid, TC_THREADS, PairGeo<MODE>::SMEM, s>>>(map, cmap, g, st);
+}
+
+// Items per CTA (one CTA per SM) with the smallest estimated makespan,
+// waves * (ipc + 1/2) items -- a CTA's pipeline fill and its last,
+// unoverlapped epilogue cost about half an item -- ties to the larger ipc.
+// `unit` CTAs share an item (1, or 2 for the CTA pairs).
+long long choose_ipc(long long nitems, int unit, long long sms, int max_items)
+{
+    long long best_ipc = 1, best_cost = -1;
+    for (long long ipc = 1; ipc <= max_items; ipc++) {
+        const long long ctas = unit * ((nitems + ipc - 1) / ipc);
+        const long long cost = ((ctas + sms - 1) / sms) * (2 * ipc + 1);
+        if (best_cost < 0 || cost <= best_cost) {
+            best_cost = cost;
+            best_ipc = ipc;
+        }
+    }
+    return best_ipc;
+}
+
 }  // namespace
 
 // Eligibility of the tensor-core update for an FP32 descriptor: general or
@@ -545,9 +918,9 @@ extern "C" int plasma_cuda_update_tc(cudaStream_t s, plasma_devstat_t *st,
 {
     if (nhi <= nlo) return 1;
     const int nb = A.mb;
-    long long pairs = 0;
-    for (int n = nlo; n < nhi; n++) pairs += A.mt - n;
-    const long long nitems = pairs * (nb / TC_M);
+    long long tiles = 0;
+    for (int n = nlo; n < nhi; n++) tiles += A.mt - n;
+    const long long nitems = tiles * (nb / TC_M);
     if (nitems <= 0) return 1;
     if (panel == nullptr || ((uintptr_t)panel & 1023) != 0 ||
         ((uintptr_t)A.matrix & 15) != 0)
@@ -581,31 +954,29 @@ extern "C" int plasma_cuda_update_tc(cudaStream_t s, plasma_devstat_t *st,
     g.nlo = nlo;
     g.nhi = nhi;
     g.mt = A.mt;
-    g.nitems = nitems;
-    // Items per CTA (one CTA per SM): the smallest estimated makespan,
-    // waves * (ipc + 1/2) items -- a CTA's pipeline fill and its last,
-    // unoverlapped epilogue cost about half an item -- ties to the larger
-    // ipc (the SMs left over serve the panel stream).
     // PLASMA_UPDATE_MAX_ITEMS caps the items per CTA (default 8): shorter
-    // CTAs hand SMs back to the panel stream sooner
-    static int max_items = -1;
+    // CTAs hand SMs back to the panel stream sooner.  PLASMA_UPDATE_PAIR
+    // selects the CTA-pair kernel for 256-wide tiles (default on; 0 = off).
+    static int max_items = -1, pair_mode = -1;
     if (max_items < 0) {
         const char *env = getenv("PLASMA_UPDATE_MAX_ITEMS");
         max_items = env ? atoi(env) : 8;
         if (max_items < 1 || max_items > 64) max_items = 8;
+        env = getenv("PLASMA_UPDATE_PAIR");
+        pair_mode = env ? atoi(env) != 0 : 1;
     }
     const long long sms = num_sms > 0 ? num_sms : 148;
-    long long best_ipc = 1, best_cost = -1;
-    for (long long ipc = 1; ipc <= max_items; ipc++) {
-        const long long ctas = (nitems + ipc - 1) / ipc;
-        const long long cost = ((ctas + sms - 1) / sms) * (2 * ipc + 1);
-        if (best_cost < 0 || cost <= best_cost) {
-            best_cost = cost;
-            best_ipc = ipc;
-        }
+    const bool use_pair = pair_mode && nb == 2 * TC_M;
+    unsigned grid;
+    if (use_pair) {
+        g.nitems = tiles;
+        g.ipc = (int)choose_ipc(tiles, 2, sms, max_items);
+        grid = (unsigned)(2 * ((tiles + g.ipc - 1) / g.ipc));
+    } else {
+        g.nitems = nitems;
+        g.ipc = (int)choose_ipc(nitems, 1, sms, max_items);
+        grid = (unsigned)((nitems + g.ipc - 1) / g.ipc);
     }
-    g.ipc = (int)best_ipc;
-    const unsigned grid = (unsigned)((nitems + g.ipc - 1) / g.ipc);
 
     PLASMA_COUNT_LAUNCH();
     double flops = 0.0, bytes = 0.0;
@@ -618,10 +989,18 @@ extern "C" int plasma_cuda_update_tc(cudaStream_t s, plasma_devstat_t *st,
         }
     }
     int prof = plasma_prof_begin(s);
-    switch (mode) {
-    case PLASMA_TC_TF32: launch_update<MODE_TF32>(s, map, cmap, g, grid, st); break;
-    case PLASMA_TC_TF32X3: launch_update<MODE_TF32X3>(s, map, cmap, g, grid, st); break;
-    default: launch_update<MODE_BF16>(s, map, cmap, g, grid, st); break;
+    if (use_pair) {
+        switch (mode) {
+        case PLASMA_TC_TF32: launch_pair<MODE_TF32>(s, map, cmap, g, grid, st); break;
+        case PLASMA_TC_TF32X3: launch_pair<MODE_TF32X3>(s, map, cmap, g, grid, st); break;
+        default: launch_pair<MODE_BF16>(s, map, cmap, g, grid, st); break;
+        }
+    } else {
+        switch (mode) {
+        case PLASMA_TC_TF32: launch_update<MODE_TF32>(s, map, cmap, g, grid, st); break;
+        case PLASMA_TC_TF32X3: launch_update<MODE_TF32X3>(s, map, cmap, g, grid, st); break;
+        default: launch_update<MODE_BF16>(s, map, cmap, g, grid, st); break;
+        }
     }
     plasma_prof_end(prof, s, PLASMA_KCLASS_UPDATE, flops, bytes);
     return 1;
