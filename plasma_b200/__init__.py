@@ -18,6 +18,12 @@ import os
 from ctypes import (POINTER, Structure, byref, c_double, c_float, c_int,
                     c_longlong, c_size_t, c_void_p, c_char_p)
 
+# The library keeps about 16 CUDA streams busy while a host matrix is still
+# being uploaded; more hardware queues than the driver's default 8 keep them
+# from holding one another up.  The driver reads this when the CUDA context
+# is created, so it is set at import, before torch touches the GPU.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libplasma_b200.so")
 

@@ -235,16 +235,96 @@ static int refine_column(refine_t *R, int scheme, double cte, double *xn_out,
     return -1;
 }
 
+/* A lower-stored host matrix whose upload overlaps the factorization. */
+typedef struct {
+    const double *pA;
+    int lda;
+} upload_t;
+
+/* Tile-column groups that each hold about the same share of the lower
+ * triangle (PLASMA_GROUP_STREAMS of them, so the first ones are narrow and
+ * the last ones wide): the right-looking update of a column needs every
+ * panel before it, so most of the update work sits in the last columns,
+ * and equal shares let it start as early as the bus allows. */
+static int column_groups(int nt, int *gstart)
+{
+    const int ng_max = nt < PLASMA_GROUP_STREAMS ? nt : PLASMA_GROUP_STREAMS;
+    const double total = 0.5 * (double)nt * (nt + 1);
+    int ng = 0;
+    double acc = 0.0;
+    gstart[0] = 0;
+    for (int j = 0; j < nt; j++) {
+        acc += nt - j;                      /* tiles of column j */
+        if ((ng < ng_max - 1 && acc >= total * (ng + 1) / ng_max) || j == nt - 1)
+            gstart[++ng] = j + 1;
+    }
+    return ng;
+}
+
+/* The first attempt of the FP32 path for a host matrix: its lower triangle
+ * goes up on the copy stream one group of tile columns at a time (one
+ * cudaMemcpy2DAsync per tile column, from the diagonal down), each group is
+ * converted to the FP64 tiles of A and the FP32 tiles of As as soon as it
+ * is in, and the factorization of As runs on the groups already in place
+ * (plasma_pXpotrf_arrivals).  ||A||_inf follows the last group on the copy
+ * stream.  With page-locked host memory the copies overlap the kernels;
+ * pageable memory gives the same result without the overlap. */
+static void upload_and_factor(plasma_context_t *plasma, const upload_t *up,
+                              plasma_desc_t A, plasma_desc_t As, double *d_anorm,
+                              double *symv_work, int call, int mode,
+                              plasma_sequence_t *sequence, plasma_request_t *request)
+{
+    cudaStream_t S = plasma->stream;
+    cudaStream_t cp = plasma->aux[PLASMA_STREAM_COPY];
+    plasma_devstat_t *st = plasma->dstat;
+    const int n = A.m, nb = A.nb;
+    /* every slot the factorization uses is sized before the first copy: a
+     * slot that grows waits for all streams, the copy stream included */
+    plasma_pXpotrf_reserve(plasma, PlasmaLower, As, mode, 1);
+    double *stage = (double *)plasma_scratch(plasma, PLASMA_SLOT_STAGING,
+                                             (size_t)n * (size_t)n * sizeof(double));
+    if (stage == NULL) {
+        plasma_request_fail(sequence, request, PlasmaErrorOutOfMemory);
+        return;
+    }
+    int gstart[PLASMA_GROUP_STREAMS + 1];
+    const int ng = column_groups(A.nt, gstart);
+    /* the copies start after everything enqueued so far (the zeroed tile
+     * storage, the right-hand side) */
+    cudaEventRecord(plasma->ev[4], S);
+    cudaStreamWaitEvent(cp, plasma->ev[4], 0);
+    for (int g = 0; g < ng; g++) {
+        for (int j = gstart[g]; j < gstart[g + 1]; j++) {
+            const int c0 = j * nb;
+            const int w = n - c0 < nb ? n - c0 : nb;
+            cudaMemcpy2DAsync(stage + (size_t)c0 * n + c0, (size_t)n * sizeof(double),
+                              up->pA + (size_t)c0 * up->lda + c0,
+                              (size_t)up->lda * sizeof(double),
+                              (size_t)(n - c0) * sizeof(double), (size_t)w,
+                              cudaMemcpyHostToDevice, cp);
+        }
+        plasma_cuda_upload_cols(cp, st, plasma->dquiet, call, A, As, stage, n, gstart[g],
+                                gstart[g + 1]);
+        cudaEventRecord(plasma->ev_group[g], cp);
+    }
+    plasma_cuda_lansy_inf(cp, plasma->dquiet, PlasmaLower, A, d_anorm, symv_work);
+    cudaEventRecord(plasma->ev[5], cp);
+    plasma_pXpotrf_arrivals(plasma, PlasmaLower, As, sequence, request, call, mode, ng,
+                            gstart, plasma->ev_group);
+    cudaStreamWaitEvent(S, plasma->ev[5], 0);
+}
+
 /*
  * The solver proper.  Returns through *iter and the sequence; fills `rep`
- * when not NULL.
+ * when not NULL.  up != NULL: A (lower) is still on the host and comes up
+ * during the first factorization (upload_and_factor).
  */
 static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
                     plasma_desc_t A, plasma_desc_t B, plasma_desc_t X,
                     plasma_desc_t As, plasma_desc_t Xs, plasma_desc_t R,
                     double *Rnorm, double *Xnorm, int *iter,
                     plasma_sequence_t *sequence, plasma_request_t *request,
-                    plasma_dsposv_info_t *rep)
+                    plasma_dsposv_info_t *rep, const upload_t *up)
 {
     const double eps = DBL_EPSILON * 0.5;   /* LAPACK dlamch('E') */
     cudaStream_t S = plasma->stream;
@@ -289,8 +369,10 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
     double Anorm = 0.0;
     double *sw = (double *)plasma_scratch(plasma, PLASMA_SLOT_SYMV,
                                           plasma_cuda_symv_work(A));
-    plasma_cuda_lansy_inf(S, st, uplo, A, d_anorm, sw);
-    cudaMemcpyAsync(&Anorm, d_anorm, sizeof(double), cudaMemcpyDeviceToHost, S);
+    if (up == NULL) {
+        plasma_cuda_lansy_inf(S, st, uplo, A, d_anorm, sw);
+        cudaMemcpyAsync(&Anorm, d_anorm, sizeof(double), cudaMemcpyDeviceToHost, S);
+    }
 
     /* ------------------------------------------------------------------
      * Low-precision phase.  An attempt = convert A, optionally scale it to
@@ -362,14 +444,24 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
         attempts++;
         if (rep) rep->factor_mode = mode;
         if (a > 0 && rep) cudaEventRecord(e0, S);
-        if (uplo_s == uplo)
-            plasma_cuda_lag2s(S, st, call, A, As, uplo);
-        else
-            plasma_cuda_lag2s_upper_to_lower(S, st, call, A, As);
         /* As may be padded to whole tiles: identity on the padding */
         if (As.m > A.m)
             plasma_cuda_set_diag(S, As, A.m, As.m, 1.0);
         RF.dscale = NULL;
+        if (a == 0 && up != NULL) {
+            upload_and_factor(plasma, up, A, As, d_anorm, sw, call, mode, sequence, request);
+            cudaMemcpyAsync(&Anorm, d_anorm, sizeof(double), cudaMemcpyDeviceToHost, S);
+            factor_failed = take_status(plasma) != 0;
+            if (rep)
+                cudaEventRecord(e1, S);
+            if (factor_failed)
+                continue;
+            goto factored;
+        }
+        if (uplo_s == uplo)
+            plasma_cuda_lag2s(S, st, call, A, As, uplo);
+        else
+            plasma_cuda_lag2s_upper_to_lower(S, st, call, A, As);
         if (plan[a].scaled) {
             /* unit diagonal, then + c u I with u the unit roundoff of the
              * products and c = 4 */
@@ -385,7 +477,7 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
             cudaEventRecord(e1, S);
         if (factor_failed)
             continue;
-
+    factored:
         cte = Anorm * eps * sqrt((double)A.n);
         /* inverses of the diagonal blocks of the factor, used by every sweep */
         if (fast_sweep)
@@ -515,7 +607,7 @@ void plasma_omp_dsposv(plasma_enum_t uplo,
     if (sequence->status != PlasmaSuccess)
         return;
     Xdsposv(plasma, uplo, A, B, X, As, Xs, R, Rnorm, Xnorm, iter, sequence,
-            request, NULL);
+            request, NULL, NULL);
 }
 
 int plasma_dsposv_ex(plasma_enum_t uplo, int n, int nrhs,
@@ -604,12 +696,23 @@ int plasma_dsposv_ex(plasma_enum_t uplo, int n, int nrhs,
     plasma_sequence_init(&sequence);
     plasma_request_init(&request);
 
-    /* only the uplo triangle of A is referenced */
-    plasma_omp_Xlapack2desc(pA, lda, A, uplo, &sequence, &request);
+    /* only the uplo triangle of A is referenced; a lower triangle on the
+     * host goes up while the factorization runs (PLASMA_PIPELINE_UPLOAD=0
+     * uploads it first) */
+    static int pipeline_env = -1;
+    if (pipeline_env < 0) {
+        const char *e = getenv("PLASMA_PIPELINE_UPLOAD");
+        pipeline_env = e == NULL || atoi(e) != 0;
+    }
+    upload_t up = {pA, lda};
+    const int pipelined = pipeline_env && uplo == PlasmaLower && plasma->lookahead != 0 &&
+                          !plasma_is_device_pointer(pA);
+    if (!pipelined)
+        plasma_omp_Xlapack2desc(pA, lda, A, uplo, &sequence, &request);
     plasma_omp_Xlapack2desc(pB, ldb, B, PlasmaGeneral, &sequence, &request);
     if (sequence.status == PlasmaSuccess) {
         Xdsposv(plasma, uplo, A, B, X, As, Xs, R, Rnorm, Xnorm, iter,
-                &sequence, &request, info);
+                &sequence, &request, info, pipelined ? &up : NULL);
     }
     plasma_sequence_wait(&sequence);
     plasma_omp_Xdesc2lapack(X, pX, ldx, PlasmaGeneral, &sequence, &request);

@@ -26,6 +26,8 @@
 
 #include <cuda_runtime_api.h>
 #include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
 
 typedef struct {
     plasma_devstat_t *st;
@@ -34,17 +36,60 @@ typedef struct {
     int sms;
     int mode;          /* PLASMA_TC_* product precision of the tensor-core
                           update, or 0 for the DMMA/SIMT update            */
-    char *panel[2];    /* rounded copies of panels k (alternating buffers)   */
+    int full;          /* panel copies: every panel (1) or two buffers (0) */
+    char *panel[2];    /* rounded copies of panel k (buffer k & 1, or all) */
 } walk_t;
+
+/* FP32 factors: every mode runs its update on the tensor cores when the
+ * tiles allow it.  FP32 accuracy comes from a split of the panel: three
+ * TF32 products of a two-part split, or with PLASMA_FP32_SPLIT=bf16x6
+ * (256-wide tiles) six BF16 products of a three-part split, which moves
+ * 6 instead of 8 operand bytes per element at the same tensor time. */
+static int tc_mode(plasma_desc_t A, int mode)
+{
+    static int split_env = -1;
+    if (split_env < 0) {
+        const char *e = getenv("PLASMA_FP32_SPLIT");
+        split_env = (e != NULL && strcmp(e, "bf16x6") == 0) ? 1 : 0;
+    }
+    return mode == PlasmaFactorTF32 ? PLASMA_TC_TF32
+         : mode == PlasmaFactorBF16 ? PLASMA_TC_BF16
+         : (A.mb == 256 && split_env) ? PLASMA_TC_BF16X6 : PLASMA_TC_TF32X3;
+}
+
+/* the panel copies: two buffers, or one holding every panel */
+static size_t panel_scratch_bytes(plasma_desc_t A, int tc, int full)
+{
+    const size_t one = (plasma_cuda_panel_bytes(tc, A, full) + 1023) & ~(size_t)1023;
+    return (full ? 1 : 2) * one + 1024;
+}
+
+void plasma_pXpotrf_reserve(plasma_context_t *plasma, plasma_enum_t uplo, plasma_desc_t A,
+                            int mode, int full)
+{
+    if (plasma_cuda_update_tc_ok(A, uplo))
+        plasma_scratch(plasma, PLASMA_SLOT_MIXED, panel_scratch_bytes(A, tc_mode(A, mode), full));
+}
+
+static void *panel_buf(walk_t *w, int k)
+{
+    return w->full ? w->panel[0] : w->panel[k & 1];
+}
 
 static void update(walk_t *w, cudaStream_t s, int k, int nlo, int nhi)
 {
     if (w->mode) {
         if (plasma_cuda_update_tc(s, w->st, w->mode, w->A, k, nlo, nhi,
-                                  w->panel[k & 1], w->sms))
+                                  panel_buf(w, k), w->full, w->sms))
             return;
     }
     plasma_cuda_update(s, w->st, w->uplo, w->A, k, nlo, nhi, w->sms);
+}
+
+static void round_panel(walk_t *w, cudaStream_t s, int k)
+{
+    if (w->mode)
+        plasma_cuda_panel_round(s, w->st, w->mode, w->A, k, panel_buf(w, k), w->full);
 }
 
 void plasma_pXpotrf(plasma_context_t *plasma, plasma_enum_t uplo,
@@ -58,6 +103,86 @@ void plasma_pXpotrf_mode(plasma_context_t *plasma, plasma_enum_t uplo,
                          plasma_desc_t A, plasma_sequence_t *sequence,
                          plasma_request_t *request, int call, int mode)
 {
+    plasma_pXpotrf_arrivals(plasma, uplo, A, sequence, request, call, mode, 0, NULL, NULL);
+}
+
+/* The arriving-columns DAG: one update stream per column group.  At step k
+ * the stream of group g applies panel k to its columns from k+2 on, after
+ * the group has arrived; a group that arrives late works through the steps
+ * it missed from the kept panel copies while the critical stream goes on
+ * with the columns that are in.  The stream holding column k+2 splits it
+ * off and records N(k), which the critical stream waits for at step k+1,
+ * as in the one-bulk-stream DAG. */
+static void walk_groups(plasma_context_t *plasma, walk_t *w, int call, int ngroups,
+                        const int *gstart, const cudaEvent_t *arrive)
+{
+    plasma_devstat_t *st = w->st;
+    plasma_enum_t uplo = w->uplo;
+    plasma_desc_t A = w->A;
+    const int mt = A.mt;
+    cudaStream_t S = plasma->stream;
+    cudaStream_t crit = plasma->aux[0];
+    cudaEvent_t ev_start = plasma->ev[0];
+    cudaEvent_t ev_panel = plasma->ev[1];
+    cudaEvent_t ev_next = plasma->ev[2];
+    cudaEvent_t ev_end = plasma->ev[3];
+
+    cudaEventRecord(ev_start, S);
+    cudaStreamWaitEvent(crit, ev_start, 0);
+    for (int g = 0; g < ngroups; g++) {
+        cudaStream_t gs = plasma->aux[3 + g];
+        cudaStreamWaitEvent(gs, ev_start, 0);
+        cudaStreamWaitEvent(gs, arrive[g], 0);
+    }
+    cudaStreamWaitEvent(crit, arrive[0], 0);
+
+    int have_next = 0;
+    int gk = 0;                      /* group of column k + 1 */
+    for (int k = 0; k < mt; k++) {
+        plasma_cuda_potrf_tile(crit, st, call, uplo, A, k, A.nb * k, NULL);
+        plasma_cuda_trsm_panel(crit, st, uplo, A, k, k + 1, mt, NULL);
+        if (k + 1 >= mt)
+            break;
+        while (gstart[gk + 1] <= k + 1) gk++;
+        cudaStreamWaitEvent(crit, arrive[gk], 0);
+        if (have_next)
+            cudaStreamWaitEvent(crit, ev_next, 0);
+        round_panel(w, crit, k);
+        cudaEventRecord(ev_panel, crit);
+        update(w, crit, k, k + 1, k + 2);
+
+        have_next = 0;
+        for (int g = gk; g < ngroups; g++) {
+            const int hi = gstart[g + 1];
+            const int lo = gstart[g] > k + 2 ? gstart[g] : k + 2;
+            if (lo >= hi)
+                continue;
+            cudaStream_t gs = plasma->aux[3 + g];
+            cudaStreamWaitEvent(gs, ev_panel, 0);
+            if (lo == k + 2) {
+                update(w, gs, k, k + 2, k + 3);
+                cudaEventRecord(ev_next, gs);
+                have_next = 1;
+                if (k + 3 < hi)
+                    update(w, gs, k, k + 3, hi);
+            } else {
+                update(w, gs, k, lo, hi);
+            }
+        }
+    }
+    cudaEventRecord(ev_end, crit);
+    cudaStreamWaitEvent(S, ev_end, 0);
+    for (int g = 0; g < ngroups; g++) {
+        cudaEventRecord(ev_end, plasma->aux[3 + g]);
+        cudaStreamWaitEvent(S, ev_end, 0);
+    }
+}
+
+void plasma_pXpotrf_arrivals(plasma_context_t *plasma, plasma_enum_t uplo,
+                             plasma_desc_t A, plasma_sequence_t *sequence,
+                             plasma_request_t *request, int call, int mode,
+                             int ngroups, const int *gstart, const cudaEvent_t *arrive)
+{
     if (sequence->status != PlasmaSuccess)
         return;
     const int mt = A.mt;
@@ -65,6 +190,16 @@ void plasma_pXpotrf_mode(plasma_context_t *plasma, plasma_enum_t uplo,
         return;
     plasma_devstat_t *st = plasma->dstat;
     cudaStream_t S = plasma->stream;
+    if (ngroups > PLASMA_GROUP_STREAMS) {
+        /* more groups than streams: wait for all of them */
+        for (int g = 0; g < ngroups; g++)
+            cudaStreamWaitEvent(S, arrive[g], 0);
+        ngroups = 0;
+    }
+    const int grouped = ngroups > 0 && plasma->lookahead != 0 && mt >= 3;
+    if (ngroups > 0 && !grouped)
+        for (int g = 0; g < ngroups; g++)
+            cudaStreamWaitEvent(S, arrive[g], 0);
 
     walk_t w;
     w.st = st;
@@ -72,15 +207,14 @@ void plasma_pXpotrf_mode(plasma_context_t *plasma, plasma_enum_t uplo,
     w.A = A;
     w.sms = plasma->num_sms;
     w.mode = 0;
+    w.full = grouped;
     w.panel[0] = w.panel[1] = NULL;
-    /* FP32 factors: every mode runs its update on the tensor cores when the
-     * tiles allow it (FP32 as the three-product TF32 split) */
-    int tc = mode == PlasmaFactorTF32 ? PLASMA_TC_TF32
-           : mode == PlasmaFactorBF16 ? PLASMA_TC_BF16 : PLASMA_TC_TF32X3;
+    int tc = tc_mode(A, mode);
     if (plasma_cuda_update_tc_ok(A, uplo)) {
-        size_t one = (plasma_cuda_panel_bytes(tc, A) + 1023) & ~(size_t)1023;
-        char *buf = (char *)plasma_scratch(plasma, PLASMA_SLOT_MIXED, 2 * one + 1024);
+        char *buf = (char *)plasma_scratch(plasma, PLASMA_SLOT_MIXED,
+                                           panel_scratch_bytes(A, tc, w.full));
         if (buf != NULL) {
+            const size_t one = (plasma_cuda_panel_bytes(tc, A, w.full) + 1023) & ~(size_t)1023;
             buf = (char *)(((uintptr_t)buf + 1023) & ~(uintptr_t)1023);
             w.mode = tc;
             w.panel[0] = buf;
@@ -98,9 +232,14 @@ void plasma_pXpotrf_mode(plasma_context_t *plasma, plasma_enum_t uplo,
             plasma_cuda_potrf_tile(S, st, call, uplo, A, k, A.nb * k, NULL);
             plasma_cuda_trsm_panel(S, st, uplo, A, k, k + 1, mt, NULL);
             if (w.mode)
-                plasma_cuda_panel_round(S, st, w.mode, A, k, w.panel[k & 1]);
+                round_panel(&w, S, k);
             update(&w, S, k, k + 1, mt);
         }
+        return;
+    }
+
+    if (grouped) {
+        walk_groups(plasma, &w, call, ngroups, gstart, arrive);
         return;
     }
 
@@ -127,8 +266,7 @@ void plasma_pXpotrf_mode(plasma_context_t *plasma, plasma_enum_t uplo,
          * the panel buffer that the rounded copy of panel k is about to reuse */
         if (have_next)
             cudaStreamWaitEvent(crit, ev_next, 0);
-        if (w.mode)
-            plasma_cuda_panel_round(crit, st, w.mode, A, k, w.panel[k & 1]);
+        round_panel(&w, crit, k);
         cudaEventRecord(ev_panel, crit);
 
         /* critical: the next panel column */

@@ -54,6 +54,14 @@ int plasma_init(void)
     context_defaults(c);
     c->device = plasma_device_request_g;
 
+    /* The factorization of a matrix that is still arriving keeps about 16
+     * streams busy at once, several of them waiting on uploads; with the
+     * driver's default of 8 hardware queues, streams share queues and a
+     * wait at the head of one holds up the critical stream behind it.  The
+     * setting takes effect when this call creates the CUDA context (an
+     * application that created it earlier sets the variable itself). */
+    setenv("CUDA_DEVICE_MAX_CONNECTIONS", "32", 0);
+
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -85,20 +93,26 @@ int plasma_init(void)
         return PlasmaErrorEnvironment;
     }
     c->stream = c->own_stream;
-    /* aux[0]: critical path (highest priority), aux[1..]: bulk updates */
+    /* aux[0]: critical path and aux[2]: uploads (highest priority: the
+     * conversion of arriving columns gates the factorization), the others
+     * (bulk and column-group updates) at the lowest priority */
     int prio_lo = 0, prio_hi = 0;
     cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
     for (int i = 0; i < PLASMA_NUM_STREAMS; i++)
         cudaStreamCreateWithPriority(&c->aux[i], cudaStreamNonBlocking,
-                                     i == 0 ? prio_hi : prio_lo);
+                                     i == 0 || i == PLASMA_STREAM_COPY ? prio_hi : prio_lo);
     for (int i = 0; i < 8; i++)
         cudaEventCreateWithFlags(&c->ev[i], cudaEventDisableTiming);
+    for (int i = 0; i < PLASMA_GROUP_STREAMS; i++)
+        cudaEventCreateWithFlags(&c->ev_group[i], cudaEventDisableTiming);
     if (cudaMalloc((void **)&c->dstat, sizeof(plasma_devstat_t)) != cudaSuccess ||
+        cudaMalloc((void **)&c->dquiet, sizeof(plasma_devstat_t)) != cudaSuccess ||
         cudaMallocHost((void **)&c->hstat, sizeof(plasma_devstat_t)) != cudaSuccess) {
         plasma_error("cannot allocate the device status word");
         return PlasmaErrorOutOfMemory;
     }
     cudaMemset(c->dstat, 0, sizeof(plasma_devstat_t));
+    cudaMemset(c->dquiet, 0, sizeof(plasma_devstat_t));
     cudaDeviceSynchronize();
     plasma_initialized_g = 1;
     return PlasmaSuccess;
@@ -120,9 +134,12 @@ int plasma_finalize(void)
         if (c->scratch[i]) cudaFree(c->scratch[i]);
     for (int i = 0; i < 8; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    for (int i = 0; i < PLASMA_GROUP_STREAMS; i++)
+        if (c->ev_group[i]) cudaEventDestroy(c->ev_group[i]);
     if (c->sweep_sync) cudaFree(c->sweep_sync);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->dstat) cudaFree(c->dstat);
+    if (c->dquiet) cudaFree(c->dquiet);
     if (c->hstat) cudaFreeHost(c->hstat);
     for (int i = 0; i < PLASMA_NUM_STREAMS; i++)
         if (c->aux[i]) cudaStreamDestroy(c->aux[i]);

@@ -38,11 +38,11 @@ __device__ __forceinline__ TileBox tile_box(const plasma_desc_t &A, int m, int n
 
 template <typename T, bool TO_TILE>
 __global__ void __launch_bounds__(kThreads)
-k_lapack_tile(plasma_desc_t A, int uplo, T *pA, int lda,
+k_lapack_tile(plasma_desc_t A, int uplo, T *pA, int lda, int n0,
               const plasma_devstat_t *st)
 {
     if (plasma_failed(st)) return;
-    int m = blockIdx.x, n = blockIdx.y;
+    int m = blockIdx.x, n = blockIdx.y + n0;
     if (!tile_in(uplo, m, n)) return;
     TileBox b = tile_box(A, m, n);
     T *tile = (T *)plasma_tile_addr(A, m, n);
@@ -64,11 +64,11 @@ k_lapack_tile(plasma_desc_t A, int uplo, T *pA, int lda,
 // overflow test (info = 1 when |a| > FLT_MAX; NaN passes, as in LAPACK).
 template <typename TA, typename TB, bool CHECK>
 __global__ void __launch_bounds__(kThreads)
-k_tile_copy(plasma_desc_t A, plasma_desc_t B, int uplo,
+k_tile_copy(plasma_desc_t A, plasma_desc_t B, int uplo, int n0,
             plasma_devstat_t *st, int call)
 {
     if (plasma_failed(st)) return;
-    int m = blockIdx.x, n = blockIdx.y;
+    int m = blockIdx.x, n = blockIdx.y + n0;
     if (!tile_in(uplo, m, n)) return;
     // source and destination may have different (padded) shapes
     int rows = min(plasma_tile_mview(A, m), plasma_tile_mview(B, m));
@@ -179,10 +179,10 @@ extern "C" void plasma_cuda_lapack_to_tile(cudaStream_t s, plasma_devstat_t *st,
     PLASMA_COUNT_LAUNCH();
     if (A.precision == PlasmaRealDouble)
         k_lapack_tile<double, true><<<tile_grid(A), kThreads, 0, s>>>(
-            A, uplo, (double *)pA, lda, st);
+            A, uplo, (double *)pA, lda, 0, st);
     else
         k_lapack_tile<float, true><<<tile_grid(A), kThreads, 0, s>>>(
-            A, uplo, (float *)pA, lda, st);
+            A, uplo, (float *)pA, lda, 0, st);
 }
 
 extern "C" void plasma_cuda_tile_to_lapack(cudaStream_t s, plasma_devstat_t *st,
@@ -193,10 +193,10 @@ extern "C" void plasma_cuda_tile_to_lapack(cudaStream_t s, plasma_devstat_t *st,
     PLASMA_COUNT_LAUNCH();
     if (A.precision == PlasmaRealDouble)
         k_lapack_tile<double, false><<<tile_grid(A), kThreads, 0, s>>>(
-            A, uplo, (double *)pA, lda, st);
+            A, uplo, (double *)pA, lda, 0, st);
     else
         k_lapack_tile<float, false><<<tile_grid(A), kThreads, 0, s>>>(
-            A, uplo, (float *)pA, lda, st);
+            A, uplo, (float *)pA, lda, 0, st);
 }
 
 extern "C" void plasma_cuda_lacpy(cudaStream_t s, plasma_devstat_t *st,
@@ -206,10 +206,10 @@ extern "C" void plasma_cuda_lacpy(cudaStream_t s, plasma_devstat_t *st,
     PLASMA_COUNT_LAUNCH();
     if (A.precision == PlasmaRealDouble)
         k_tile_copy<double, double, false><<<tile_grid(A), kThreads, 0, s>>>(
-            A, B, PlasmaGeneral, st, 0);
+            A, B, PlasmaGeneral, 0, st, 0);
     else
         k_tile_copy<float, float, false><<<tile_grid(A), kThreads, 0, s>>>(
-            A, B, PlasmaGeneral, st, 0);
+            A, B, PlasmaGeneral, 0, st, 0);
 }
 
 // As (lower tiles) <- A held in upper storage: the conversion of dsposv
@@ -230,7 +230,29 @@ extern "C" void plasma_cuda_lag2s(cudaStream_t s, plasma_devstat_t *st, int call
     if (A.mt == 0 || A.nt == 0) return;
     PLASMA_COUNT_LAUNCH();
     k_tile_copy<double, float, true><<<tile_grid(A), kThreads, 0, s>>>(
-        A, As, uplo, st, call);
+        A, As, uplo, 0, st, call);
+}
+
+// Tile columns [n0, n1) only: the FP64 tiles of A from a column-major copy
+// (src, ld: the whole matrix) and their FP32 conversion into As, lower
+// tiles -- the per-group conversion of an upload that runs alongside the
+// factorization of the groups before it.
+extern "C" void plasma_cuda_upload_cols(cudaStream_t s, plasma_devstat_t *st,
+                                        const plasma_devstat_t *quiet, int call,
+                                        plasma_desc_t A, plasma_desc_t As, const double *src,
+                                        int ld, int n0, int n1)
+{
+    if (n1 <= n0 || A.mt == 0) return;
+    PLASMA_COUNT_LAUNCH();
+    dim3 grid((unsigned)A.mt, (unsigned)(n1 - n0));
+    // the FP64 tiles are needed whatever the FP32 factorization reports
+    // (the later attempts and the FP64 fallback read them): they follow a
+    // status word that no kernel sets
+    k_lapack_tile<double, true><<<grid, kThreads, 0, s>>>(A, PlasmaLower, (double *)src, ld,
+                                                           n0, quiet);
+    PLASMA_COUNT_LAUNCH();
+    k_tile_copy<double, float, true><<<grid, kThreads, 0, s>>>(A, As, PlasmaLower, n0, st,
+                                                               call);
 }
 
 extern "C" void plasma_cuda_slag2d(cudaStream_t s, plasma_devstat_t *st,
@@ -239,7 +261,7 @@ extern "C" void plasma_cuda_slag2d(cudaStream_t s, plasma_devstat_t *st,
     if (A.mt == 0 || A.nt == 0) return;
     PLASMA_COUNT_LAUNCH();
     k_tile_copy<float, double, false><<<tile_grid(As), kThreads, 0, s>>>(
-        As, A, PlasmaGeneral, st, 0);
+        As, A, PlasmaGeneral, 0, st, 0);
 }
 
 extern "C" void plasma_cuda_geadd(cudaStream_t s, plasma_devstat_t *st,

@@ -11,7 +11,14 @@
 //   BF16   : one kind::f16 MMA per k-step on the BF16-rounded panel;
 //   TF32X3 : the panel split as a = hi + lo (hi = tf32(a), lo = tf32(a - hi))
 //            and a*b formed as lo*hi + hi*lo + hi*hi, three kind::tf32 MMAs,
-//            which keeps about 22 bits of every product (the FP32 factor).
+//            which keeps about 22 bits of every product (the FP32 factor);
+//   BF16X6 : the panel split in three BF16 parts, a = h + m + l (h = bf16(a),
+//            m = bf16(a - h), l = bf16(a - h - m)), and a*b formed from the six
+//            products whose order is at most 2^-16 (l*h, h*l, m*m, m*h, h*m,
+//            h*h), six kind::f16 MMAs: about 23 bits of every product, the
+//            same tensor time as TF32X3 (a BF16 MMA covers twice the K) and
+//            6 instead of 8 operand bytes per element (the FP32 factor on
+//            256-wide tiles, CTA-pair kernel only).
 //
 // One CTA owns a run of `ipc` consecutive work items (a 128 x nb block of one
 // output tile each; items of one tile column are adjacent, so they share the
@@ -53,17 +60,19 @@ constexpr int TC_STAGE_BYTES = 48 * 1024;
 constexpr int TC_EPI_BUF_BYTES = 32 * 32 * 4;
 
 enum { MODE_TF32 = PLASMA_TC_TF32, MODE_BF16 = PLASMA_TC_BF16,
-       MODE_TF32X3 = PLASMA_TC_TF32X3 };
+       MODE_TF32X3 = PLASMA_TC_TF32X3, MODE_BF16X6 = PLASMA_TC_BF16X6 };
 
 template <int MODE>
 struct Geo {
-    static constexpr int ESZ = MODE == MODE_BF16 ? 2 : 4;
+    static constexpr bool HALF16 = MODE == MODE_BF16 || MODE == MODE_BF16X6;
+    static constexpr int ESZ = HALF16 ? 2 : 4;
     static constexpr int MNBOX = 128 / ESZ;           // elements per 128-byte row
-    static constexpr int BK = MODE == MODE_BF16 ? 64 : (MODE == MODE_TF32 ? 32 : 16);
-    static constexpr int KI = MODE == MODE_BF16 ? 16 : 8;   // K per instruction
-    static constexpr int PARTS = MODE == MODE_TF32X3 ? 2 : 1;
-    static constexpr uint32_t LAYOUT = MODE == MODE_BF16 ? 2u : 1u;
-    static constexpr uint32_t SBO = MODE == MODE_BF16 ? 1024u : 512u;
+    static constexpr int BK = MODE == MODE_BF16 ? 64
+                            : (MODE == MODE_TF32 || MODE == MODE_BF16X6) ? 32 : 16;
+    static constexpr int KI = HALF16 ? 16 : 8;        // K per instruction
+    static constexpr int PARTS = MODE == MODE_TF32X3 ? 2 : MODE == MODE_BF16X6 ? 3 : 1;
+    static constexpr uint32_t LAYOUT = HALF16 ? 2u : 1u;
+    static constexpr uint32_t SBO = HALF16 ? 1024u : 512u;
     static constexpr int CHUNK = BK * 128;            // one MN chunk of a stage
     static constexpr int A_BYTES = (TC_M / MNBOX) * CHUNK;
     // TF32X3 moves twice the operand bytes per product: a deeper ring (more
@@ -226,7 +235,8 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
 struct TcArgs {
     plasma_desc_t A;    // FP32 general or packed-lower descriptor holding C
     int k, nlo, nhi;
-    int mt;             // tiles per part in the operand map (lo part at +mt)
+    int poff;           // operand tile of panel row m: poff + m (first part)
+    int mt;             // tiles per part in the operand map (part p at +p*mt)
     long long nitems;
     int ipc;            // items per CTA
 };
@@ -315,7 +325,7 @@ k_update_tc(const __grid_constant__ CUtensorMap opmap,
                 for (int p = 0; p < G::PARTS; p++) {
                     unsigned char *sa = sp + p * G::A_BYTES;
                     unsigned char *sb = sp + G::PARTS * G::A_BYTES + p * b_bytes;
-                    const int toff = p * g.mt;
+                    const int toff = g.poff + p * g.mt;
                     tma_load_4d(sa, &opmap, &full_bar[s], 0, kb * G::BK,
                                 i0 / G::MNBOX, m + toff);
                     for (int c = 0; c < nb / TC_M; c++)
@@ -457,15 +467,16 @@ k_update_tc(const __grid_constant__ CUtensorMap opmap,
 // tensor memory is freed; every loop in between ends (waits are bounded),
 // so both CTAs always reach them.
 // ---------------------------------------------------------------------------
-constexpr int PAIR_STAGE_BYTES = 32 * 1024;
-
 template <int MODE>
 struct PairGeo {
     using G = Geo<MODE>;
-    static constexpr int EPI_BUFS = MODE == MODE_TF32X3 ? 1 : 2;
-    static constexpr int STAGES = MODE == MODE_TF32X3 ? 6 : 5;
-    static constexpr int SMEM = STAGES * PAIR_STAGE_BYTES +
+    // per part: 128 rows of A(m,k) and 128 rows of A(n,k), BK columns each
+    static constexpr int STAGE = G::PARTS * 2 * G::A_BYTES;   // 32 KB, BF16X6 48 KB
+    static constexpr int EPI_BUFS = MODE == MODE_TF32X3 || MODE == MODE_BF16X6 ? 1 : 2;
+    static constexpr int STAGES = MODE == MODE_TF32X3 ? 6 : MODE == MODE_BF16X6 ? 4 : 5;
+    static constexpr int SMEM = STAGES * STAGE +
                                 TC_EPI_WARPS * EPI_BUFS * TC_EPI_BUF_BYTES + 1024;
+    static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
 __device__ __forceinline__ uint32_t cluster_rank()
@@ -539,7 +550,7 @@ __device__ __forceinline__ void mma_pair(uint32_t tmem, uint64_t a, uint64_t b,
                                          uint32_t idesc, uint32_t acc)
 {
     const uint32_t z = 0;
-    if (MODE != MODE_BF16)
+    if (!Geo<MODE>::HALF16)
         asm volatile(
             "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
             "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, "
@@ -565,7 +576,7 @@ __device__ __forceinline__ void mma_commit_pair(uint64_t *bar)
 
 __device__ __forceinline__ uint32_t instr_desc_pair(int mode)
 {
-    uint32_t fmt = mode == MODE_BF16 ? 1u : 2u;
+    uint32_t fmt = mode == MODE_BF16 || mode == MODE_BF16X6 ? 1u : 2u;
     return (1u << 4) | (fmt << 7) | (fmt << 10) | (1u << 15) | (1u << 16) |
            ((uint32_t)(256 >> 3) << 17) | ((uint32_t)(256 >> 4) << 24);
 }
@@ -599,10 +610,9 @@ k_update_pair(const __grid_constant__ CUtensorMap opmap,
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     unsigned char *stage_base =
         (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    // per part: 128 rows of A(m,k) then 128 rows of A(n,k), BK columns each
+    // stage: the PARTS parts of 128 rows of A(m,k), then those of A(n,k)
     constexpr int HALF = G::A_BYTES;
-    constexpr int STAGE_BYTES = G::PARTS * 2 * HALF;
-    static_assert(STAGE_BYTES == PAIR_STAGE_BYTES, "stage size");
+    constexpr int STAGE_BYTES = P::STAGE;
     constexpr int nkb = NB / G::BK;
     constexpr uint32_t tmem_cols = 2 * NB;
 
@@ -656,12 +666,12 @@ k_update_pair(const __grid_constant__ CUtensorMap opmap,
                     ok = false;
                     break;
                 }
-                unsigned char *sp = stage_base + s * PAIR_STAGE_BYTES;
+                unsigned char *sp = stage_base + s * STAGE_BYTES;
                 const uint32_t fb = full_lead0 + (uint32_t)(s * sizeof(uint64_t));
                 if (leader) mbar_expect_tx(&full_bar[s], 2u * (uint32_t)STAGE_BYTES);
 #pragma unroll
                 for (int p = 0; p < G::PARTS; p++) {
-                    const int toff = p * g.mt;
+                    const int toff = g.poff + p * g.mt;
                     tma_load_4d_pair(sp + p * HALF, &opmap, fb, 0, kb * G::BK,
                                      row0 / G::MNBOX, m + toff);
                     tma_load_4d_pair(sp + (G::PARTS + p) * HALF, &opmap, fb, 0, kb * G::BK,
@@ -687,7 +697,7 @@ k_update_pair(const __grid_constant__ CUtensorMap opmap,
                     break;
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                unsigned char *sp = stage_base + s * PAIR_STAGE_BYTES;
+                unsigned char *sp = stage_base + s * STAGE_BYTES;
                 unsigned char *sa_hi = sp;
                 unsigned char *sb_hi = sp + G::PARTS * HALF;
 #pragma unroll
@@ -705,6 +715,22 @@ k_update_pair(const __grid_constant__ CUtensorMap opmap,
                         mma_pair<MODE>(acc_t, dal, db, idesc, acc_on);
                         mma_pair<MODE>(acc_t, da, dbl, idesc, 1u);
                         mma_pair<MODE>(acc_t, da, db, idesc, 1u);
+                    } else if (MODE == MODE_BF16X6) {
+                        // parts h, m, l at offsets 0, HALF, 2 HALF; small terms first
+                        uint64_t dam = smem_desc(sa_hi + HALF + kk * G::KI * 128, G::CHUNK,
+                                                 G::SBO, G::LAYOUT);
+                        uint64_t dal = smem_desc(sa_hi + 2 * HALF + kk * G::KI * 128,
+                                                 G::CHUNK, G::SBO, G::LAYOUT);
+                        uint64_t dbm = smem_desc(sb_hi + HALF + kk * G::KI * 128, G::CHUNK,
+                                                 G::SBO, G::LAYOUT);
+                        uint64_t dbl = smem_desc(sb_hi + 2 * HALF + kk * G::KI * 128,
+                                                 G::CHUNK, G::SBO, G::LAYOUT);
+                        mma_pair<MODE>(acc_t, dal, db, idesc, acc_on);
+                        mma_pair<MODE>(acc_t, da, dbl, idesc, 1u);
+                        mma_pair<MODE>(acc_t, dam, dbm, idesc, 1u);
+                        mma_pair<MODE>(acc_t, dam, db, idesc, 1u);
+                        mma_pair<MODE>(acc_t, da, dbm, idesc, 1u);
+                        mma_pair<MODE>(acc_t, da, db, idesc, 1u);
                     } else {
                         mma_pair<MODE>(acc_t, da, db, idesc, acc_on);
                     }
@@ -718,7 +744,7 @@ k_update_pair(const __grid_constant__ CUtensorMap opmap,
         const int e = warp - TC_EPI_WARP0;
         const int q = warp & 3;
         const int half = e / 4;
-        float *stage_epi = (float *)(stage_base + STAGES * PAIR_STAGE_BYTES) +
+        float *stage_epi = (float *)(stage_base + STAGES * STAGE_BYTES) +
                            (size_t)e * EPI_BUFS * (TC_EPI_BUF_BYTES / 4);
         int nchunk = 0;
         for (int j = 0; j < nit; j++) {
@@ -887,6 +913,31 @@ long long choose_ipc(long long nitems, int unit, long long sms, int max_items)
 
 }  // namespace
 
+// Layout of the rounded panel copies.  full = 0: one panel per buffer (the
+// caller alternates two), row tile m of the panel at tile m, part p at
+// + p * mt.  full = 1: every panel of the factor, row tile m of panel k at
+// k*mt - k(k-1)/2 + (m - k) (packed lower order), part p at + p * T with
+// T = mt(mt+1)/2 -- the storage a trailing update that lags behind the
+// panel stream reads from.
+namespace {
+void panel_layout(const plasma_desc_t &A, int k, int full, int *poff, int *pstride)
+{
+    const int mt = A.mt;
+    if (!full) {
+        *poff = 0;
+        *pstride = mt;
+    } else {
+        *poff = k * mt - k * (k - 1) / 2 - k;
+        *pstride = mt * (mt + 1) / 2;
+    }
+}
+
+int mode_parts(int mode)
+{
+    return mode == PLASMA_TC_TF32X3 ? 2 : mode == PLASMA_TC_BF16X6 ? 3 : 1;
+}
+}  // namespace
+
 // Eligibility of the tensor-core update for an FP32 descriptor: general or
 // packed-lower storage, lower, square tiles of 128 or 256, no ragged tile.
 extern "C" int plasma_cuda_update_tc_ok(plasma_desc_t A, plasma_enum_t uplo)
@@ -897,24 +948,23 @@ extern "C" int plasma_cuda_update_tc_ok(plasma_desc_t A, plasma_enum_t uplo)
            A.gm % A.mb == 0 && A.gn % A.nb == 0 && A.i == 0 && A.j == 0;
 }
 
-// Bytes of one operand copy of a panel (plasma_cuda_panel_round).
-extern "C" size_t plasma_cuda_panel_bytes(int mode, plasma_desc_t A)
+// Bytes of the operand copies (plasma_cuda_panel_round): one panel
+// (full = 0) or all panels of the factor (full = 1).
+extern "C" size_t plasma_cuda_panel_bytes(int mode, plasma_desc_t A, int full)
 {
-    size_t tile = (size_t)A.mb * A.mb;
-    switch (mode) {
-    case PLASMA_TC_BF16: return (size_t)A.mt * tile * 2;
-    case PLASMA_TC_TF32: return (size_t)A.mt * tile * 4;
-    case PLASMA_TC_TF32X3: return 2 * (size_t)A.mt * tile * 4;
-    default: return 0;
-    }
+    if (mode < PLASMA_TC_TF32 || mode > PLASMA_TC_BF16X6) return 0;
+    int poff, pstride;
+    panel_layout(A, 0, full, &poff, &pstride);
+    const size_t esz = mode == PLASMA_TC_BF16 || mode == PLASMA_TC_BF16X6 ? 2 : 4;
+    return (size_t)mode_parts(mode) * pstride * A.mb * A.mb * esz;
 }
 
 // The operands come from `panel`: the copy of panel k made by
-// plasma_cuda_panel_round for the same mode, 1024-byte aligned.  Returns 0
-// (nothing launched) when the update is not eligible.
+// plasma_cuda_panel_round for the same mode and layout (`full`), 1024-byte
+// aligned.  Returns 0 (nothing launched) when the update is not eligible.
 extern "C" int plasma_cuda_update_tc(cudaStream_t s, plasma_devstat_t *st,
                                      int mode, plasma_desc_t A, int k, int nlo,
-                                     int nhi, const void *panel, int num_sms)
+                                     int nhi, const void *panel, int full, int num_sms)
 {
     if (nhi <= nlo) return 1;
     const int nb = A.mb;
@@ -926,21 +976,29 @@ extern "C" int plasma_cuda_update_tc(cudaStream_t s, plasma_devstat_t *st,
         ((uintptr_t)A.matrix & 15) != 0)
         return 0;
 
+    int poff, pstride;
+    panel_layout(A, k, full, &poff, &pstride);
+    const long long ntiles = (long long)mode_parts(mode) * pstride;
     CUtensorMap map, cmap;
     bool enc;
     switch (mode) {
     case PLASMA_TC_TF32:
         enc = encode_tile_map(&map, (void *)panel, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, nb,
-                              A.mt, Geo<MODE_TF32>::BK, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B);
+                              ntiles, Geo<MODE_TF32>::BK, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B);
         break;
     case PLASMA_TC_TF32X3:
         enc = encode_tile_map(&map, (void *)panel, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, nb,
-                              2LL * A.mt, Geo<MODE_TF32X3>::BK,
+                              ntiles, Geo<MODE_TF32X3>::BK,
                               CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B);
         break;
     case PLASMA_TC_BF16:
         enc = encode_tile_map(&map, (void *)panel, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, nb,
-                              A.mt, Geo<MODE_BF16>::BK, CU_TENSOR_MAP_SWIZZLE_128B);
+                              ntiles, Geo<MODE_BF16>::BK, CU_TENSOR_MAP_SWIZZLE_128B);
+        break;
+    case PLASMA_TC_BF16X6:
+        if (nb != 2 * TC_M) return 0;                 // CTA-pair kernel only
+        enc = encode_tile_map(&map, (void *)panel, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, nb,
+                              ntiles, Geo<MODE_BF16X6>::BK, CU_TENSOR_MAP_SWIZZLE_128B);
         break;
     default:
         return 0;
@@ -953,7 +1011,8 @@ extern "C" int plasma_cuda_update_tc(cudaStream_t s, plasma_devstat_t *st,
     g.k = k;
     g.nlo = nlo;
     g.nhi = nhi;
-    g.mt = A.mt;
+    g.poff = poff;
+    g.mt = pstride;
     // PLASMA_UPDATE_MAX_ITEMS caps the items per CTA (default 8): shorter
     // CTAs hand SMs back to the panel stream sooner.  PLASMA_UPDATE_PAIR
     // selects the CTA-pair kernel for 256-wide tiles (default on; 0 = off).
@@ -966,7 +1025,7 @@ extern "C" int plasma_cuda_update_tc(cudaStream_t s, plasma_devstat_t *st,
         pair_mode = env ? atoi(env) != 0 : 1;
     }
     const long long sms = num_sms > 0 ? num_sms : 148;
-    const bool use_pair = pair_mode && nb == 2 * TC_M;
+    const bool use_pair = (pair_mode || mode == PLASMA_TC_BF16X6) && nb == 2 * TC_M;
     unsigned grid;
     if (use_pair) {
         g.nitems = tiles;
@@ -993,6 +1052,7 @@ extern "C" int plasma_cuda_update_tc(cudaStream_t s, plasma_devstat_t *st,
         switch (mode) {
         case PLASMA_TC_TF32: launch_pair<MODE_TF32>(s, map, cmap, g, grid, st); break;
         case PLASMA_TC_TF32X3: launch_pair<MODE_TF32X3>(s, map, cmap, g, grid, st); break;
+        case PLASMA_TC_BF16X6: launch_pair<MODE_BF16X6>(s, map, cmap, g, grid, st); break;
         default: launch_pair<MODE_BF16>(s, map, cmap, g, grid, st); break;
         }
     } else {
@@ -1013,7 +1073,7 @@ extern "C" int plasma_cuda_update_tc(cudaStream_t s, plasma_devstat_t *st,
 // (a - hi is exact in FP32).
 namespace {
 template <int MODE>
-__global__ void k_panel_round(plasma_desc_t A, int k, void *panel,
+__global__ void k_panel_round(plasma_desc_t A, int k, void *panel, int poff, int pstride,
                               const plasma_devstat_t *st)
 {
     if (plasma_failed(st)) return;
@@ -1021,14 +1081,30 @@ __global__ void k_panel_round(plasma_desc_t A, int k, void *panel,
     const int nb = A.mb;
     const float4 *a = (const float4 *)plasma_tile_addr(A, m, k);
     const size_t tot = (size_t)nb * nb;
+    const size_t t = (size_t)poff + m;          // operand tile of row m
     for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot / 4;
          e += (size_t)gridDim.x * blockDim.x) {
         const float4 x = a[e];
         const float xs[4] = {x.x, x.y, x.z, x.w};
         if (MODE == MODE_BF16) {
-            __nv_bfloat16 *o = (__nv_bfloat16 *)panel + (size_t)m * tot + 4 * e;
+            __nv_bfloat16 *o = (__nv_bfloat16 *)panel + t * tot + 4 * e;
 #pragma unroll
             for (int i = 0; i < 4; i++) o[i] = __float2bfloat16_rn(xs[i]);
+        } else if (MODE == MODE_BF16X6) {
+            // h, m, l planes at tiles m, m + mt, m + 2 mt; both differences
+            // are exact in FP32 (each drops the leading 8 significant bits)
+            __nv_bfloat16 *o = (__nv_bfloat16 *)panel + t * tot + 4 * e;
+            const size_t plane = (size_t)pstride * tot;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const __nv_bfloat16 h = __float2bfloat16_rn(xs[i]);
+                const float r1 = xs[i] - __bfloat162float(h);
+                const __nv_bfloat16 md = __float2bfloat16_rn(r1);
+                const float r2 = r1 - __bfloat162float(md);
+                o[i] = h;
+                o[plane + i] = md;
+                o[2 * plane + i] = __float2bfloat16_rn(r2);
+            }
         } else {
             uint32_t hi[4], lo[4];
 #pragma unroll
@@ -1039,10 +1115,10 @@ __global__ void k_panel_round(plasma_desc_t A, int k, void *panel,
                     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo[i]) : "f"(r));
                 }
             }
-            uint4 *o = (uint4 *)panel + ((size_t)m * tot) / 4 + e;
+            uint4 *o = (uint4 *)panel + (t * tot) / 4 + e;
             *o = make_uint4(hi[0], hi[1], hi[2], hi[3]);
             if (MODE == MODE_TF32X3) {
-                uint4 *ol = (uint4 *)panel + ((size_t)(m + A.mt) * tot) / 4 + e;
+                uint4 *ol = (uint4 *)panel + ((t + pstride) * tot) / 4 + e;
                 *ol = make_uint4(lo[0], lo[1], lo[2], lo[3]);
             }
         }
@@ -1052,15 +1128,26 @@ __global__ void k_panel_round(plasma_desc_t A, int k, void *panel,
 
 extern "C" void plasma_cuda_panel_round(cudaStream_t s, plasma_devstat_t *st,
                                         int mode, plasma_desc_t A, int k,
-                                        void *panel)
+                                        void *panel, int full)
 {
     int rows = A.mt - k - 1;
     if (rows <= 0) return;
+    int poff, pstride;
+    panel_layout(A, k, full, &poff, &pstride);
     PLASMA_COUNT_LAUNCH();
     dim3 grid(16, rows);
     switch (mode) {
-    case PLASMA_TC_BF16: k_panel_round<MODE_BF16><<<grid, 256, 0, s>>>(A, k, panel, st); break;
-    case PLASMA_TC_TF32X3: k_panel_round<MODE_TF32X3><<<grid, 256, 0, s>>>(A, k, panel, st); break;
-    default: k_panel_round<MODE_TF32><<<grid, 256, 0, s>>>(A, k, panel, st); break;
+    case PLASMA_TC_BF16:
+        k_panel_round<MODE_BF16><<<grid, 256, 0, s>>>(A, k, panel, poff, pstride, st);
+        break;
+    case PLASMA_TC_TF32X3:
+        k_panel_round<MODE_TF32X3><<<grid, 256, 0, s>>>(A, k, panel, poff, pstride, st);
+        break;
+    case PLASMA_TC_BF16X6:
+        k_panel_round<MODE_BF16X6><<<grid, 256, 0, s>>>(A, k, panel, poff, pstride, st);
+        break;
+    default:
+        k_panel_round<MODE_TF32><<<grid, 256, 0, s>>>(A, k, panel, poff, pstride, st);
+        break;
     }
 }

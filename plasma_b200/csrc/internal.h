@@ -34,7 +34,11 @@ typedef struct {
 } plasma_devstat_t;
 
 #define PLASMA_MAX_PENDING_CALLS 4096
-#define PLASMA_NUM_STREAMS 4
+/* aux[0]: critical path, aux[1]: bulk updates, aux[2]: uploads,
+ * aux[3 ..]: one update stream per group of arriving tile columns */
+#define PLASMA_NUM_STREAMS 16
+#define PLASMA_STREAM_COPY 2
+#define PLASMA_GROUP_STREAMS (PLASMA_NUM_STREAMS - 3)
 #define PLASMA_SCRATCH_SLOTS 9
 
 /* scratch slots */
@@ -69,6 +73,8 @@ typedef struct {
     cudaStream_t own_stream;                 /* created by plasma_init()    */
     cudaStream_t aux[PLASMA_NUM_STREAMS];    /* look-ahead / update streams */
     plasma_devstat_t *dstat;                 /* device status word          */
+    plasma_devstat_t *dquiet;                /* a status word no kernel sets
+                                                (work that must complete)  */
     plasma_devstat_t *hstat;                 /* pinned host mirror          */
 
     /* ids of plasma_omp_* calls since the last plasma_sequence_wait() */
@@ -82,6 +88,7 @@ typedef struct {
     void  *pinned;
     size_t pinned_bytes;
     cudaEvent_t ev[8];                        /* DAG edges (reused)        */
+    cudaEvent_t ev_group[PLASMA_GROUP_STREAMS]; /* arrival of column groups */
     /* ready flags of the one-launch triangular sweeps */
     void  *sweep_sync;
     size_t sweep_sync_bytes;
@@ -170,6 +177,13 @@ int plasma_cuda_lansy_tiles(cudaStream_t s, plasma_devstat_t *st,
 void plasma_cuda_lansy_inf(cudaStream_t s, plasma_devstat_t *st,
                            plasma_enum_t uplo, plasma_desc_t A,
                            double *dnorm, double *work);
+/* Tile columns [n0, n1) of a host upload in flight: FP64 tiles of A (lower)
+ * from the column-major device copy src (leading dimension ld) and their
+ * FP32 conversion into As (dlag2s overflow test). */
+void plasma_cuda_upload_cols(cudaStream_t s, plasma_devstat_t *st,
+                             const plasma_devstat_t *quiet, int call,
+                             plasma_desc_t A, plasma_desc_t As, const double *src,
+                             int ld, int n0, int n1);
 /* As (lower tiles) <- (float)A with A in upper storage (transposed tiles). */
 void plasma_cuda_lag2s_upper_to_lower(cudaStream_t s, plasma_devstat_t *st, int call,
                                       plasma_desc_t A, plasma_desc_t As);
@@ -196,16 +210,21 @@ void plasma_cuda_lacpy(cudaStream_t s, plasma_devstat_t *st,
 #define PLASMA_TC_TF32   1   /* one TF32 product                         */
 #define PLASMA_TC_BF16   2   /* one BF16 product                         */
 #define PLASMA_TC_TF32X3 3   /* lo*hi + hi*lo + hi*hi TF32 split (FP32)   */
+#define PLASMA_TC_BF16X6 4   /* six products of a three-part BF16 split
+                                (FP32; 256-wide tiles)                     */
 int plasma_cuda_update_tc_ok(plasma_desc_t A, plasma_enum_t uplo);
-size_t plasma_cuda_panel_bytes(int tc_mode, plasma_desc_t A);
+/* Operand copies of the panels: full = 0 holds one panel (the caller
+ * alternates two buffers), full = 1 every panel of the factor, so that an
+ * update may lag any number of steps behind the panel stream. */
+size_t plasma_cuda_panel_bytes(int tc_mode, plasma_desc_t A, int full);
 int plasma_cuda_update_tc(cudaStream_t s, plasma_devstat_t *st, int tc_mode,
                           plasma_desc_t A, int k, int nlo, int nhi,
-                          const void *panel, int num_sms);
-/* Copy of panel k in the operand format of tc_mode (plasma_cuda_panel_bytes
- * bytes, tile m at panel + m*nb*nb elements; TF32X3 adds the low parts at
- * tile m + mt). */
+                          const void *panel, int full, int num_sms);
+/* Copy of panel k in the operand format of tc_mode, in the layout `full`
+ * (row tile m of the panel at tile m, or at k*mt - k(k-1)/2 + m - k; the
+ * further parts of a split at one plane further each). */
 void plasma_cuda_panel_round(cudaStream_t s, plasma_devstat_t *st, int tc_mode,
-                             plasma_desc_t A, int k, void *panel);
+                             plasma_desc_t A, int k, void *panel, int full);
 /* FP32 diagonal tile held in shared memory (order a multiple of 32, at most
  * 256); 0 when not applicable. */
 int plasma_cuda_potrf_diag_smem(cudaStream_t s, plasma_devstat_t *st, int call,
@@ -294,6 +313,18 @@ void plasma_pXpotrf(plasma_context_t *plasma, plasma_enum_t uplo,
 void plasma_pXpotrf_mode(plasma_context_t *plasma, plasma_enum_t uplo,
                          plasma_desc_t A, plasma_sequence_t *sequence,
                          plasma_request_t *request, int call, int mode);
+/* The same factorization of a matrix whose tile columns are still arriving:
+ * group g = tile columns [gstart[g], gstart[g+1]) is in place once event
+ * arrive[g] has completed (gstart[0] = 0, gstart[ngroups] = A.nt,
+ * 1 <= ngroups <= PLASMA_GROUP_STREAMS). */
+/* Grows the panel-copy scratch of plasma_pXpotrf_arrivals beforehand (a
+ * slot that grows waits for every stream). */
+void plasma_pXpotrf_reserve(plasma_context_t *plasma, plasma_enum_t uplo, plasma_desc_t A,
+                            int mode, int full);
+void plasma_pXpotrf_arrivals(plasma_context_t *plasma, plasma_enum_t uplo,
+                             plasma_desc_t A, plasma_sequence_t *sequence,
+                             plasma_request_t *request, int call, int mode,
+                             int ngroups, const int *gstart, const cudaEvent_t *arrive);
 void plasma_pXpotrs(plasma_context_t *plasma, plasma_enum_t uplo,
                     plasma_desc_t A, plasma_desc_t B,
                     plasma_sequence_t *sequence, plasma_request_t *request);

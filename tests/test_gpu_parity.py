@@ -7,6 +7,7 @@ import ctypes
 
 import numpy as np
 import pytest
+import torch
 
 import gen
 import oracle
@@ -531,3 +532,54 @@ def test_dposv_many_rhs(L, uplo):
     xo = np.asfortranarray(b.copy())
     assert oracle.posv(uplo, np.asfortranarray(a.copy()), xo, 128) == 0
     np.testing.assert_allclose(x, xo, rtol=1e-11, atol=1e-14)
+
+
+# ------------------------------------------------------------------ overlapped upload
+def _pinned_colmajor(a):
+    """A page-locked host copy of `a` in column-major order."""
+    a = np.asarray(a)
+    t = torch.empty((a.shape[1], a.shape[0]), dtype=torch.float64, pin_memory=True)
+    t.copy_(torch.from_numpy(np.ascontiguousarray(a.T)))
+    return t
+
+
+@pytest.mark.parametrize("n,nb,kappa", [(3000, 256, 1e3), (2048, 128, 1e5)])
+def test_dsposv_overlapped_upload(L, n, nb, kappa):
+    """A lower-stored host matrix in page-locked memory goes up in groups of
+    tile columns while the factorization of the groups already in place runs
+    (ragged n included): the answer matches the oracle."""
+    set_nb(L, nb)
+    a = gen.spectrum(n, kappa, seed=2100 + n)
+    xt = np.random.default_rng(n).standard_normal((n, 1))
+    b = a @ xt
+    A, B = _pinned_colmajor(a), _pinned_colmajor(b)
+    X = torch.zeros((1, n), dtype=torch.float64, pin_memory=True)
+    it = ctypes.c_int(-99)
+    info = pb.plasma_dsposv_info_t()
+    assert L.plasma_dsposv_ex(LO, n, 1, A.data_ptr(), n, B.data_ptr(), n, X.data_ptr(), n,
+                              ctypes.byref(it), ctypes.byref(info)) == 0
+    assert it.value >= 0
+    x = X.numpy().T.copy()
+    assert solve_residual(a, x, b) < TOL * EPS
+    assert abs(info.anorm - np.abs(a).sum(axis=1).max()) <= 1e-13 * info.anorm
+    xo = np.zeros((n, 1), order="F")
+    assert oracle.dsposv(oracle.LOWER, np.asfortranarray(a), np.asfortranarray(b), xo, nb)[0] == 0
+    # two FP64-accurate solutions differ by about kappa * eps (normwise)
+    assert np.abs(x - xo).max() / np.abs(xo).max() < kappa * 1e-14
+
+
+def test_dsposv_overlapped_upload_fallback(L):
+    """kappa = 1e12: the FP32 factorization fails while later column groups
+    are still on their way; the FP64 tiles of A are completed regardless
+    and the FP64 fallback solves the system (iter = -31)."""
+    set_nb(L, 128)
+    n = 2048
+    a = gen.spectrum(n, 1e12, seed=11)
+    b = np.random.default_rng(1).standard_normal((n, 1))
+    A, B = _pinned_colmajor(a), _pinned_colmajor(b)
+    X = torch.zeros((1, n), dtype=torch.float64, pin_memory=True)
+    it = ctypes.c_int()
+    assert L.plasma_dsposv(LO, n, 1, A.data_ptr(), n, B.data_ptr(), n, X.data_ptr(), n,
+                           ctypes.byref(it)) == 0
+    assert it.value == -31
+    assert solve_residual(a, X.numpy().T.copy(), b) < TOL * EPS
