@@ -59,7 +59,7 @@ def parse():
 
 
 MODES = {"fp32": 0, "tf32": 1, "bf16": 2, "auto": 3}
-UPDATE_DRAM_BYTES_PER_TILE = {"fp32": 389908}
+UPDATE_DRAM_BYTES_PER_TILE = {"fp32": 384465}
 REFINE = {"ir": 0, "gmres": 1, "auto": 2}
 
 
@@ -545,9 +545,10 @@ def main():
                  "bf16": ("bf16", peaks.get("bf16"), 1), "auto": ("bf16", peaks.get("bf16"), 1)}
     pk_name, pk, passes = mode_peak[args.mode]
     achieved = passes * upd["flops"] / upd["ms"] / 1e9 if upd["ms"] > 0 else None
-    # DRAM bytes per 256 x 256 tile-update of k_update_tc, read + write, from
-    # one ncu capture (profiles/k_update_tc_tf32x3_n8192.md: a bulk launch of
-    # 325 tile-updates); a launch's traffic grows with the tiles it updates
+    # DRAM bytes per 256 x 256 tile-update of the CTA-pair update kernel, read
+    # + write, from one ncu capture (profiles/k_update_pair_tf32x3_n8192.md: a
+    # bulk launch of 325 tile-updates); a launch's traffic grows with the
+    # tiles it updates
     # (the algorithmic C read + write is 524288 bytes per tile-update)
     traffic = None
     dram_per_tile = UPDATE_DRAM_BYTES_PER_TILE.get(args.mode)
@@ -575,7 +576,8 @@ def main():
         "dposv": dposv,
         "speedup_vs_dposv": (dposv["ms"] / ms) if dposv else None,
         "roofline": {"bound": "tensor",
-                     "kernel": "k_update_tc trailing update (SYRK+GEMM)",
+                     "kernel": "k_update_pair trailing update (SYRK+GEMM, "
+                               "tcgen05 cta_group::2)",
                      "achieved": achieved, "peak": pk, "unit": "TFLOP/s",
                      "frac": (achieved / pk) if achieved and pk else None,
                      "tensor_products_per_flop": passes,
