@@ -370,7 +370,7 @@ int plasma_sweep_reserve(plasma_context_t *c, plasma_desc_t A)
     int sb = plasma_cuda_trsv_block(A);
     if (sb == 0)
         return 0;
-    size_t need = plasma_cuda_trsv_sync_bytes((A.m + sb - 1) / sb);
+    size_t need = plasma_cuda_trsv_scratch_bytes(A);
     if (need > c->sweep_sync_bytes) {
         if (c->sweep_sync) {
             cudaStreamSynchronize(c->stream);

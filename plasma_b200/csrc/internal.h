@@ -269,6 +269,7 @@ int plasma_cuda_symv(cudaStream_t s, plasma_devstat_t *st, plasma_enum_t uplo,
 int plasma_cuda_trsv_block(plasma_desc_t A);
 size_t plasma_cuda_trsv_sync_bytes(int nblk);
 size_t plasma_cuda_trsv_w_bytes(plasma_desc_t A);
+size_t plasma_cuda_trsv_scratch_bytes(plasma_desc_t A);
 void plasma_cuda_trtri_blocks(cudaStream_t s, plasma_devstat_t *st,
                               plasma_enum_t uplo, plasma_desc_t A, void *W);
 int plasma_cuda_trsv(cudaStream_t s, plasma_devstat_t *st, plasma_enum_t uplo,
