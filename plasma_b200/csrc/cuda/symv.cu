@@ -6,10 +6,11 @@
 //
 // Each stored tile S = A(p,q) is read from HBM exactly once by one CTA, which
 // forms both contributions  S x_q  (to rows of block p)  and  S^T x_p  (to
-// rows of block q).  Lanes own rows, so every warp load is 32 consecutive
-// doubles of one column; the transposed product of a 32x32 block is reduced
-// across lanes by a butterfly (16 columns per warp pass; one CTA per SM
-// keeps the loop in registers).  The per-tile partial vectors go to
+// rows of block q).  Lanes own rows, so every warp load is consecutive
+// doubles of one column (16-byte loads of two rows per lane on the full
+// off-diagonal tiles); the transposed product of a block is reduced across
+// lanes by a butterfly (16 columns per warp pass; one CTA per SM keeps the
+// loop in registers).  The per-tile partial vectors go to
 // a workspace and a second kernel sums them in a fixed order, so results are
 // bit-reproducible.
 //
@@ -59,7 +60,8 @@ __global__ void __launch_bounds__(SV_THREADS, 1)
 k_symv_tiles(plasma_desc_t A, int uplo, const double *x, double *part,
              const plasma_devstat_t *st)
 {
-    __shared__ double xp_s[512], xq_s[512];
+    __shared__ __align__(16) double xp_s[512];
+    __shared__ double xq_s[512];
     __shared__ double ypart[8][512];
     if (plasma_failed(st)) return;
     const int mt = A.mt, nb = A.mb;
@@ -81,9 +83,44 @@ k_symv_tiles(plasma_desc_t A, int uplo, const double *x, double *part,
     __syncthreads();
 
     double *yq_out = part + ((size_t)q * mt + p) * nb;     // S^T x_p -> block q
-    // warps take 16-column groups (16 accumulators and 16 loads in flight
-    // per lane keep the loop in registers); lanes walk rows
-    const int nbr = (rows + 31) / 32, nbc = (cols + 15) / 16;
+    // Full off-diagonal tiles (all but mt of the mt(mt+1)/2): 16-byte loads,
+    // lane l owns rows 2l and 2l+1 of each 64-row block, no predicates.
+    const bool fast = !diag && rows == nb && cols == nb && nb % 64 == 0 && nb <= 512 &&
+                      (ld & 1) == 0 && ((uintptr_t)S & 15) == 0;
+    if (fast) {
+        for (int cb = warp; cb < nb / 16; cb += 8) {
+            double v[16];
+#pragma unroll
+            for (int c = 0; c < 16; c++) v[c] = 0.0;
+            for (int rb = 0; rb < nb / 64; rb++) {
+                const int row = rb * 64 + 2 * lane;
+                const double2 xr = *reinterpret_cast<const double2 *>(xp_s + row);
+                double y0 = 0.0, y1 = 0.0;
+#pragma unroll
+                for (int c = 0; c < 16; c++) {
+                    const int col = cb * 16 + c;
+                    double2 a = __ldg(reinterpret_cast<const double2 *>(S + (size_t)col * ld + row));
+                    if (ABS) {
+                        a.x = fabs(a.x);
+                        a.y = fabs(a.y);
+                    }
+                    const double xc = xq_s[col];
+                    y0 += a.x * xc;
+                    y1 += a.y * xc;
+                    v[c] += a.x * xr.x + a.y * xr.y;
+                }
+                ypart[warp][row] += y0;
+                ypart[warp][row + 1] += y1;
+            }
+            double colsum = butterfly16(v, lane);
+            const int col = cb * 16 + (lane & 15);
+            if (lane < 16) yq_out[col] = colsum;
+        }
+    }
+    // the general path: lanes walk rows one at a time; warps take 16-column
+    // groups (16 accumulators and 16 loads in flight per lane keep the loop
+    // in registers)
+    const int nbr = (rows + 31) / 32, nbc = fast ? 0 : (cols + 15) / 16;
     for (int cb = warp; cb < nbc; cb += 8) {
         double v[16];
 #pragma unroll
