@@ -303,8 +303,7 @@ static void upload_and_factor(plasma_context_t *plasma, const upload_t *up,
                               (size_t)(n - c0) * sizeof(double), (size_t)w,
                               cudaMemcpyHostToDevice, cp);
         }
-        plasma_cuda_upload_cols(cp, st, plasma->dquiet, call, A, As, stage, n, gstart[g],
-                                gstart[g + 1]);
+        plasma_cuda_upload_cols(cp, st, call, A, As, stage, n, gstart[g], gstart[g + 1]);
         cudaEventRecord(plasma->ev_group[g], cp);
     }
     plasma_cuda_lansy_inf(cp, plasma->dquiet, PlasmaLower, A, d_anorm, symv_work);

@@ -89,6 +89,41 @@ k_tile_copy(plasma_desc_t A, plasma_desc_t B, int uplo, int n0,
         plasma_fail(st, 1, call);
 }
 
+// Lower tile (m,n) of an upload in flight, in one pass over the staged
+// column-major copy: the FP64 tile of A and its FP32 conversion into As
+// (dlag2s overflow test into st).  The kernel never returns early on the
+// device status: the FP64 tiles are needed whatever the FP32 factorization
+// reports (later attempts and the FP64 fallback read them).  Warps take
+// columns, lanes consecutive rows.
+__global__ void __launch_bounds__(kThreads)
+k_upload_tile(plasma_desc_t A, plasma_desc_t As, const double *src, int ld, int n0,
+              plasma_devstat_t *st, int call)
+{
+    const int m = blockIdx.x, n = blockIdx.y + n0;
+    if (n > m) return;
+    const TileBox b = tile_box(A, m, n);
+    double *t = (double *)plasma_tile_addr(A, m, n);
+    float *ts = (float *)plasma_tile_addr(As, m, n);
+    const int ldt = plasma_tile_mmain(A, m), lds = plasma_tile_mmain(As, m);
+    const double *f = src + (size_t)A.nb * ld * n + (size_t)A.mb * m;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    bool overflow = false;
+    for (int x = b.x1 + warp; x < b.x2; x += kThreads / 32) {
+        const double *fc = f + (size_t)x * ld;
+        double *tc = t + (size_t)x * ldt;
+        float *sc = ts + (size_t)x * lds;
+#pragma unroll 4
+        for (int y = b.y1 + lane; y < b.y2; y += 32) {
+            const double v = fc[y];
+            tc[y] = v;
+            if (v > (double)FLT_MAX || v < -(double)FLT_MAX) overflow = true;
+            sc[y] = (float)v;
+        }
+    }
+    if (__syncthreads_or(overflow) && threadIdx.x == 0)
+        plasma_fail(st, 1, call);
+}
+
 // B(m,n) <- A(n,m)^T for the lower tiles of B (m >= n) from the upper tiles
 // of A (same symmetric matrix in the other triangle), FP64 -> FP32 with the
 // overflow test; 32 x 32 blocks transposed through shared memory so that
@@ -237,22 +272,14 @@ extern "C" void plasma_cuda_lag2s(cudaStream_t s, plasma_devstat_t *st, int call
 // (src, ld: the whole matrix) and their FP32 conversion into As, lower
 // tiles -- the per-group conversion of an upload that runs alongside the
 // factorization of the groups before it.
-extern "C" void plasma_cuda_upload_cols(cudaStream_t s, plasma_devstat_t *st,
-                                        const plasma_devstat_t *quiet, int call,
+extern "C" void plasma_cuda_upload_cols(cudaStream_t s, plasma_devstat_t *st, int call,
                                         plasma_desc_t A, plasma_desc_t As, const double *src,
                                         int ld, int n0, int n1)
 {
     if (n1 <= n0 || A.mt == 0) return;
     PLASMA_COUNT_LAUNCH();
     dim3 grid((unsigned)A.mt, (unsigned)(n1 - n0));
-    // the FP64 tiles are needed whatever the FP32 factorization reports
-    // (the later attempts and the FP64 fallback read them): they follow a
-    // status word that no kernel sets
-    k_lapack_tile<double, true><<<grid, kThreads, 0, s>>>(A, PlasmaLower, (double *)src, ld,
-                                                           n0, quiet);
-    PLASMA_COUNT_LAUNCH();
-    k_tile_copy<double, float, true><<<grid, kThreads, 0, s>>>(A, As, PlasmaLower, n0, st,
-                                                               call);
+    k_upload_tile<<<grid, kThreads, 0, s>>>(A, As, src, ld, n0, st, call);
 }
 
 extern "C" void plasma_cuda_slag2d(cudaStream_t s, plasma_devstat_t *st,

@@ -179,9 +179,9 @@ void plasma_cuda_lansy_inf(cudaStream_t s, plasma_devstat_t *st,
                            double *dnorm, double *work);
 /* Tile columns [n0, n1) of a host upload in flight: FP64 tiles of A (lower)
  * from the column-major device copy src (leading dimension ld) and their
- * FP32 conversion into As (dlag2s overflow test). */
-void plasma_cuda_upload_cols(cudaStream_t s, plasma_devstat_t *st,
-                             const plasma_devstat_t *quiet, int call,
+ * FP32 conversion into As (dlag2s overflow test), in one pass that runs
+ * whatever the device status says. */
+void plasma_cuda_upload_cols(cudaStream_t s, plasma_devstat_t *st, int call,
                              plasma_desc_t A, plasma_desc_t As, const double *src,
                              int ld, int n0, int n1);
 /* As (lower tiles) <- (float)A with A in upper storage (transposed tiles). */
