@@ -242,13 +242,13 @@ typedef struct {
 } upload_t;
 
 /* Tile-column groups that each hold about the same share of the lower
- * triangle (PLASMA_GROUP_STREAMS of them, so the first ones are narrow and
- * the last ones wide): the right-looking update of a column needs every
+ * triangle (up to PLASMA_MAX_GROUPS of them, so the first ones are narrow
+ * and the last ones wide): the right-looking update of a column needs every
  * panel before it, so most of the update work sits in the last columns,
- * and equal shares let it start as early as the bus allows. */
+ * and fine groups let it start as early as the bus allows. */
 static int column_groups(int nt, int *gstart)
 {
-    const int ng_max = nt < PLASMA_GROUP_STREAMS ? nt : PLASMA_GROUP_STREAMS;
+    const int ng_max = nt < PLASMA_MAX_GROUPS ? nt : PLASMA_MAX_GROUPS;
     const double total = 0.5 * (double)nt * (nt + 1);
     int ng = 0;
     double acc = 0.0;
@@ -287,7 +287,7 @@ static void upload_and_factor(plasma_context_t *plasma, const upload_t *up,
         plasma_request_fail(sequence, request, PlasmaErrorOutOfMemory);
         return;
     }
-    int gstart[PLASMA_GROUP_STREAMS + 1];
+    int gstart[PLASMA_MAX_GROUPS + 1];
     const int ng = column_groups(A.nt, gstart);
     /* the copies start after everything enqueued so far (the zeroed tile
      * storage, the right-hand side) */

@@ -112,7 +112,13 @@ void plasma_pXpotrf_mode(plasma_context_t *plasma, plasma_enum_t uplo,
  * it missed from the kept panel copies while the critical stream goes on
  * with the columns that are in.  The stream holding column k+2 splits it
  * off and records N(k), which the critical stream waits for at step k+1,
- * as in the one-bulk-stream DAG. */
+ * as in the one-bulk-stream DAG.
+ *
+ * Groups outnumber the streams: group g runs on stream g mod S.  It starts
+ * (waits for its arrival, then applies panels 0 .. k-1 in one stretch) at
+ * the step k where group g-S has taken its last update, step
+ * gstart[g-S+1] - 3; that is always before group g's first column needs
+ * its first update (step gstart[g] - 2), since every group holds a column. */
 static void walk_groups(plasma_context_t *plasma, walk_t *w, int call, int ngroups,
                         const int *gstart, const cudaEvent_t *arrive)
 {
@@ -120,6 +126,7 @@ static void walk_groups(plasma_context_t *plasma, walk_t *w, int call, int ngrou
     plasma_enum_t uplo = w->uplo;
     plasma_desc_t A = w->A;
     const int mt = A.mt;
+    const int nstreams = ngroups < PLASMA_GROUP_STREAMS ? ngroups : PLASMA_GROUP_STREAMS;
     cudaStream_t S = plasma->stream;
     cudaStream_t crit = plasma->aux[0];
     cudaEvent_t ev_start = plasma->ev[0];
@@ -129,13 +136,14 @@ static void walk_groups(plasma_context_t *plasma, walk_t *w, int call, int ngrou
 
     cudaEventRecord(ev_start, S);
     cudaStreamWaitEvent(crit, ev_start, 0);
-    for (int g = 0; g < ngroups; g++) {
-        cudaStream_t gs = plasma->aux[3 + g];
+    for (int s = 0; s < nstreams; s++) {
+        cudaStream_t gs = plasma->aux[3 + s];
         cudaStreamWaitEvent(gs, ev_start, 0);
-        cudaStreamWaitEvent(gs, arrive[g], 0);
+        cudaStreamWaitEvent(gs, arrive[s], 0);   /* groups 0 .. nstreams-1 */
     }
     cudaStreamWaitEvent(crit, arrive[0], 0);
 
+    int active = nstreams;           /* groups [0, active) have started */
     int have_next = 0;
     int gk = 0;                      /* group of column k + 1 */
     for (int k = 0; k < mt; k++) {
@@ -151,13 +159,24 @@ static void walk_groups(plasma_context_t *plasma, walk_t *w, int call, int ngrou
         cudaEventRecord(ev_panel, crit);
         update(w, crit, k, k + 1, k + 2);
 
+        /* groups whose stream came free: arrival, then the missed steps
+         * (panels 0 .. k-1 are done once panel k is) */
+        while (active < ngroups && gstart[active - nstreams + 1] - 3 < k) {
+            const int g = active++;
+            cudaStream_t gs = plasma->aux[3 + g % nstreams];
+            cudaStreamWaitEvent(gs, arrive[g], 0);
+            cudaStreamWaitEvent(gs, ev_panel, 0);
+            for (int kk = 0; kk < k; kk++)
+                update(w, gs, kk, gstart[g], gstart[g + 1]);
+        }
+
         have_next = 0;
-        for (int g = gk; g < ngroups; g++) {
+        for (int g = gk; g < active; g++) {
             const int hi = gstart[g + 1];
             const int lo = gstart[g] > k + 2 ? gstart[g] : k + 2;
             if (lo >= hi)
                 continue;
-            cudaStream_t gs = plasma->aux[3 + g];
+            cudaStream_t gs = plasma->aux[3 + g % nstreams];
             cudaStreamWaitEvent(gs, ev_panel, 0);
             if (lo == k + 2) {
                 update(w, gs, k, k + 2, k + 3);
@@ -172,8 +191,8 @@ static void walk_groups(plasma_context_t *plasma, walk_t *w, int call, int ngrou
     }
     cudaEventRecord(ev_end, crit);
     cudaStreamWaitEvent(S, ev_end, 0);
-    for (int g = 0; g < ngroups; g++) {
-        cudaEventRecord(ev_end, plasma->aux[3 + g]);
+    for (int s = 0; s < nstreams; s++) {
+        cudaEventRecord(ev_end, plasma->aux[3 + s]);
         cudaStreamWaitEvent(S, ev_end, 0);
     }
 }
@@ -190,8 +209,8 @@ void plasma_pXpotrf_arrivals(plasma_context_t *plasma, plasma_enum_t uplo,
         return;
     plasma_devstat_t *st = plasma->dstat;
     cudaStream_t S = plasma->stream;
-    if (ngroups > PLASMA_GROUP_STREAMS) {
-        /* more groups than streams: wait for all of them */
+    if (ngroups > PLASMA_MAX_GROUPS) {
+        /* more groups than arrival slots: wait for all of them */
         for (int g = 0; g < ngroups; g++)
             cudaStreamWaitEvent(S, arrive[g], 0);
         ngroups = 0;

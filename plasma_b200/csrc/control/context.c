@@ -103,7 +103,7 @@ int plasma_init(void)
                                      i == 0 || i == PLASMA_STREAM_COPY ? prio_hi : prio_lo);
     for (int i = 0; i < 8; i++)
         cudaEventCreateWithFlags(&c->ev[i], cudaEventDisableTiming);
-    for (int i = 0; i < PLASMA_GROUP_STREAMS; i++)
+    for (int i = 0; i < PLASMA_MAX_GROUPS; i++)
         cudaEventCreateWithFlags(&c->ev_group[i], cudaEventDisableTiming);
     if (cudaMalloc((void **)&c->dstat, sizeof(plasma_devstat_t)) != cudaSuccess ||
         cudaMalloc((void **)&c->dquiet, sizeof(plasma_devstat_t)) != cudaSuccess ||
@@ -134,7 +134,7 @@ int plasma_finalize(void)
         if (c->scratch[i]) cudaFree(c->scratch[i]);
     for (int i = 0; i < 8; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
-    for (int i = 0; i < PLASMA_GROUP_STREAMS; i++)
+    for (int i = 0; i < PLASMA_MAX_GROUPS; i++)
         if (c->ev_group[i]) cudaEventDestroy(c->ev_group[i]);
     if (c->sweep_sync) cudaFree(c->sweep_sync);
     if (c->pinned) cudaFreeHost(c->pinned);

@@ -39,6 +39,7 @@ typedef struct {
 #define PLASMA_NUM_STREAMS 16
 #define PLASMA_STREAM_COPY 2
 #define PLASMA_GROUP_STREAMS (PLASMA_NUM_STREAMS - 3)
+#define PLASMA_MAX_GROUPS 32     /* column groups of an arriving matrix */
 #define PLASMA_SCRATCH_SLOTS 9
 
 /* scratch slots */
@@ -88,7 +89,7 @@ typedef struct {
     void  *pinned;
     size_t pinned_bytes;
     cudaEvent_t ev[8];                        /* DAG edges (reused)        */
-    cudaEvent_t ev_group[PLASMA_GROUP_STREAMS]; /* arrival of column groups */
+    cudaEvent_t ev_group[PLASMA_MAX_GROUPS]; /* arrival of column groups   */
     /* ready flags of the one-launch triangular sweeps */
     void  *sweep_sync;
     size_t sweep_sync_bytes;
@@ -317,7 +318,7 @@ void plasma_pXpotrf_mode(plasma_context_t *plasma, plasma_enum_t uplo,
 /* The same factorization of a matrix whose tile columns are still arriving:
  * group g = tile columns [gstart[g], gstart[g+1]) is in place once event
  * arrive[g] has completed (gstart[0] = 0, gstart[ngroups] = A.nt,
- * 1 <= ngroups <= PLASMA_GROUP_STREAMS). */
+ * 1 <= ngroups <= PLASMA_MAX_GROUPS). */
 /* Grows the panel-copy scratch of plasma_pXpotrf_arrivals beforehand (a
  * slot that grows waits for every stream). */
 void plasma_pXpotrf_reserve(plasma_context_t *plasma, plasma_enum_t uplo, plasma_desc_t A,

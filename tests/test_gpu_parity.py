@@ -543,11 +543,12 @@ def _pinned_colmajor(a):
     return t
 
 
-@pytest.mark.parametrize("n,nb,kappa", [(3000, 256, 1e3), (2048, 128, 1e5)])
+@pytest.mark.parametrize("n,nb,kappa", [(3000, 256, 1e3), (2048, 128, 1e5), (2500, 64, 1e3)])
 def test_dsposv_overlapped_upload(L, n, nb, kappa):
     """A lower-stored host matrix in page-locked memory goes up in groups of
     tile columns while the factorization of the groups already in place runs
-    (ragged n included): the answer matches the oracle."""
+    (ragged n included; 16 and 32 groups on 13 streams, so streams take on
+    later groups): the answer matches the oracle."""
     set_nb(L, nb)
     a = gen.spectrum(n, kappa, seed=2100 + n)
     xt = np.random.default_rng(n).standard_normal((n, 1))
