@@ -30,6 +30,18 @@ int plasma_spotrs(plasma_enum_t uplo, int n, int nrhs,
 int plasma_sposv(plasma_enum_t uplo, int n, int nrhs,
                  float *pA, int lda, float *pB, int ldb);
 
+/* reference compute/zpotri.c:65-185: inverse from the Cholesky factor */
+int plasma_spotri(plasma_enum_t uplo, int n, float *pA, int lda);
+/* reference compute/zpoinv.c:67-185: inverse of an SPD matrix */
+int plasma_spoinv(plasma_enum_t uplo, int n, float *pA, int lda);
+
+/* reference compute/zpotri.c:187-236 */
+void plasma_omp_spotri(plasma_enum_t uplo, plasma_desc_t A,
+                       plasma_sequence_t *sequence, plasma_request_t *request);
+/* reference compute/zpoinv.c:187-236 */
+void plasma_omp_spoinv(plasma_enum_t uplo, plasma_desc_t A,
+                       plasma_sequence_t *sequence, plasma_request_t *request);
+
 /* reference compute/zpotrf.c:206-246 */
 void plasma_omp_spotrf(plasma_enum_t uplo, plasma_desc_t A,
                        plasma_sequence_t *sequence, plasma_request_t *request);

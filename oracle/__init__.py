@@ -28,7 +28,8 @@ def lib():
             getattr(L, f"{p}oracle_potrf").argtypes = [ci, ci, vp, ci, ci]
             getattr(L, f"{p}oracle_potrs").argtypes = [ci, ci, ci, vp, ci, vp, ci, ci]
             getattr(L, f"{p}oracle_posv").argtypes = [ci, ci, ci, vp, ci, vp, ci, ci]
-            for f in ("potrf", "potrs", "posv"):
+            getattr(L, f"{p}oracle_potri").argtypes = [ci, ci, vp, ci]
+            for f in ("potrf", "potrs", "posv", "potri"):
                 getattr(L, f"{p}oracle_{f}").restype = ci
         L.oracle_dsposv.argtypes = [ci, ci, ci, vp, ci, vp, ci, vp, ci,
                                     ctypes.POINTER(ci), ci]
@@ -54,6 +55,13 @@ def potrf(uplo, a, nb):
     """In-place tile Cholesky of the Fortran-ordered array a; returns info."""
     n = a.shape[0]
     return getattr(lib(), f"{_prefix(a)}oracle_potrf")(uplo, n, _p(a), a.shape[0], nb)
+
+
+def potri(uplo, a):
+    """In-place inverse from the Cholesky factor in the uplo triangle of the
+    Fortran-ordered array a (dtrtri + dlauum); returns info."""
+    n = a.shape[0]
+    return getattr(lib(), f"{_prefix(a)}oracle_potri")(uplo, n, _p(a), a.shape[0])
 
 
 def potrs(uplo, a, b, nb):

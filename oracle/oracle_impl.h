@@ -422,3 +422,77 @@ int P(oracle_posv)(int uplo, int n, int nrhs, REAL *A, int lda, REAL *B,
     P(tiles_free)(&TB, nrhs);
     return info;
 }
+
+/* Inverse of an SPD matrix from its Cholesky factor held in the uplo
+ * triangle of A (compute/zpotri.c:228-235: plasma_pztrtri(uplo, NonUnit)
+ * then plasma_pzlauum(uplo)), restated unblocked from the published LAPACK
+ * algorithms the reference's tile kernels implement: dtrti2 (inverse of a
+ * triangular matrix, column by column against the part already inverted)
+ * and dlauu2 (L^T L, or U U^T, row by row).  Returns info = i + 1 when
+ * A(i,i) is exactly zero (dtrtri), leaving A unchanged; the other triangle
+ * is not touched. */
+int P(oracle_potri)(int uplo, int n, REAL *A, int lda)
+{
+#define AE(i, j) A[(i) + (size_t)(j) * lda]
+    for (int i = 0; i < n; i++)
+        if (AE(i, i) == (REAL)0)
+            return i + 1;
+    REAL *x = (REAL *)malloc(sizeof(REAL) * (size_t)(n > 0 ? n : 1));
+    if (uplo == ORACLE_LOWER) {
+        /* dtrti2, lower: columns from the last one back */
+        for (int j = n - 1; j >= 0; j--) {
+            AE(j, j) = (REAL)1 / AE(j, j);
+            const REAL ajj = -AE(j, j);
+            /* A(j+1:n, j) = ajj * T(j+1:n, j+1:n) A(j+1:n, j), T lower */
+            for (int i = j + 1; i < n; i++) x[i] = AE(i, j);
+            for (int i = j + 1; i < n; i++) {
+                REAL t = 0;
+                for (int k = j + 1; k <= i; k++) t += AE(i, k) * x[k];
+                AE(i, j) = ajj * t;
+            }
+        }
+        /* dlauu2, lower: A <- L^T L */
+        for (int i = 0; i < n; i++) {
+            const REAL aii = AE(i, i);
+            REAL d = 0;
+            for (int k = i; k < n; k++) d += AE(k, i) * AE(k, i);
+            /* A(i, 0:i) = aii A(i, 0:i) + A(i+1:n, 0:i)^T A(i+1:n, i) */
+            for (int j = 0; j < i; j++) {
+                REAL t = aii * AE(i, j);
+                for (int k = i + 1; k < n; k++) t += AE(k, j) * AE(k, i);
+                AE(i, j) = t;
+            }
+            AE(i, i) = d;
+        }
+    } else {
+        /* dtrti2, upper: columns from the first one on */
+        for (int j = 0; j < n; j++) {
+            AE(j, j) = (REAL)1 / AE(j, j);
+            const REAL ajj = -AE(j, j);
+            /* A(0:j, j) = ajj * T(0:j, 0:j) A(0:j, j), T upper */
+            for (int i = 0; i < j; i++) x[i] = AE(i, j);
+            for (int i = 0; i < j; i++) {
+                REAL t = 0;
+                for (int k = i; k < j; k++) t += AE(i, k) * x[k];
+                AE(i, j) = ajj * t;
+            }
+        }
+        /* dlauu2, upper: A <- U U^T */
+        for (int i = 0; i < n; i++) {
+            const REAL aii = AE(i, i);
+            REAL d = 0;
+            for (int k = i; k < n; k++) d += AE(i, k) * AE(i, k);
+            /* A(0:i, i) = aii A(0:i, i) + A(0:i, i+1:n) A(i, i+1:n)^T */
+            for (int j = 0; j < i; j++) {
+                REAL t = aii * AE(j, i);
+                for (int k = i + 1; k < n; k++) t += AE(j, k) * AE(i, k);
+                AE(j, i) = t;
+            }
+            AE(i, i) = d;
+        }
+    }
+    free(x);
+    return 0;
+#undef AE
+}
+

@@ -156,6 +156,14 @@ _SIGNATURES = [
     ("plasma_omp_dpotrs_adjoint", None, [c_int, _DESC, _DESC, _DESC, _DESC, _SEQ, _REQ]),
     ("plasma_omp_spotrs_adjoint", None, [c_int, _DESC, _DESC, _DESC, _DESC, _SEQ, _REQ]),
     ("plasma_omp_spotrs", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
+    ("plasma_dpotri", c_int, [c_int, c_int, c_void_p, c_int]),
+    ("plasma_spotri", c_int, [c_int, c_int, c_void_p, c_int]),
+    ("plasma_dpoinv", c_int, [c_int, c_int, c_void_p, c_int]),
+    ("plasma_spoinv", c_int, [c_int, c_int, c_void_p, c_int]),
+    ("plasma_omp_dpotri", None, [c_int, _DESC, _SEQ, _REQ]),
+    ("plasma_omp_spotri", None, [c_int, _DESC, _SEQ, _REQ]),
+    ("plasma_omp_dpoinv", None, [c_int, _DESC, _SEQ, _REQ]),
+    ("plasma_omp_spoinv", None, [c_int, _DESC, _SEQ, _REQ]),
     ("plasma_omp_dposv", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
     ("plasma_omp_sposv", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
     ("plasma_omp_dsposv", None, [c_int, _DESC, _DESC, _DESC, _DESC, _DESC, _DESC,

@@ -10,6 +10,7 @@
 #include "common.cuh"
 
 #include <float.h>
+#include <limits.h>
 
 namespace {
 
@@ -122,6 +123,45 @@ k_upload_tile(plasma_desc_t A, plasma_desc_t As, const double *src, int ld, int 
     }
     if (__syncthreads_or(overflow) && threadIdx.x == 0)
         plasma_fail(st, 1, call);
+}
+
+// info of dtrtri on the factor held in A: the smallest i with A(i,i) == 0
+// (one CTA; the diagonal has n elements)
+template <typename T>
+__global__ void __launch_bounds__(1024)
+k_diag_zero_info(plasma_desc_t A, plasma_devstat_t *st, int call)
+{
+    __shared__ int first;
+    if (threadIdx.x == 0) first = INT_MAX;
+    __syncthreads();
+    for (int i = threadIdx.x; i < A.m; i += blockDim.x) {
+        const int m = i / A.mb, r = i - m * A.mb;
+        const T *t = (const T *)plasma_tile_addr(A, m, m);
+        if (t[(size_t)r * plasma_tile_mmain(A, m) + r] == T(0)) atomicMin(&first, i);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && first != INT_MAX) plasma_fail(st, first + 1, call);
+}
+
+// A <- the uplo triangle of B, tile by tile (diagonal tiles: only the uplo
+// part, the rest of A stays as it is); A and B have the same tiling
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_copy_uplo(plasma_desc_t B, plasma_desc_t A, int uplo, const plasma_devstat_t *st)
+{
+    if (plasma_failed(st)) return;
+    const int m = blockIdx.x, n = blockIdx.y;
+    if (!tile_in(uplo, m, n)) return;
+    const T *b = (const T *)plasma_tile_addr(B, m, n);
+    T *a = (T *)plasma_tile_addr(A, m, n);
+    const int ldb = plasma_tile_mmain(B, m), lda = plasma_tile_mmain(A, m);
+    const int rows = plasma_tile_mview(A, m), cols = plasma_tile_nview(A, n);
+    const bool diag = m == n, lower = uplo == PlasmaLower;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int x = warp; x < cols; x += kThreads / 32)
+        for (int y = lane; y < rows; y += 32)
+            if (!diag || (lower ? y >= x : y <= x))
+                a[(size_t)x * lda + y] = b[(size_t)x * ldb + y];
 }
 
 // B(m,n) <- A(n,m)^T for the lower tiles of B (m >= n) from the upper tiles
@@ -280,6 +320,28 @@ extern "C" void plasma_cuda_upload_cols(cudaStream_t s, plasma_devstat_t *st, in
     PLASMA_COUNT_LAUNCH();
     dim3 grid((unsigned)A.mt, (unsigned)(n1 - n0));
     k_upload_tile<<<grid, kThreads, 0, s>>>(A, As, src, ld, n0, st, call);
+}
+
+extern "C" void plasma_cuda_diag_zero_info(cudaStream_t s, plasma_devstat_t *st, int call,
+                                           plasma_desc_t A)
+{
+    if (A.m == 0) return;
+    PLASMA_COUNT_LAUNCH();
+    if (A.precision == PlasmaRealDouble)
+        k_diag_zero_info<double><<<1, 1024, 0, s>>>(A, st, call);
+    else
+        k_diag_zero_info<float><<<1, 1024, 0, s>>>(A, st, call);
+}
+
+extern "C" void plasma_cuda_copy_uplo(cudaStream_t s, plasma_devstat_t *st, plasma_enum_t uplo,
+                                      plasma_desc_t B, plasma_desc_t A)
+{
+    if (A.mt == 0 || A.nt == 0) return;
+    PLASMA_COUNT_LAUNCH();
+    if (A.precision == PlasmaRealDouble)
+        k_copy_uplo<double><<<tile_grid(A), kThreads, 0, s>>>(B, A, uplo, st);
+    else
+        k_copy_uplo<float><<<tile_grid(A), kThreads, 0, s>>>(B, A, uplo, st);
 }
 
 extern "C" void plasma_cuda_slag2d(cudaStream_t s, plasma_devstat_t *st,

@@ -178,6 +178,12 @@ int plasma_cuda_lansy_tiles(cudaStream_t s, plasma_devstat_t *st,
 void plasma_cuda_lansy_inf(cudaStream_t s, plasma_devstat_t *st,
                            plasma_enum_t uplo, plasma_desc_t A,
                            double *dnorm, double *work);
+/* info = i + 1 for the first zero A(i,i) of a triangular factor (dtrtri). */
+void plasma_cuda_diag_zero_info(cudaStream_t s, plasma_devstat_t *st, int call,
+                                plasma_desc_t A);
+/* A <- uplo triangle of B (same tiling; the other triangle of A kept). */
+void plasma_cuda_copy_uplo(cudaStream_t s, plasma_devstat_t *st, plasma_enum_t uplo,
+                           plasma_desc_t B, plasma_desc_t A);
 /* Tile columns [n0, n1) of a host upload in flight: FP64 tiles of A (lower)
  * from the column-major device copy src (leading dimension ld) and their
  * FP32 conversion into As (dlag2s overflow test), in one pass that runs

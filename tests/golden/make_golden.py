@@ -70,6 +70,17 @@ def main():
         _, x, info = lapack.dposv(a, bb, lower=1)
         d[f"spec{int(np.log10(kappa))}_X"] = x
         d[f"spec{int(np.log10(kappa))}_xtrue"] = xt
+    # inverse from the Cholesky factor (dpotri; the reference tester
+    # test/test_zpotri.c:135-155 compares plasma_zpotri with LAPACKE_zpotri)
+    for n in (7, 64, 100):
+        a, _ = gen.diag_dominant(n, 1, seed=4000 + n)
+        for lower, tag in ((1, "L"), (0, "U")):
+            c, info = lapack.dpotrf(a, lower=lower, clean=1)
+            inv, info_i = lapack.dpotri(c, lower=lower)
+            assert info == 0 and info_i == 0
+            tri = np.tril if lower else np.triu
+            d[f"potri{n}_{tag}_factor"] = tri(c)
+            d[f"potri{n}_{tag}_inv"] = tri(inv)
     np.savez_compressed(OUT, **d)
     print("wrote", OUT, os.path.getsize(OUT), "bytes")
 

@@ -264,3 +264,16 @@ def test_dsposv_descriptor_triangles(hostonly):
                             ctypes.byref(seq), ctypes.byref(req))
         assert seq.status == want, (uplo, A.type, As.type)
         assert it.value == 0
+
+
+def test_potri_poinv_argument_codes(hostonly):
+    """plasma_{d,s}{potri,poinv}: -1 uplo, -2 n, -4 lda (compute/zpotri.c:76-90,
+    zpoinv.c:78-92), quick return for n = 0, no device -> Environment."""
+    L = hostonly
+    for f in ("plasma_dpotri", "plasma_spotri", "plasma_dpoinv", "plasma_spoinv"):
+        fn = getattr(L, f)
+        assert fn(0, 4, None, 4) == -1
+        assert fn(pb.PlasmaLower, -1, None, 4) == -2
+        assert fn(pb.PlasmaUpper, 4, None, 3) == -4
+        assert fn(pb.PlasmaLower, 0, None, 1) == 0
+        assert fn(pb.PlasmaLower, 4, None, 4) == pb.PlasmaErrorEnvironment

@@ -584,3 +584,74 @@ def test_dsposv_overlapped_upload_fallback(L):
                            ctypes.byref(it)) == 0
     assert it.value == -31
     assert solve_residual(a, X.numpy().T.copy(), b) < TOL * EPS
+
+
+# ------------------------------------------------------------------ potri / poinv
+def _factor_with_noise(a, uplo, seed):
+    """The Cholesky factor in the uplo triangle, noise in the other one
+    (which potri must leave as it is)."""
+    n = a.shape[0]
+    lf = np.linalg.cholesky(a)
+    f = np.asfortranarray(lf if uplo == LO else lf.T)
+    mask = (np.triu(np.ones((n, n), bool), 1) if uplo == LO
+            else np.tril(np.ones((n, n), bool), -1))
+    f[mask] = np.random.default_rng(seed).standard_normal(int(mask.sum()))
+    return f, mask
+
+
+@pytest.mark.parametrize("uplo", [LO, UP])
+@pytest.mark.parametrize("n,nb", [(64, 64), (300, 128), (777, 256), (1024, 256)])
+def test_potri_against_oracle(L, uplo, n, nb):
+    """plasma_dpotri against the oracle's dtrtri + dlauum with the reference
+    tester's check (test/test_zpotri.c:135-155): ||inv - inv_ref||_F /
+    ||inv_ref||_F < 50 eps on the uplo triangle; the other triangle of pA
+    is not touched."""
+    set_nb(L, nb)
+    a, _ = gen.diag_dominant(n, 1, seed=4100 + n)
+    f, mask = _factor_with_noise(a, uplo, n)
+    ref = np.asfortranarray(f.copy())
+    assert oracle.potri(uplo, ref) == 0
+    got = np.asfortranarray(f.copy())
+    assert L.plasma_dpotri(uplo, n, got.ctypes.data, n) == 0
+    tri = np.tril if uplo == LO else np.triu
+    assert np.linalg.norm(tri(got) - tri(ref)) / np.linalg.norm(tri(ref)) < TOL * EPS
+    np.testing.assert_array_equal(got[mask], f[mask])
+    # FP32
+    f32 = np.asfortranarray(f.astype(np.float32))
+    assert L.plasma_spotri(uplo, n, f32.ctypes.data, n) == 0
+    assert (np.linalg.norm(tri(f32).astype(np.float64) - tri(ref)) / np.linalg.norm(tri(ref))
+            < TOL * SEPS)
+
+
+@pytest.mark.parametrize("uplo", [LO, UP])
+@pytest.mark.parametrize("n,nb", [(300, 128), (1000, 256)])
+def test_poinv_against_oracle(L, uplo, n, nb):
+    """plasma_dpoinv = potrf + potri on the matrix itself, against the
+    oracle's tile potrf + potri; A inv(A) = I to the tester's tolerance."""
+    set_nb(L, nb)
+    a, _ = gen.diag_dominant(n, 1, seed=4200 + n)
+    ref = np.asfortranarray(a.copy())
+    assert oracle.potrf(uplo, ref, nb) == 0
+    assert oracle.potri(uplo, ref) == 0
+    got = np.asfortranarray(a.copy())
+    assert L.plasma_dpoinv(uplo, n, got.ctypes.data, n) == 0
+    tri = np.tril if uplo == LO else np.triu
+    assert np.linalg.norm(tri(got) - tri(ref)) / np.linalg.norm(tri(ref)) < TOL * EPS
+    full = tri(got) + tri(got, -1 if uplo == LO else 1).T
+    assert np.abs(a @ full - np.eye(n)).max() < TOL * EPS * n
+
+
+def test_potri_poinv_info(L):
+    """A zero on the factor's diagonal: potri returns its order (dtrtri)
+    and leaves pA as it was; poinv of a non-SPD matrix returns potrf's."""
+    set_nb(L, 64)
+    n = 200
+    a, _ = gen.diag_dominant(n, 1, seed=4300)
+    f, _ = _factor_with_noise(a, LO, 1)
+    f[73, 73] = 0.0
+    f[150, 150] = 0.0
+    keep = f.copy()
+    assert L.plasma_dpotri(LO, n, f.ctypes.data, n) == 74
+    np.testing.assert_array_equal(f, keep)
+    z = np.asfortranarray(gen.zerocol(a, 120))
+    assert L.plasma_dpoinv(LO, n, z.ctypes.data, n) == 121

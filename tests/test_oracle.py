@@ -135,3 +135,32 @@ def test_single_precision_potrf():
     assert oracle.potrf(LO, f, 32) == 0
     l = np.tril(f).astype(np.float64)
     assert np.linalg.norm(a - l @ l.T) / (100 * np.linalg.norm(a)) < 50 * np.finfo(np.float32).eps
+
+
+@pytest.mark.parametrize("n", [7, 64, 100])
+@pytest.mark.parametrize("tag", ["L", "U"])
+def test_potri_against_lapack(golden, n, tag):
+    """The oracle's dtrtri + dlauum against LAPACK dpotri: the reference
+    tester's check (test/test_zpotri.c:135-155), ||inv - inv_lapack||_F /
+    ||inv_lapack||_F < 50 eps on the uplo triangle; the other triangle is
+    left as it was."""
+    f = np.asfortranarray(golden[f"potri{n}_{tag}_factor"].copy())
+    ref = golden[f"potri{n}_{tag}_inv"]
+    uplo = oracle.LOWER if tag == "L" else oracle.UPPER
+    tri = np.tril if tag == "L" else np.triu
+    other = (lambda m: np.triu(m, 1)) if tag == "L" else (lambda m: np.tril(m, -1))
+    before = other(f).copy()
+    assert oracle.potri(uplo, f) == 0
+    assert np.linalg.norm(tri(f) - ref) / np.linalg.norm(ref) < 50 * EPS
+    np.testing.assert_array_equal(other(f), before)
+
+
+def test_potri_zero_diagonal_info():
+    """dtrtri's info: the first zero on the diagonal of the factor."""
+    a, _ = gen.diag_dominant(50, 1, seed=9)
+    f = np.asfortranarray(np.linalg.cholesky(a))
+    f[17, 17] = 0.0
+    f[30, 30] = 0.0
+    keep = f.copy()
+    assert oracle.potri(oracle.LOWER, f) == 18
+    np.testing.assert_array_equal(f, keep)
