@@ -52,7 +52,7 @@ def parse():
     p.add_argument("--no-dposv", action="store_true")
     p.add_argument("--batch-count", type=int, default=4096,
                    help="matrices of the batched workload")
-    p.add_argument("--workload", default="dsposv", choices=["dsposv", "adjoint", "batched"],
+    p.add_argument("--workload", default="dsposv", choices=["dsposv", "adjoint", "batched", "inverse"],
                    help="dsposv: the headline; adjoint / batched: the differentiation "
                         "and batched-solve configurations, one JSON line each")
     return p.parse_args()
@@ -297,6 +297,55 @@ def run_adjoint(args):
     return 0
 
 
+def run_inverse(args):
+    """plasma_dpoinv / plasma_spoinv (potrf + potri) on device-resident A,
+    n in {8192, 16384}.  A = G G^T/n + I (G ~ N(0,1), seed 3).  GFLOP/s counts the reference's
+    flops (potrf n^3/3, potri 2n^3/3: trtri + lauum); the library's potri
+    does 2n^3 (the tile sweeps on the identity), reported as
+    executed_tflops.  Error: ||A inv(A) - I||_max."""
+    import torch
+    import plasma_b200 as pb
+    L = pb.lib()
+    assert L.plasma_init() == 0
+    rows = []
+    for n in (8192, 16384):
+        g = torch.Generator(device="cuda").manual_seed(3)
+        G = torch.randn(n, n, generator=g, device="cuda", dtype=torch.float64)
+        A0 = G @ G.T / n + torch.eye(n, device="cuda", dtype=torch.float64)
+        del G
+        for dt, fn in ((torch.float64, "d"), (torch.float32, "s")):
+            A1 = A0.to(dt)
+            times = []
+            for rep in range(args.warmup + args.steps):
+                A = A1.clone()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record()
+                rc = getattr(L, f"plasma_{fn}poinv")(pb.PlasmaLower, n, A.data_ptr(), n)
+                e1.record()
+                torch.cuda.synchronize()
+                assert rc == 0, rc
+                if rep >= args.warmup:
+                    times.append(e0.elapsed_time(e1))
+            # A holds the column-major result, i.e. its transpose: the lower
+            # triangle of the inverse is the tensor's upper triangle
+            inv = torch.triu(A.double()) + torch.triu(A.double(), 1).T
+            err = (A0 @ inv - torch.eye(n, device="cuda", dtype=torch.float64)).abs().max().item()
+            ms = min(times)
+            rows.append({"routine": f"{fn}poinv", "n": n, "ms": ms,
+                         "gflops": n ** 3 / ms / 1e6,
+                         "executed_tflops": (n ** 3 / 3 + 2 * n ** 3) / ms / 1e9,
+                         "max_error_A_invA_minus_I": err})
+            del A, A1, inv
+    print(json.dumps({"workload": "inverse", "metric": "time of the SPD inverse "
+                      "(poinv = potrf + potri), device-resident A, uplo = L",
+                      "unit": "ms", "steps": args.steps, "warmup": args.warmup,
+                      "results": rows}), flush=True)
+    L.plasma_finalize()
+    return 0
+
+
 def run_batched(args):
     """4096 SPD systems, n uniform in [16, 512] (seed 5), A = G G^T / n + 0.1 I,
     b ~ N(0,1), FP64 and FP32: one batched posv (factor + solve) launch per
@@ -382,6 +431,8 @@ def main():
     args = parse()
     if args.workload == "adjoint":
         return run_adjoint(args)
+    if args.workload == "inverse":
+        return run_inverse(args)
     if args.workload == "batched":
         return run_batched(args)
     if args.impl == "reference":
