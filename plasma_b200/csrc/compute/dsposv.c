@@ -235,10 +235,13 @@ static int refine_column(refine_t *R, int scheme, double cte, double *xn_out,
     return -1;
 }
 
-/* A lower-stored host matrix whose upload overlaps the factorization. */
+/* The caller's lower-stored matrix, converted inside the solve: from the
+ * host, with the upload overlapping the factorization; from the device, in
+ * one pass to the FP64 tiles of A and the FP32 tiles of As. */
 typedef struct {
     const double *pA;
     int lda;
+    int on_device;
 } upload_t;
 
 /* Tile-column groups that each hold about the same share of the lower
@@ -368,7 +371,9 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
     double Anorm = 0.0;
     double *sw = (double *)plasma_scratch(plasma, PLASMA_SLOT_SYMV,
                                           plasma_cuda_symv_work(A));
-    if (up == NULL) {
+    if (up != NULL && up->on_device)
+        plasma_cuda_upload_cols(S, st, call, A, As, up->pA, up->lda, 0, A.nt);
+    if (up == NULL || up->on_device) {
         plasma_cuda_lansy_inf(S, st, uplo, A, d_anorm, sw);
         cudaMemcpyAsync(&Anorm, d_anorm, sizeof(double), cudaMemcpyDeviceToHost, S);
     }
@@ -447,7 +452,7 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
         if (As.m > A.m)
             plasma_cuda_set_diag(S, As, A.m, As.m, 1.0);
         RF.dscale = NULL;
-        if (a == 0 && up != NULL) {
+        if (a == 0 && up != NULL && !up->on_device) {
             upload_and_factor(plasma, up, A, As, d_anorm, sw, call, mode, sequence, request);
             cudaMemcpyAsync(&Anorm, d_anorm, sizeof(double), cudaMemcpyDeviceToHost, S);
             factor_failed = take_status(plasma) != 0;
@@ -457,10 +462,13 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
                 continue;
             goto factored;
         }
-        if (uplo_s == uplo)
-            plasma_cuda_lag2s(S, st, call, A, As, uplo);
-        else
-            plasma_cuda_lag2s_upper_to_lower(S, st, call, A, As);
+        /* (a device A of the first attempt was converted with As above) */
+        if (a > 0 || up == NULL) {
+            if (uplo_s == uplo)
+                plasma_cuda_lag2s(S, st, call, A, As, uplo);
+            else
+                plasma_cuda_lag2s_upper_to_lower(S, st, call, A, As);
+        }
         if (plan[a].scaled) {
             /* unit diagonal, then + c u I with u the unit roundoff of the
              * products and c = 4 */
@@ -703,15 +711,19 @@ int plasma_dsposv_ex(plasma_enum_t uplo, int n, int nrhs,
         const char *e = getenv("PLASMA_PIPELINE_UPLOAD");
         pipeline_env = e == NULL || atoi(e) != 0;
     }
-    upload_t up = {pA, lda};
+    const int on_device = plasma_is_device_pointer(pA);
+    upload_t up = {pA, lda, on_device};
     const int pipelined = pipeline_env && uplo == PlasmaLower && plasma->lookahead != 0 &&
-                          !plasma_is_device_pointer(pA);
-    if (!pipelined)
+                          !on_device;
+    /* a lower-stored device matrix goes to both tile copies in one pass
+     * inside the solve */
+    const int direct = uplo == PlasmaLower && on_device;
+    if (!pipelined && !direct)
         plasma_omp_Xlapack2desc(pA, lda, A, uplo, &sequence, &request);
     plasma_omp_Xlapack2desc(pB, ldb, B, PlasmaGeneral, &sequence, &request);
     if (sequence.status == PlasmaSuccess) {
         Xdsposv(plasma, uplo, A, B, X, As, Xs, R, Rnorm, Xnorm, iter,
-                &sequence, &request, info, pipelined ? &up : NULL);
+                &sequence, &request, info, pipelined || direct ? &up : NULL);
     }
     plasma_sequence_wait(&sequence);
     plasma_omp_Xdesc2lapack(X, pX, ldx, PlasmaGeneral, &sequence, &request);
