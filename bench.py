@@ -209,6 +209,18 @@ def cpu_baseline(n, nrhs, kappa, threads=None):
             "seconds": dt}
 
 
+def max_over_ranks(ms, world, device):
+    """The job's step time: the slowest replica's (MAX over the ranks of the
+    initialised process group; every rank gets it)."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.item()
+
+
 def run_reference(args):
     rank, world, _ = dist_info()
     if rank != 0:
@@ -498,11 +510,7 @@ def main():
     prof = {k: pb.profile_query(k) for k in pb.KCLASS}
     pb.profile_enable(False)
     clk = clocks.stop()
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = t.item()
+    ms = max_over_ranks(ms, world, "cuda")
 
     # accuracy of the last solve
     Xc = X.T
