@@ -129,7 +129,10 @@ void sweep(cudaStream_t s, plasma_devstat_t *st, int uplo, int trans,
             B, k, W, nbw, trans, st);
         int mlo = trans ? 0 : k + 1;
         int mhi = trans ? k : mt;
-        if (gemm && mhi > mlo) {
+        if (gemm && mhi > mlo &&
+            plasma_cuda_sweep_update_dmma(s, st, uplo, trans, A, B, k, mlo, mhi)) {
+            // FP64: the DMMA update kernel (cuda/update.cu)
+        } else if (gemm && mhi > mlo) {
             const int mb = B.mb, kr = plasma_tile_mview(B, k);
             plasma_view_t lv, bv, cv;
             memset(&lv, 0, sizeof(lv));
