@@ -130,8 +130,9 @@ void sweep(cudaStream_t s, plasma_devstat_t *st, int uplo, int trans,
         int mlo = trans ? 0 : k + 1;
         int mhi = trans ? k : mt;
         if (gemm && mhi > mlo &&
-            plasma_cuda_sweep_update_dmma(s, st, uplo, trans, A, B, k, mlo, mhi)) {
-            // FP64: the DMMA update kernel (cuda/update.cu)
+            plasma_cuda_sweep_update_mma(s, st, uplo, trans, A, B, k, mlo, mhi)) {
+            // square tiles, a multiple of 128: the tensor-core sweep update
+            // (cuda/update.cu)
         } else if (gemm && mhi > mlo) {
             const int mb = B.mb, kr = plasma_tile_mview(B, k);
             plasma_view_t lv, bv, cv;

@@ -16,6 +16,7 @@
 // FP32 (and the transposed upper-storage fallback): SIMT FFMA/DFMA 8x8
 // register tiles.
 #include "common.cuh"
+#include "mma.cuh"
 
 namespace {
 
@@ -273,13 +274,13 @@ k_update_dmma(plasma_desc_t A, int k, int nlo, int nhi, int nitems,
 }
 
 // ---------------------------------------------------------------------------
-// FP64 update step of a tile sweep with many right-hand sides (solve.cu):
+// Update step of a tile sweep with many right-hand sides (solve.cu):
 //     B(m, :) -= a_m B(k, :)      for the row tiles m in [mlo, mhi)
 // with a_m the factor block that couples tile row m with tile row k:
 // L(m,k) (forward) or L(k,m)^T (backward), read from the storage triangle.
-// Same DMMA core as k_update_dmma (128 x 64 CTA tiles, 8 warps, K in
-// chunks of 16 through a 4-stage cp.async ring, two CTAs per SM); the
-// operands differ: the right-hand-side block b(kk, j) = B(k, :)(kk, j) is
+// Same core as k_update_dmma (128 x 64 CTA tiles, 8 warps, K in chunks of
+// 16 through a 4-stage cp.async ring, two CTAs per SM): DMMA for FP64, the
+// three-product TF32 split (FP32-accurate) for FP32.  The operands differ: the right-hand-side block b(kk, j) = B(k, :)(kk, j) is
 // contiguous along K, and so is a_m when it is the transposed view.
 // Those are copied element by element into the [K][row] stage layout (the
 // shared-memory writes conflict, the tensor-core reads stay conflict-free).
@@ -292,13 +293,24 @@ struct SweepArgs {
     int sbm, ncb;             // row halves per tile, 64-column blocks of B
 };
 
+template <typename T>
+struct SweepGeo {
+    static constexpr int LDS_A = DBM + Pad<T>::v;   // conflict-free fragment reads
+    static constexpr int LDS_B = DBN + Pad<T>::v;
+    static constexpr int EPV = 16 / (int)sizeof(T); // elements per 16-byte copy
+    static constexpr int SMEM = DSTAGES * DBK * (LDS_A + LDS_B) * (int)sizeof(T);
+};
+
+template <typename T>
 __global__ void __launch_bounds__(THREADS, 2)
-k_sweep_dmma(SweepArgs g, int nitems, const plasma_devstat_t *st)
+k_sweep_mma(SweepArgs g, int nitems, const plasma_devstat_t *st)
 {
+    using G = SweepGeo<T>;
+    constexpr int LA = G::LDS_A, LB = G::LDS_B, EPV = G::EPV;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (plasma_failed(st)) return;
-    double *As = reinterpret_cast<double *>(smem_raw);
-    double *Bs = As + DSTAGES * DBK * DLDS_A;
+    T *As = reinterpret_cast<T *>(smem_raw);
+    T *Bs = As + DSTAGES * DBK * LA;
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int gq = lane >> 2, t = lane & 3;
@@ -328,28 +340,27 @@ k_sweep_dmma(SweepArgs g, int nitems, const plasma_devstat_t *st)
         // U(k,m)^T)
         const int am = a_rows ? m : g.k;
         const int an = a_rows ? g.k : m;
-        const double *pa = (const double *)plasma_tile_addr(g.L, am, an);
+        const T *pa = (const T *)plasma_tile_addr(g.L, am, an);
         const int lda = plasma_tile_mmain(g.L, am);
-        const double *pb = (const double *)plasma_tile_addr(g.B, g.k, jt) +
+        const T *pb = (const T *)plasma_tile_addr(g.B, g.k, jt) +
                            (size_t)jo * plasma_tile_mmain(g.B, g.k);
         const int ldb = plasma_tile_mmain(g.B, g.k);
-        double *C = (double *)plasma_tile_addr(g.B, m, jt) +
+        T *C = (T *)plasma_tile_addr(g.B, m, jt) +
                     (size_t)jo * plasma_tile_mmain(g.B, m);
         const int ldc = plasma_tile_mmain(g.B, m);
-        const bool vec = a_rows && ((lda | rows) & 1) == 0;
+        const bool vec = a_rows && lda % EPV == 0 && rows % EPV == 0;
 
         auto load_stage = [&](int kc, int sl) {
-            double *as = As + sl * DBK * DLDS_A;
-            double *bs = Bs + sl * DBK * DLDS_B;
+            T *as = As + sl * DBK * LA;
+            T *bs = Bs + sl * DBK * LB;
             if (vec) {
 #pragma unroll
-                for (int q = 0; q < (DBM * DBK / 2) / THREADS; q++) {
+                for (int q = 0; q < (DBM * DBK / EPV) / THREADS; q++) {
                     const int e = tid + q * THREADS;
-                    const int r = 2 * (e % (DBM / 2)), c = e / (DBM / 2);
+                    const int r = EPV * (e % (DBM / EPV)), c = e / (DBM / EPV);
                     const int gi = i0 + r, gk = kc + c;
                     const bool v = gi < rows && gk < K;
-                    cp_async_16(as + c * DLDS_A + r,
-                                v ? pa + (size_t)gk * lda + gi : pa, v);
+                    cp_async_16(as + c * LA + r, v ? pa + (size_t)gk * lda + gi : pa, v);
                 }
             } else if (a_rows) {
 #pragma unroll
@@ -358,7 +369,7 @@ k_sweep_dmma(SweepArgs g, int nitems, const plasma_devstat_t *st)
                     const int r = e % DBM, c = e / DBM;
                     const int gi = i0 + r, gk = kc + c;
                     const bool v = gi < rows && gk < K;
-                    cp_async_8(as + c * DLDS_A + r, v ? pa + (size_t)gk * lda + gi : pa, v);
+                    cp_async_el(as + c * LA + r, v ? pa + (size_t)gk * lda + gi : pa, v);
                 }
             } else {
                 // a_m(i, kk) = tile[i * lda + kk]: lanes walk kk
@@ -368,7 +379,7 @@ k_sweep_dmma(SweepArgs g, int nitems, const plasma_devstat_t *st)
                     const int c = e % DBK, r = e / DBK;
                     const int gi = i0 + r, gk = kc + c;
                     const bool v = gi < rows && gk < K;
-                    cp_async_8(as + c * DLDS_A + r, v ? pa + (size_t)gi * lda + gk : pa, v);
+                    cp_async_el(as + c * LA + r, v ? pa + (size_t)gi * lda + gk : pa, v);
                 }
             }
             // b(kk, j) = B(k)(kk, jo + j) = pb[j * ldb + kk]: lanes walk kk
@@ -378,17 +389,17 @@ k_sweep_dmma(SweepArgs g, int nitems, const plasma_devstat_t *st)
                 const int c = e % DBK, r = e / DBK;
                 const int gk = kc + c;
                 const bool v = r < cols && gk < K;
-                cp_async_8(bs + c * DLDS_B + r, v ? pb + (size_t)r * ldb + gk : pb, v);
+                cp_async_el(bs + c * LB + r, v ? pb + (size_t)r * ldb + gk : pb, v);
             }
         };
 
-        double acc[2][4][4];
+        T acc[2][4][4];
 #pragma unroll
         for (int a = 0; a < 2; a++)
 #pragma unroll
             for (int b = 0; b < 4; b++)
 #pragma unroll
-                for (int c = 0; c < 4; c++) acc[a][b][c] = 0.0;
+                for (int c = 0; c < 4; c++) acc[a][b][c] = T(0);
 
         const int nk = (K + DBK - 1) / DBK;
         __syncthreads();   // the previous item's readers are done with smem
@@ -403,25 +414,25 @@ k_sweep_dmma(SweepArgs g, int nitems, const plasma_devstat_t *st)
             const int pf = kt + DSTAGES - 1;
             if (pf < nk) load_stage(pf * DBK, pf % DSTAGES);
             cp_async_commit();
-            const double *as = As + (kt % DSTAGES) * DBK * DLDS_A + wm * 32;
-            const double *bs = Bs + (kt % DSTAGES) * DBK * DLDS_B + wn * 32;
+            const T *as = As + (kt % DSTAGES) * DBK * LA + wm * 32;
+            const T *bs = Bs + (kt % DSTAGES) * DBK * LB + wn * 32;
 #pragma unroll
             for (int k8 = 0; k8 < DBK; k8 += 8) {
-                double bf[4][2];
+                T bf[4][2];
 #pragma unroll
                 for (int ni = 0; ni < 4; ni++) {
-                    bf[ni][0] = bs[(k8 + t) * DLDS_B + ni * 8 + gq];
-                    bf[ni][1] = bs[(k8 + t + 4) * DLDS_B + ni * 8 + gq];
+                    bf[ni][0] = bs[(k8 + t) * LB + ni * 8 + gq];
+                    bf[ni][1] = bs[(k8 + t + 4) * LB + ni * 8 + gq];
                 }
 #pragma unroll
                 for (int mi = 0; mi < 2; mi++) {
-                    double af[4];
-                    af[0] = as[(k8 + t) * DLDS_A + mi * 16 + gq];
-                    af[1] = as[(k8 + t) * DLDS_A + mi * 16 + gq + 8];
-                    af[2] = as[(k8 + t + 4) * DLDS_A + mi * 16 + gq];
-                    af[3] = as[(k8 + t + 4) * DLDS_A + mi * 16 + gq + 8];
+                    T af[4];
+                    af[0] = as[(k8 + t) * LA + mi * 16 + gq];
+                    af[1] = as[(k8 + t) * LA + mi * 16 + gq + 8];
+                    af[2] = as[(k8 + t + 4) * LA + mi * 16 + gq];
+                    af[3] = as[(k8 + t + 4) * LA + mi * 16 + gq + 8];
 #pragma unroll
-                    for (int ni = 0; ni < 4; ni++) dmma_16x8x8(acc[mi][ni], af, bf[ni]);
+                    for (int ni = 0; ni < 4; ni++) mma8<3>(acc[mi][ni], af, bf[ni]);
                 }
             }
         }
@@ -430,7 +441,7 @@ k_sweep_dmma(SweepArgs g, int nitems, const plasma_devstat_t *st)
         // C -= acc, all loads of a row fragment before its stores
 #pragma unroll
         for (int mi = 0; mi < 2; mi++) {
-            double cv[2][4][2];
+            T cv[2][4][2];
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const int i = i0 + wm * 32 + mi * 16 + gq + h * 8;
@@ -439,7 +450,7 @@ k_sweep_dmma(SweepArgs g, int nitems, const plasma_devstat_t *st)
 #pragma unroll
                     for (int e = 0; e < 2; e++) {
                         const int j = wn * 32 + ni * 8 + 2 * t + e;
-                        cv[h][ni][e] = (i < rows && j < cols) ? C[(size_t)j * ldc + i] : 0.0;
+                        cv[h][ni][e] = (i < rows && j < cols) ? C[(size_t)j * ldc + i] : T(0);
                     }
             }
 #pragma unroll
@@ -593,16 +604,18 @@ extern "C" void plasma_cuda_update(cudaStream_t s, plasma_devstat_t *st,
     plasma_prof_end(prof, s, PLASMA_KCLASS_UPDATE, flops, bytes);
 }
 
-// One update step of an FP64 tile sweep with many right-hand sides (see
-// k_sweep_dmma): B rows of tiles [mlo, mhi) -= the factor block coupling
-// them with tile row k times B(k, :).  Returns 0 (nothing launched) when
-// the tiling does not fit (square tiles, a multiple of 128).
-extern "C" int plasma_cuda_sweep_update_dmma(cudaStream_t s, plasma_devstat_t *st,
-                                             plasma_enum_t uplo, int trans,
-                                             plasma_desc_t L, plasma_desc_t B, int k,
-                                             int mlo, int mhi)
+// One update step of a tile sweep with many right-hand sides (see
+// k_sweep_mma): B rows of tiles [mlo, mhi) -= the factor block coupling them
+// with tile row k times B(k, :).  FP64 on DMMA, FP32 as three TF32
+// products.  Returns 0 (nothing launched) when the tiling does not fit
+// (square tiles, a multiple of 128).
+extern "C" int plasma_cuda_sweep_update_mma(cudaStream_t s, plasma_devstat_t *st,
+                                            plasma_enum_t uplo, int trans,
+                                            plasma_desc_t L, plasma_desc_t B, int k,
+                                            int mlo, int mhi)
 {
-    if (L.precision != PlasmaRealDouble || B.precision != PlasmaRealDouble ||
+    if (L.precision != B.precision ||
+        (L.precision != PlasmaRealDouble && L.precision != PlasmaRealFloat) ||
         L.mb != L.nb || B.mb != L.mb || B.nb != L.nb || L.mb % DBM != 0 ||
         L.i != 0 || L.j != 0 || B.i != 0 || B.j != 0)
         return 0;
@@ -619,14 +632,25 @@ extern "C" int plasma_cuda_sweep_update_dmma(cudaStream_t s, plasma_devstat_t *s
     // 64-column blocks per column tile, times the column tiles
     g.ncb = ((B.nb + DBN - 1) / DBN) * B.nt;
     const long long nitems = (long long)(mhi - mlo) * g.sbm * g.ncb;
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_sweep_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             DSMEM);
-        attr_set = true;
-    }
     PLASMA_COUNT_LAUNCH();
-    k_sweep_dmma<<<(unsigned)nitems, THREADS, DSMEM, s>>>(g, (int)nitems, st);
+    if (L.precision == PlasmaRealDouble) {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_sweep_mma<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 SweepGeo<double>::SMEM);
+            attr = true;
+        }
+        k_sweep_mma<double><<<(unsigned)nitems, THREADS, SweepGeo<double>::SMEM, s>>>(
+            g, (int)nitems, st);
+    } else {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_sweep_mma<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 SweepGeo<float>::SMEM);
+            attr = true;
+        }
+        k_sweep_mma<float><<<(unsigned)nitems, THREADS, SweepGeo<float>::SMEM, s>>>(
+            g, (int)nitems, st);
+    }
     return 1;
 }
-

@@ -141,9 +141,9 @@ void plasma_cuda_trtri_tiles(cudaStream_t s, plasma_devstat_t *st,
 
 /* op(L) X = B in place (trans = PlasmaNoTrans or PlasmaTrans); W as above,
  * computed first when have_w == 0. */
-/* One FP64 update step of a many-rhs tile sweep on the DMMA kernel; 0
- * when the tiling does not fit (cuda/update.cu). */
-int plasma_cuda_sweep_update_dmma(cudaStream_t s, plasma_devstat_t *st,
+/* One update step of a many-rhs tile sweep on the tensor cores (FP64 DMMA,
+ * FP32 three-product TF32); 0 when the tiling does not fit (cuda/update.cu). */
+int plasma_cuda_sweep_update_mma(cudaStream_t s, plasma_devstat_t *st,
                                   plasma_enum_t uplo, int trans, plasma_desc_t L,
                                   plasma_desc_t B, int k, int mlo, int mhi);
 void plasma_cuda_trsm_sweep(cudaStream_t s, plasma_devstat_t *st,
