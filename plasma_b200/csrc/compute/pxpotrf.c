@@ -17,6 +17,8 @@
  * still running (look-ahead of depth 1).  Column k+2 is split off the bulk
  * update so that the critical stream only waits for the part it touches.
  * With PlasmaLookahead = 0 everything runs in program order on one stream.
+ * A matrix whose tile columns are still arriving (plasma_pXpotrf_arrivals)
+ * replaces the bulk stream by one stream per group of columns (walk_groups).
  *
  * Failure handling: POTRF(k) writes the device status word with
  * info = A.nb*k + j (compute/pzpotrf.c:44); every later kernel reads the word

@@ -3,7 +3,7 @@
 The reference's testers accept a result when it agrees with LAPACK within
 tol * eps, tol = 50 (test/test_zpotrf.c:124-152, test/test_zposv.c:137-167,
 test/test_zcposv.c:139-193).  The oracle must pass the same checks on the
-committed fixtures before it is trusted to judge the GPU library.
+committed fixtures before it is trusted as the checker of the GPU library.
 """
 import numpy as np
 import pytest
