@@ -655,3 +655,49 @@ def test_potri_poinv_info(L):
     np.testing.assert_array_equal(f, keep)
     z = np.asfortranarray(gen.zerocol(a, 120))
     assert L.plasma_dpoinv(LO, n, z.ctypes.data, n) == 121
+
+
+def _device_colmajor(a, lda):
+    """Column-major device copy of a with leading dimension lda."""
+    n, m = a.shape
+    t = torch.zeros((m, lda), dtype=torch.float64, device="cuda")
+    t[:, :n] = torch.from_numpy(np.ascontiguousarray(a.T)).cuda()
+    return t
+
+
+@pytest.mark.parametrize("n,nb", [(1000, 256), (777, 128)])
+def test_dsposv_device_pointer(L, n, nb):
+    """A lower-stored device matrix (lda > n) goes to the FP64 and FP32 tile
+    copies in one pass inside the solve; the answer matches the oracle."""
+    set_nb(L, nb)
+    a, b = gen.diag_dominant(n, 2, seed=4400 + n)
+    lda = n + 3
+    A, B = _device_colmajor(a, lda), _device_colmajor(b, lda)
+    X = torch.zeros((2, lda), dtype=torch.float64, device="cuda")
+    it = ctypes.c_int(-99)
+    assert L.plasma_dsposv(LO, n, 2, A.data_ptr(), lda, B.data_ptr(), lda, X.data_ptr(), lda,
+                           ctypes.byref(it)) == 0
+    assert 0 <= it.value <= 30
+    x = X[:, :n].cpu().numpy().T
+    xo = np.zeros((n, 2), order="F")
+    assert oracle.dsposv(oracle.LOWER, np.asfortranarray(a), np.asfortranarray(b), xo, nb)[0] == 0
+    np.testing.assert_allclose(x, xo, rtol=1e-12, atol=1e-15)
+    # the caller's array is not modified
+    np.testing.assert_array_equal(A[:, :n].cpu().numpy().T, a)
+
+
+def test_dsposv_device_pointer_fp32_overflow(L):
+    """Entries beyond the FP32 range: the one-pass conversion reports the
+    overflow, the FP32 attempt is abandoned and the FP64 fallback solves the
+    system from the FP64 tiles the same pass wrote (iter = -31)."""
+    set_nb(L, 128)
+    n = 600
+    a, b = gen.diag_dominant(n, 1, seed=4500)
+    a = a * 1e39
+    A, B = _device_colmajor(a, n), _device_colmajor(b, n)
+    X = torch.zeros((1, n), dtype=torch.float64, device="cuda")
+    it = ctypes.c_int()
+    assert L.plasma_dsposv(LO, n, 1, A.data_ptr(), n, B.data_ptr(), n, X.data_ptr(), n,
+                           ctypes.byref(it)) == 0
+    assert it.value == -31
+    assert solve_residual(a, X.cpu().numpy().T.copy(), b) < TOL * EPS
