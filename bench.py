@@ -52,7 +52,8 @@ def parse():
     p.add_argument("--no-dposv", action="store_true")
     p.add_argument("--batch-count", type=int, default=4096,
                    help="matrices of the batched workload")
-    p.add_argument("--workload", default="dsposv", choices=["dsposv", "adjoint", "batched", "inverse"],
+    p.add_argument("--workload", default="dsposv", choices=["dsposv", "adjoint", "batched", "inverse",
+                                                     "band"],
                    help="dsposv: the headline; adjoint / batched: the differentiation "
                         "and batched-solve configurations, one JSON line each")
     return p.parse_args()
@@ -358,6 +359,63 @@ def run_inverse(args):
     return 0
 
 
+def run_band(args):
+    """plasma_dpbsv / plasma_spbsv (band Cholesky + the two band sweeps) on a
+    device-resident SPD band matrix in LAPACK band storage, n = 32768 and
+    kd in {256, 1024, 4096}, one right-hand side.  AB = U[-0.5, 0.5] with
+    2 kd + 1 added to the diagonal (diagonally dominant), b ~ U[-1, 1]
+    (seed 9).  GFLOP/s counts LAPACK's flops for dpbtrf (n (kd^2 + 3 kd))
+    and dpbtrs (4 n kd nrhs); the error is the reference tester's residual
+    ||b - A x||_inf / (n ||A||_F ||x||_inf)."""
+    import torch
+    import plasma_b200 as pb
+    L = pb.lib()
+    assert L.plasma_init() == 0
+    n, rows = 32768, []
+    for kd in (256, 1024, 4096):
+        g = torch.Generator(device="cuda").manual_seed(9)
+        # column-major (kd+1) x n storage = row-major n x (kd+1)
+        AB0 = torch.rand(n, kd + 1, generator=g, device="cuda", dtype=torch.float64) - 0.5
+        AB0[:, 0] += 2 * kd + 1
+        for d in range(1, kd + 1):
+            AB0[n - d:, d] = 0.0
+        b0 = torch.rand(n, generator=g, device="cuda", dtype=torch.float64) * 2 - 1
+        for dt, fn in ((torch.float64, "d"), (torch.float32, "s")):
+            AB1, b1 = AB0.to(dt), b0.to(dt)
+            times = []
+            for rep in range(args.warmup + args.steps):
+                AB, x = AB1.clone(), b1.clone()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record()
+                rc = getattr(L, f"plasma_{fn}pbsv")(pb.PlasmaLower, n, kd, 1, AB.data_ptr(),
+                                                    kd + 1, x.data_ptr(), n)
+                e1.record()
+                torch.cuda.synchronize()
+                assert rc == 0, rc
+                if rep >= args.warmup:
+                    times.append(e0.elapsed_time(e1))
+            xd = x.double()
+            ax = AB0[:, 0] * xd
+            for d in range(1, kd + 1):
+                ax[d:] += AB0[:n - d, d] * xd[:n - d]
+                ax[:n - d] += AB0[:n - d, d] * xd[d:]
+            anorm = torch.sqrt((AB0[:, 0] ** 2).sum() + 2 * (AB0[:, 1:] ** 2).sum())
+            res = ((b0 - ax).abs().max() / (n * anorm * xd.abs().max())).item()
+            ms = min(times)
+            flops = n * (kd * kd + 3.0 * kd) + 4.0 * n * kd
+            rows.append({"routine": f"{fn}pbsv", "n": n, "kd": kd, "ms": ms,
+                         "gflops": flops / ms / 1e6, "tester_residual": res})
+            del AB, AB1, x
+    print(json.dumps({"workload": "band", "metric": "time of the SPD band solve "
+                      "(pbsv = pbtrf + pbtrs), device-resident AB, uplo = L, nrhs = 1",
+                      "unit": "ms", "steps": args.steps, "warmup": args.warmup,
+                      "results": rows}), flush=True)
+    L.plasma_finalize()
+    return 0
+
+
 def run_batched(args):
     """4096 SPD systems, n uniform in [16, 512] (seed 5), A = G G^T / n + 0.1 I,
     b ~ N(0,1), FP64 and FP32: one batched posv (factor + solve) launch per
@@ -445,6 +503,8 @@ def main():
         return run_adjoint(args)
     if args.workload == "inverse":
         return run_inverse(args)
+    if args.workload == "band":
+        return run_band(args)
     if args.workload == "batched":
         return run_batched(args)
     if args.impl == "reference":

@@ -11,7 +11,9 @@
  *   triangle : lower  tile (m,n), n <= m, at mb*nb*((m-n) + n*(2*lm1-n+1)/2),
  *              upper  tile (m,n), m <= n, at mb*nb*(m + n*(n+1)/2);
  *   ragged   : the last tile row (height gm%mb) lives in region A21, the last
- *              tile column (width gn%nb) in A12, the corner tile in A22.
+ *              tile column (width gn%nb) in A12, the corner tile in A22;
+ *   band     : tile (m,n) at the general position ((kut-1)+m-n, n) of a
+ *              layout gm = mb*(kut+klt-1) rows high (:154-157).
  *
  * Each tile is column-major with leading dimension plasma_tile_mmain().
  *
@@ -118,10 +120,19 @@ PLASMA_HD size_t plasma_tile_offset_triangle(plasma_desc_t A, int m, int n)
                     : A.A22;
 }
 
+/* Element offset of tile (m,n) of a band descriptor (type PlasmaGeneralBand,
+ * reference include/plasma_descriptor.h:154-157): the tiles of the band of
+ * tile column n are stored down column n of a general layout with gm/mb tile
+ * rows, tile (m,n) at tile row (kut-1) + m - n.  The view starts on the
+ * diagonal (i = j), and gm is a multiple of mb, so only the last tile column
+ * can be narrow (region A12) -- plasma_desc_general_band_check. */
 PLASMA_HD size_t plasma_tile_offset(plasma_desc_t A, int m, int n)
 {
-    return A.type == PlasmaGeneral ? plasma_tile_offset_general(A, m, n)
-                                   : plasma_tile_offset_triangle(A, m, n);
+    if (A.type == PlasmaLower || A.type == PlasmaUpper)
+        return plasma_tile_offset_triangle(A, m, n);
+    /* band: the general formula at the stored tile row */
+    const int row = A.type == PlasmaGeneralBand ? A.kut - 1 + m - n - A.i / A.mb : m;
+    return plasma_tile_offset_general(A, row, n);
 }
 
 PLASMA_HD void *plasma_tile_addr(plasma_desc_t A, int m, int n)
@@ -133,7 +144,10 @@ PLASMA_HD void *plasma_tile_addr(plasma_desc_t A, int m, int n)
 /* Height of the tile stored at tile row k (its leading dimension). */
 PLASMA_HD int plasma_tile_mmain(plasma_desc_t A, int k)
 {
-    return (A.i / A.mb + k < A.gm / A.mb) ? A.mb : A.gm % A.mb;
+    /* with gm a multiple of mb every stored tile is mb rows high (no tile
+     * row of height 0 exists); band descriptors always are, and ask with
+     * their matrix row index k */
+    return (A.i / A.mb + k < A.gm / A.mb || A.gm % A.mb == 0) ? A.mb : A.gm % A.mb;
 }
 
 /* Width of the tile stored at tile column k. */
@@ -179,9 +193,21 @@ int plasma_desc_general_init(plasma_enum_t precision, void *matrix,
 int plasma_desc_triangular_init(plasma_enum_t precision, plasma_enum_t uplo,
                                 void *matrix, int mb, int nb, int lm, int ln,
                                 int i, int j, int m, int n, plasma_desc_t *A);
+/* reference control/descriptor.c:50-82 (band storage, device memory) */
+int plasma_desc_general_band_create(plasma_enum_t precision, plasma_enum_t uplo,
+                                    int mb, int nb, int lm, int ln,
+                                    int i, int j, int m, int n, int kl, int ku,
+                                    plasma_desc_t *A);
+/* reference control/descriptor.c:178-213 */
+int plasma_desc_general_band_init(plasma_enum_t precision, plasma_enum_t uplo,
+                                  void *matrix, int mb, int nb, int lm, int ln,
+                                  int i, int j, int m, int n, int kl, int ku,
+                                  plasma_desc_t *A);
 /* reference control/descriptor.c:267-319 */
 int plasma_desc_check(plasma_desc_t A);
 int plasma_desc_general_check(plasma_desc_t A);
+/* reference control/descriptor.c:321-369 */
+int plasma_desc_general_band_check(plasma_desc_t A);
 /* reference control/descriptor.c:374-397 */
 plasma_desc_t plasma_desc_view(plasma_desc_t A, int i, int j, int m, int n);
 

@@ -42,6 +42,32 @@ void plasma_omp_spotri(plasma_enum_t uplo, plasma_desc_t A,
 void plasma_omp_spoinv(plasma_enum_t uplo, plasma_desc_t A,
                        plasma_sequence_t *sequence, plasma_request_t *request);
 
+/* reference compute/zpbtrf.c:77-158: Cholesky of an SPD band matrix in
+ * LAPACK band storage (AB(kd+1+i-j,j) upper, AB(1+i-j,j) lower) */
+int plasma_spbtrf(plasma_enum_t uplo, int n, int kd, float *pAB, int ldab);
+/* reference compute/zpbtrs.c:81-182: solve with the band factor */
+int plasma_spbtrs(plasma_enum_t uplo, int n, int kd, int nrhs,
+                  float *pAB, int ldab, float *pB, int ldb);
+/* reference compute/zpbsv.c:92-193: factor and solve */
+int plasma_spbsv(plasma_enum_t uplo, int n, int kd, int nrhs,
+                 float *pAB, int ldab, float *pB, int ldb);
+
+/* reference compute/zpbtrf.c:202-242 (AB: a band descriptor) */
+void plasma_omp_spbtrf(plasma_enum_t uplo, plasma_desc_t AB,
+                       plasma_sequence_t *sequence, plasma_request_t *request);
+/* reference compute/zpbtrs.c:236-295 */
+void plasma_omp_spbtrs(plasma_enum_t uplo, plasma_desc_t AB, plasma_desc_t B,
+                       plasma_sequence_t *sequence, plasma_request_t *request);
+/* reference compute/zpbsv.c:242-302 */
+void plasma_omp_spbsv(plasma_enum_t uplo, plasma_desc_t AB, plasma_desc_t B,
+                      plasma_sequence_t *sequence, plasma_request_t *request);
+/* reference compute/zpb2desc.c (pAB host or device) */
+void plasma_omp_spb2desc(float *pAB, int ldab, plasma_desc_t A,
+                         plasma_sequence_t *sequence, plasma_request_t *request);
+/* reference compute/zdesc2pb.c */
+void plasma_omp_sdesc2pb(plasma_desc_t A, float *pAB, int ldab,
+                         plasma_sequence_t *sequence, plasma_request_t *request);
+
 /* reference compute/zpotrf.c:206-246 */
 void plasma_omp_spotrf(plasma_enum_t uplo, plasma_desc_t A,
                        plasma_sequence_t *sequence, plasma_request_t *request);

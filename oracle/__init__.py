@@ -29,7 +29,9 @@ def lib():
             getattr(L, f"{p}oracle_potrs").argtypes = [ci, ci, ci, vp, ci, vp, ci, ci]
             getattr(L, f"{p}oracle_posv").argtypes = [ci, ci, ci, vp, ci, vp, ci, ci]
             getattr(L, f"{p}oracle_potri").argtypes = [ci, ci, vp, ci]
-            for f in ("potrf", "potrs", "posv", "potri"):
+            getattr(L, f"{p}oracle_pbtrf").argtypes = [ci, ci, ci, vp, ci, ci]
+            getattr(L, f"{p}oracle_pbtrs").argtypes = [ci, ci, ci, ci, vp, ci, vp, ci, ci]
+            for f in ("potrf", "potrs", "posv", "potri", "pbtrf", "pbtrs"):
                 getattr(L, f"{p}oracle_{f}").restype = ci
         L.oracle_dsposv.argtypes = [ci, ci, ci, vp, ci, vp, ci, vp, ci,
                                     ctypes.POINTER(ci), ci]
@@ -74,6 +76,21 @@ def posv(uplo, a, b, nb):
     n, nrhs = b.shape
     return getattr(lib(), f"{_prefix(a)}oracle_posv")(uplo, n, nrhs, _p(a),
                                                       a.shape[0], _p(b), b.shape[0], nb)
+
+
+def pbtrf(uplo, ab, kd, nb):
+    """In-place band tile Cholesky of the Fortran-ordered LAPACK band array ab
+    ((ldab >= kd+1) x n); returns info (ab unchanged when info > 0)."""
+    return getattr(lib(), f"{_prefix(ab)}oracle_pbtrf")(uplo, ab.shape[1], kd, _p(ab),
+                                                        ab.shape[0], nb)
+
+
+def pbtrs(uplo, ab, kd, b, nb):
+    """Solves with the band factor held in ab; b (n x nrhs, Fortran order) is
+    overwritten with the solution."""
+    n, nrhs = b.shape
+    return getattr(lib(), f"{_prefix(ab)}oracle_pbtrs")(uplo, n, kd, nrhs, _p(ab),
+                                                        ab.shape[0], _p(b), b.shape[0], nb)
 
 
 def dsposv(uplo, a, b, x, nb):

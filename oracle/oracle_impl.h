@@ -9,6 +9,8 @@
  *   tile Cholesky        compute/pzpotrf.c:27-126
  *   tile triangular solve compute/pztrsm.c:113-177 (Left, Lower) and
  *                        :43-107 (Left, Upper)
+ *   band tile Cholesky   compute/pzpbtrf.c:37-118, and the band solves
+ *                        (compute/pztbsm.c) as the tile solve cut to the band
  *   the LAPACK/BLAS tile kernels the reference calls through CBLAS/LAPACKE
  *   (core_blas/core_zpotrf.c:54-63, core_ztrsm.c:87-100, core_zsyrk.c,
  *   core_zgemm.c:89-102), written out from the published LAPACK algorithms
@@ -312,8 +314,12 @@ static int P(p_potrf)(P(tiles_t) *A, int uplo)
 }
 
 /* compute/pztrsm.c (Left): trans = 0 solves op = L (or U^T), 1 solves L^T (or U)
- * B is n x nrhs in tiles (B->mt row tiles, one column block per nb cols). */
-static void P(p_trsm)(P(tiles_t) *A, P(tiles_t) *B, int nrhs, int uplo, int second)
+ * B is n x nrhs in tiles (B->mt row tiles, one column block per nb cols).
+ * kt > 0: the factor is a band of kt tiles per tile column (diagonal
+ * included), and only those tiles are visited, as in the reference's band
+ * solve compute/pztbsm.c. */
+static void P(p_trsm)(P(tiles_t) *A, P(tiles_t) *B, int nrhs, int uplo, int second,
+                      int kt)
 {
     const int mt = A->mt, nb = A->nb;
     const int nt = (nrhs + nb - 1) / nb;
@@ -339,6 +345,10 @@ static void P(p_trsm)(P(tiles_t) *A, P(tiles_t) *B, int nrhs, int uplo, int seco
             }
         }
         int mlo = second ? 0 : k + 1, mhi = second ? k : mt;
+        if (kt > 0) {
+            if (second) mlo = k - kt + 1 > 0 ? k - kt + 1 : 0;
+            else        mhi = k + kt < mt ? k + kt : mt;
+        }
         for (int m = mlo; m < mhi; m++) {
             int nm = P(tile_rows)(A, m);
             for (int n = 0; n < nt; n++) {
@@ -370,7 +380,134 @@ static void P(p_trsm)(P(tiles_t) *A, P(tiles_t) *B, int nrhs, int uplo, int seco
     }
 }
 
+/* compute/pzpbtrf.c:37-118: the band tile loop.  For each k: POTRF of tile
+ * (k,k); for the tiles m = k+1 .. k+kt-1 of the band below it (right of it
+ * for upper storage): TRSM, SYRK on (m,m), GEMM on (m,n) for k < n < m.
+ * Tiles outside the band are never visited.  Returns info as p_potrf. */
+static int P(p_pbtrf)(P(tiles_t) *A, int uplo, int kt)
+{
+    int info = 0;
+    const int mt = A->mt, nb = A->nb;
+    #pragma omp parallel
+    #pragma omp master
+    {
+        for (int k = 0; k < mt; k++) {
+            REAL *akk = TL(A, k, k);
+            int nk = P(tile_rows)(A, k);
+            #pragma omp task depend(inout: akk[0]) shared(info)
+            {
+                int st;
+                #pragma omp atomic read
+                st = info;
+                if (st == 0) {
+                    int i = uplo == ORACLE_LOWER ? P(k_potrf_lower)(nk, akk, nk)
+                                                 : P(k_potrf_upper)(nk, akk, nk);
+                    if (i != 0) {
+                        #pragma omp critical (oracle_info)
+                        if (info == 0) info = nb * k + i;
+                    }
+                }
+            }
+            const int mhi = k + kt < mt ? k + kt : mt;
+            for (int m = k + 1; m < mhi; m++) {
+                int nm = P(tile_rows)(A, m);
+                if (uplo == ORACLE_LOWER) {
+                    REAL *amk = TL(A, m, k);
+                    #pragma omp task depend(in: akk[0]) depend(inout: amk[0]) shared(info)
+                    if (info == 0) P(k_trsm_rlt)(nm, nk, akk, nk, amk, nm);
+                } else {
+                    REAL *akm = TL(A, k, m);
+                    #pragma omp task depend(in: akk[0]) depend(inout: akm[0]) shared(info)
+                    if (info == 0) P(k_trsm_lut)(nk, nm, akk, nk, akm, nk);
+                }
+                for (int n = k + 1; n <= m; n++) {
+                    int nn = P(tile_rows)(A, n);
+                    if (uplo == ORACLE_LOWER) {
+                        REAL *amk = TL(A, m, k), *ank = TL(A, n, k), *amn = TL(A, m, n);
+                        #pragma omp task depend(in: amk[0], ank[0]) depend(inout: amn[0]) shared(info)
+                        if (info == 0)
+                            P(k_gemm_nt)(nm, nn, nk, amk, nm, ank, nn, amn, nm, m == n);
+                    } else {
+                        REAL *akn = TL(A, k, n), *akm = TL(A, k, m), *anm = TL(A, n, m);
+                        #pragma omp task depend(in: akn[0], akm[0]) depend(inout: anm[0]) shared(info)
+                        if (info == 0)
+                            P(k_gemm_tn)(nn, nm, nk, akn, nk, akm, nk, anm, nn, m == n);
+                    }
+                }
+            }
+        }
+    }
+    return info;
+}
+
+/* LAPACK band storage <-> tiles of the n x n matrix (zero outside the band):
+ * A(i,j) = AB[off + i - j + j*ldab], off = kd (upper) or 0 (lower), for
+ * 0 <= i-j <= kd (lower) or 0 <= j-i <= kd (upper) -- the layout of
+ * compute/pzpb2desc.c:20-22. */
+static void P(band_to_tiles)(P(tiles_t) *T, int uplo, int kd, const REAL *AB, int ldab)
+{
+    const int n = T->n, nb = T->nb, off = uplo == ORACLE_UPPER ? kd : 0;
+    for (int j = 0; j < n; j++) {
+        int i0 = uplo == ORACLE_LOWER ? j : (j - kd > 0 ? j - kd : 0);
+        int i1 = uplo == ORACLE_LOWER ? (j + kd < n - 1 ? j + kd : n - 1) : j;
+        for (int i = i0; i <= i1; i++) {
+            int m = i / nb, k = j / nb;
+            TL(T, m, k)[(size_t)(j - k * nb) * P(tile_rows)(T, m) + (i - m * nb)] =
+                AB[(size_t)j * ldab + off + i - j];
+        }
+    }
+}
+
+static void P(tiles_to_band)(const P(tiles_t) *T, int uplo, int kd, REAL *AB, int ldab)
+{
+    const int n = T->n, nb = T->nb, off = uplo == ORACLE_UPPER ? kd : 0;
+    for (int j = 0; j < n; j++) {
+        int i0 = uplo == ORACLE_LOWER ? j : (j - kd > 0 ? j - kd : 0);
+        int i1 = uplo == ORACLE_LOWER ? (j + kd < n - 1 ? j + kd : n - 1) : j;
+        for (int i = i0; i <= i1; i++) {
+            int m = i / nb, k = j / nb;
+            AB[(size_t)j * ldab + off + i - j] =
+                TL(T, m, k)[(size_t)(j - k * nb) * P(tile_rows)(T, m) + (i - m * nb)];
+        }
+    }
+}
+
 /* ---------------- LAPACK-layout entry points ---------------------------- */
+
+/* plasma_pbtrf (compute/zpbtrf.c): band tiles with kt = 1 + ceil(kd/nb), the
+ * reference's klt/kut (control/descriptor.c:204-211); AB is left unchanged
+ * when info > 0. */
+int P(oracle_pbtrf)(int uplo, int n, int kd, REAL *AB, int ldab, int nb)
+{
+    if (n == 0) return 0;
+    P(tiles_t) T;
+    P(tiles_alloc)(&T, n, nb, n);
+    P(band_to_tiles)(&T, uplo, kd, AB, ldab);
+    int info = P(p_pbtrf)(&T, uplo, 1 + (kd + nb - 1) / nb);
+    if (info == 0)
+        P(tiles_to_band)(&T, uplo, kd, AB, ldab);
+    P(tiles_free)(&T, n);
+    return info;
+}
+
+/* plasma_pbtrs (compute/zpbtrs.c:280-294): the two band sweeps */
+int P(oracle_pbtrs)(int uplo, int n, int kd, int nrhs, const REAL *AB, int ldab,
+                    REAL *B, int ldb, int nb)
+{
+    if (n == 0 || nrhs == 0) return 0;
+    P(tiles_t) TA, TB;
+    P(tiles_alloc)(&TA, n, nb, n);
+    P(tiles_alloc)(&TB, n, nb, nrhs);
+    P(band_to_tiles)(&TA, uplo, kd, AB, ldab);
+    P(to_tiles)(&TB, B, ldb, nrhs);
+    const int kt = 1 + (kd + nb - 1) / nb;
+    P(p_trsm)(&TA, &TB, nrhs, uplo, 0, kt);
+    P(p_trsm)(&TA, &TB, nrhs, uplo, 1, kt);
+    P(from_tiles)(&TB, B, ldb, nrhs, 0);
+    P(tiles_free)(&TA, n);
+    P(tiles_free)(&TB, nrhs);
+    return 0;
+}
 
 int P(oracle_potrf)(int uplo, int n, REAL *A, int lda, int nb)
 {
@@ -394,8 +531,8 @@ int P(oracle_potrs)(int uplo, int n, int nrhs, const REAL *A, int lda,
     P(tiles_alloc)(&TB, n, nb, nrhs);
     P(to_tiles)(&TA, A, lda, n);
     P(to_tiles)(&TB, B, ldb, nrhs);
-    P(p_trsm)(&TA, &TB, nrhs, uplo, 0);
-    P(p_trsm)(&TA, &TB, nrhs, uplo, 1);
+    P(p_trsm)(&TA, &TB, nrhs, uplo, 0, 0);
+    P(p_trsm)(&TA, &TB, nrhs, uplo, 1, 0);
     P(from_tiles)(&TB, B, ldb, nrhs, 0);
     P(tiles_free)(&TA, n);
     P(tiles_free)(&TB, nrhs);
@@ -413,8 +550,8 @@ int P(oracle_posv)(int uplo, int n, int nrhs, REAL *A, int lda, REAL *B,
     P(to_tiles)(&TB, B, ldb, nrhs);
     int info = P(p_potrf)(&TA, uplo);
     if (info == 0) {
-        P(p_trsm)(&TA, &TB, nrhs, uplo, 0);
-        P(p_trsm)(&TA, &TB, nrhs, uplo, 1);
+        P(p_trsm)(&TA, &TB, nrhs, uplo, 0, 0);
+        P(p_trsm)(&TA, &TB, nrhs, uplo, 1, 0);
         P(from_tiles)(&TA, A, lda, n, uplo);
         P(from_tiles)(&TB, B, ldb, nrhs, 0);
     }

@@ -37,6 +37,7 @@ PlasmaTrans = 112
 PlasmaUpper = 121
 PlasmaLower = 122
 PlasmaGeneral = 123
+PlasmaGeneralBand = 124
 PlasmaSuccess = 0
 PlasmaErrorNotInitialized = -101
 PlasmaErrorNotSupported = -102
@@ -164,6 +165,22 @@ _SIGNATURES = [
     ("plasma_omp_spotri", None, [c_int, _DESC, _SEQ, _REQ]),
     ("plasma_omp_dpoinv", None, [c_int, _DESC, _SEQ, _REQ]),
     ("plasma_omp_spoinv", None, [c_int, _DESC, _SEQ, _REQ]),
+    ("plasma_dpbtrf", c_int, [c_int, c_int, c_int, c_void_p, c_int]),
+    ("plasma_spbtrf", c_int, [c_int, c_int, c_int, c_void_p, c_int]),
+    ("plasma_dpbtrs", c_int, [c_int, c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_int]),
+    ("plasma_spbtrs", c_int, [c_int, c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_int]),
+    ("plasma_dpbsv", c_int, [c_int, c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_int]),
+    ("plasma_spbsv", c_int, [c_int, c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_int]),
+    ("plasma_omp_dpbtrf", None, [c_int, _DESC, _SEQ, _REQ]),
+    ("plasma_omp_spbtrf", None, [c_int, _DESC, _SEQ, _REQ]),
+    ("plasma_omp_dpbtrs", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
+    ("plasma_omp_spbtrs", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
+    ("plasma_omp_dpbsv", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
+    ("plasma_omp_spbsv", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
+    ("plasma_omp_dpb2desc", None, [c_void_p, c_int, _DESC, _SEQ, _REQ]),
+    ("plasma_omp_spb2desc", None, [c_void_p, c_int, _DESC, _SEQ, _REQ]),
+    ("plasma_omp_ddesc2pb", None, [_DESC, c_void_p, c_int, _SEQ, _REQ]),
+    ("plasma_omp_sdesc2pb", None, [_DESC, c_void_p, c_int, _SEQ, _REQ]),
     ("plasma_omp_dposv", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
     ("plasma_omp_sposv", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
     ("plasma_omp_dsposv", None, [c_int, _DESC, _DESC, _DESC, _DESC, _DESC, _DESC,
@@ -184,7 +201,11 @@ _SIGNATURES = [
      + [POINTER(plasma_desc_t)]),
     ("plasma_desc_triangular_init", c_int, [c_int, c_int, c_void_p] + [c_int] * 8
      + [POINTER(plasma_desc_t)]),
+    ("plasma_desc_general_band_create", c_int, [c_int] * 12 + [POINTER(plasma_desc_t)]),
+    ("plasma_desc_general_band_init", c_int, [c_int, c_int, c_void_p] + [c_int] * 10
+     + [POINTER(plasma_desc_t)]),
     ("plasma_desc_check", c_int, [_DESC]),
+    ("plasma_desc_general_band_check", c_int, [_DESC]),
     ("plasma_desc_general_check", c_int, [_DESC]),
     ("plasma_desc_view", plasma_desc_t, [_DESC, c_int, c_int, c_int, c_int]),
     ("plasma_desc_storage_bytes", c_size_t, [_DESC]),

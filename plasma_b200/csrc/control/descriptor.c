@@ -3,8 +3,9 @@
  *
  * Shape arithmetic and checks follow the reference's control/descriptor.c
  * (general_init :134-175, triangular_init :216-264, general_check :283-319,
- * view :374-397) because the region offsets A21/A12/A22 define the storage
- * format shared with callers.  Storage made by the *_create routines is device
+ * view :374-397; band init and check :178-213, :321-369) because the region
+ * offsets A21/A12/A22 and the band tile counts define the storage format
+ * shared with callers.  Storage made by the *_create routines is device
  * memory of the context's GPU (the reference uses malloc, :40 and :108-113),
  * zero-filled so that padding never holds stale values.
  */
@@ -16,7 +17,7 @@
 size_t plasma_desc_storage_bytes(plasma_desc_t A)
 {
     size_t elems;
-    if (A.type == PlasmaGeneral) {
+    if (A.type == PlasmaGeneral || A.type == PlasmaGeneralBand) {
         elems = (size_t)A.gm * A.gn;
     }
     else {
@@ -88,6 +89,26 @@ int plasma_desc_triangular_create(plasma_enum_t precision, plasma_enum_t uplo,
     return desc_alloc(A);
 }
 
+int plasma_desc_general_band_create(plasma_enum_t precision, plasma_enum_t uplo,
+                                    int mb, int nb, int lm, int ln,
+                                    int i, int j, int m, int n, int kl, int ku,
+                                    plasma_desc_t *A)
+{
+    if (plasma_context_self() == NULL) {
+        plasma_error("PLASMA not initialized");
+        return PlasmaErrorNotInitialized;
+    }
+    int retval = plasma_desc_general_band_init(precision, uplo, NULL, mb, nb, lm, ln,
+                                               i, j, m, n, kl, ku, A);
+    if (retval != PlasmaSuccess)
+        return retval;
+    if (plasma_desc_check(*A) != PlasmaSuccess) {
+        plasma_error("plasma_desc_check() failed");
+        return PlasmaErrorIllegalValue;
+    }
+    return desc_alloc(A);
+}
+
 int plasma_desc_destroy(plasma_desc_t *A)
 {
     plasma_context_t *plasma = plasma_context_self();
@@ -145,6 +166,38 @@ int plasma_desc_general_init(plasma_enum_t precision, void *matrix,
     return PlasmaSuccess;
 }
 
+/* A general layout whose tile columns hold the band's tiles; the tile-row
+ * counts of the band (reference control/descriptor.c:199-211):
+ * klt = tiles on and below the diagonal, kut = on and above. */
+int plasma_desc_general_band_init(plasma_enum_t precision, plasma_enum_t uplo,
+                                  void *matrix, int mb, int nb, int lm, int ln,
+                                  int i, int j, int m, int n, int kl, int ku,
+                                  plasma_desc_t *A)
+{
+    int retval = plasma_desc_general_init(precision, matrix, mb, nb, lm, ln, i, j, m, n, A);
+    if (retval != PlasmaSuccess)
+        return retval;
+    A->type = PlasmaGeneralBand;
+    A->uplo = uplo;
+    A->kl = kl;
+    A->ku = ku;
+    if (mb <= 0 || nb <= 0)
+        return PlasmaSuccess;
+    if (uplo == PlasmaGeneral) {
+        A->klt = 1 + (i + kl + mb - 1) / mb - i / mb;
+        A->kut = 1 + (i + ku + kl + nb - 1) / nb - i / nb;
+    }
+    else if (uplo == PlasmaUpper) {
+        A->klt = 1;
+        A->kut = 1 + (i + ku + nb - 1) / nb - i / nb;
+    }
+    else {
+        A->klt = 1 + (i + kl + mb - 1) / mb - i / mb;
+        A->kut = 1;
+    }
+    return PlasmaSuccess;
+}
+
 int plasma_desc_triangular_init(plasma_enum_t precision, plasma_enum_t uplo,
                                 void *matrix, int mb, int nb, int lm, int ln,
                                 int i, int j, int m, int n, plasma_desc_t *A)
@@ -182,8 +235,61 @@ int plasma_desc_check(plasma_desc_t A)
     if (A.type == PlasmaGeneral || A.type == PlasmaUpper ||
         A.type == PlasmaLower)
         return plasma_desc_general_check(A);
+    if (A.type == PlasmaGeneralBand)
+        return plasma_desc_general_band_check(A);
     plasma_error("invalid matrix type");
     return PlasmaErrorIllegalValue;
+}
+
+/* The reference's checks (control/descriptor.c:321-369), with the storage
+ * rule the tile addressing relies on stated exactly: gm holds the
+ * kut + klt - 1 tile rows of a band column and is a multiple of mb, and the
+ * view starts on the diagonal (i = j). */
+int plasma_desc_general_band_check(plasma_desc_t A)
+{
+    if (A.precision != PlasmaRealFloat && A.precision != PlasmaRealDouble &&
+        A.precision != PlasmaComplexFloat &&
+        A.precision != PlasmaComplexDouble) {
+        plasma_error("invalid matrix type");
+        return PlasmaErrorIllegalValue;
+    }
+    if (A.uplo != PlasmaGeneral && A.uplo != PlasmaUpper && A.uplo != PlasmaLower) {
+        plasma_error("invalid band uplo");
+        return PlasmaErrorIllegalValue;
+    }
+    if (A.mb <= 0 || A.nb <= 0) {
+        plasma_error("negative tile dimension");
+        return PlasmaErrorIllegalValue;
+    }
+    if (A.m < 0 || A.n < 0 || A.kl < 0 || A.ku < 0) {
+        plasma_error("negative matrix dimension");
+        return PlasmaErrorIllegalValue;
+    }
+    if (A.gn < A.n) {
+        plasma_error("invalid leading column dimensions");
+        return PlasmaErrorIllegalValue;
+    }
+    if (A.gm % A.mb != 0 || A.gm < A.mb * (A.kut + A.klt - 1)) {
+        plasma_error("invalid leading row dimensions");
+        return PlasmaErrorIllegalValue;
+    }
+    if (A.j > 0 && A.j >= A.gn) {
+        plasma_error("beginning of the matrix out of bounds");
+        return PlasmaErrorIllegalValue;
+    }
+    if (A.j + A.n > A.gn) {
+        plasma_error("submatrix out of bounds");
+        return PlasmaErrorIllegalValue;
+    }
+    if (A.i % A.mb != 0 || A.j % A.nb != 0 || A.i != A.j) {
+        plasma_error("submatrix not aligned to a diagonal tile");
+        return PlasmaErrorIllegalValue;
+    }
+    if (A.kl + 1 > A.m || A.ku + 1 > A.n) {
+        plasma_error("band width larger than matrix dimension");
+        return PlasmaErrorIllegalValue;
+    }
+    return PlasmaSuccess;
 }
 
 int plasma_desc_general_check(plasma_desc_t A)

@@ -2,7 +2,8 @@
 // additions and precision conversions.
 //
 // Replaces the per-tile lacpy tasks of the reference's layout converters
-// (compute/pzge2desc.c:38-55, pztr2desc.c:31-50, pzdesc2ge.c, pzdesc2tr.c),
+// (compute/pzge2desc.c:38-55, pztr2desc.c:31-50, pzdesc2ge.c, pzdesc2tr.c,
+// and for band storage pzpb2desc.c, pzdesc2pb.c),
 // pzlacpy.c, pzgeadd.c, pzlag2c.c:47-85 and pclag2z.c:28-67 with one launch
 // per whole-matrix operation: one CTA per tile, threads striding down the
 // rows of a column so that global accesses are coalesced.  All kernels are
@@ -239,6 +240,42 @@ __global__ void k_set_diag(plasma_desc_t A, int i0, int i1, T v)
     t[(size_t)r * plasma_tile_mmain(A, m) + r] = v;
 }
 
+// LAPACK band storage <-> band tile descriptor (the reference's
+// compute/pzpb2desc.c:31-61 and pzdesc2pb.c).  Element (i,j) of the band
+// (view coordinates) sits at pAB[off + i - j + j*ldab], off = ku for upper
+// and 0 for lower storage.  One CTA per stored tile: blockIdx.x walks the
+// kut+klt-1 tiles of band column blockIdx.y.  On the way in every element of
+// the stored tile is written (zero outside the band and below the matrix),
+// so the tile kernels never read stale values; on the way out only band
+// elements are written.
+template <typename T, bool TO_TILE>
+__global__ void __launch_bounds__(kThreads)
+k_band_tile(plasma_desc_t A, T *pAB, int ldab, const plasma_devstat_t *st)
+{
+    if (plasma_failed(st)) return;
+    const int n = blockIdx.y;
+    const int m = n - (A.kut - 1) + (int)blockIdx.x;
+    if (m < 0 || m >= A.mt) return;
+    const bool lower = A.uplo == PlasmaLower;
+    const int off = lower ? 0 : A.ku;
+    const int rows = plasma_tile_mview(A, m);
+    const int cols = plasma_tile_nview(A, n);
+    T *tile = (T *)plasma_tile_addr(A, m, n);
+    const int ldt = plasma_tile_mmain(A, m);
+    const int h = TO_TILE ? A.mb : rows;     // stored rows visited
+    const int d0 = m * A.mb - n * A.nb;      // i - j at the tile's corner
+    for (int e = threadIdx.x; e < h * cols; e += kThreads) {
+        const int r = e % h, c = e / h;
+        const int d = d0 + r - c;
+        const bool in = r < rows && (lower ? (d >= 0 && d <= A.kl) : (d <= 0 && d >= -A.ku));
+        const size_t ab = (size_t)(n * A.nb + c) * ldab + (off + d);
+        if (TO_TILE)
+            tile[(size_t)c * ldt + r] = in ? pAB[ab] : T(0);
+        else if (in)
+            pAB[ab] = tile[(size_t)c * ldt + r];
+    }
+}
+
 dim3 tile_grid(const plasma_desc_t &A)
 {
     return dim3((unsigned)A.mt, (unsigned)A.nt);
@@ -272,6 +309,32 @@ extern "C" void plasma_cuda_tile_to_lapack(cudaStream_t s, plasma_devstat_t *st,
     else
         k_lapack_tile<float, false><<<tile_grid(A), kThreads, 0, s>>>(
             A, uplo, (float *)pA, lda, 0, st);
+}
+
+// Band descriptors of lower or upper storage (A.uplo); the caller checks
+// ldab >= kl+1 (lower) or ku+1 (upper).
+extern "C" void plasma_cuda_band_to_tile(cudaStream_t s, plasma_devstat_t *st,
+                                         plasma_desc_t A, const void *pAB, int ldab)
+{
+    if (A.mt == 0 || A.nt == 0) return;
+    PLASMA_COUNT_LAUNCH();
+    dim3 grid((unsigned)(A.kut + A.klt - 1), (unsigned)A.nt);
+    if (A.precision == PlasmaRealDouble)
+        k_band_tile<double, true><<<grid, kThreads, 0, s>>>(A, (double *)pAB, ldab, st);
+    else
+        k_band_tile<float, true><<<grid, kThreads, 0, s>>>(A, (float *)pAB, ldab, st);
+}
+
+extern "C" void plasma_cuda_tile_to_band(cudaStream_t s, plasma_devstat_t *st,
+                                         plasma_desc_t A, void *pAB, int ldab)
+{
+    if (A.mt == 0 || A.nt == 0) return;
+    PLASMA_COUNT_LAUNCH();
+    dim3 grid((unsigned)(A.kut + A.klt - 1), (unsigned)A.nt);
+    if (A.precision == PlasmaRealDouble)
+        k_band_tile<double, false><<<grid, kThreads, 0, s>>>(A, (double *)pAB, ldab, st);
+    else
+        k_band_tile<float, false><<<grid, kThreads, 0, s>>>(A, (float *)pAB, ldab, st);
 }
 
 extern "C" void plasma_cuda_lacpy(cudaStream_t s, plasma_devstat_t *st,

@@ -101,9 +101,13 @@ k_solve_update(plasma_desc_t A, int uplo, plasma_desc_t B, int k, int mlo,
     }
 }
 
+// kt > 0: A is a band factor whose tile columns hold kt tiles from the
+// diagonal down (logical lower view), so step k only reaches tile rows
+// [k+1, k+kt) forward and [k-kt+1, k) backward (the reference's band solve,
+// compute/pztbsm.c, visits the same tiles).
 template <typename T>
 void sweep(cudaStream_t s, plasma_devstat_t *st, int uplo, int trans,
-           const plasma_desc_t &A, const plasma_desc_t &B, const T *W)
+           const plasma_desc_t &A, const plasma_desc_t &B, const T *W, int kt)
 {
     const int mt = B.mt;
     const int nbw = A.mb;
@@ -129,11 +133,15 @@ void sweep(cudaStream_t s, plasma_devstat_t *st, int uplo, int trans,
             B, k, W, nbw, trans, st);
         int mlo = trans ? 0 : k + 1;
         int mhi = trans ? k : mt;
+        if (kt > 0) {
+            if (trans) mlo = max(0, k - kt + 1);
+            else mhi = min(mt, k + kt);
+        }
         if (gemm && mhi > mlo &&
             plasma_cuda_sweep_update_mma(s, st, uplo, trans, A, B, k, mlo, mhi)) {
             // square tiles, a multiple of 128: the tensor-core sweep update
             // (cuda/update.cu)
-        } else if (gemm && mhi > mlo) {
+        } else if (gemm && mhi > mlo && kt == 0) {
             const int mb = B.mb, kr = plasma_tile_mview(B, k);
             plasma_view_t lv, bv, cv;
             memset(&lv, 0, sizeof(lv));
@@ -183,13 +191,17 @@ extern "C" void plasma_cuda_trsm_sweep(cudaStream_t s, plasma_devstat_t *st,
     if (!have_w)
         plasma_cuda_trtri_tiles(s, st, uplo, A, W);
     int t = trans != PlasmaNoTrans;
+    const int kt = A.type == PlasmaGeneralBand
+                 ? (uplo == PlasmaLower ? A.klt : A.kut) : 0;
     double n = B.m, nrhs = B.n, es = plasma_element_size(A.precision);
     int prof = plasma_prof_begin(s);
     if (A.precision == PlasmaRealDouble)
-        sweep<double>(s, st, uplo, t, A, B, (const double *)W);
+        sweep<double>(s, st, uplo, t, A, B, (const double *)W, kt);
     else
-        sweep<float>(s, st, uplo, t, A, B, (const float *)W);
-    // one triangle of the factor read once, B read and written once
-    plasma_prof_end(prof, s, PLASMA_KCLASS_SOLVE, n * n * nrhs,
-                    es * (n * n / 2.0 + 2.0 * n * nrhs));
+        sweep<float>(s, st, uplo, t, A, B, (const float *)W, kt);
+    // one triangle of the factor (or its band) read once, B read and
+    // written once
+    double w = kt > 0 ? fmin(n, (double)kt * A.mb) : n;
+    plasma_prof_end(prof, s, PLASMA_KCLASS_SOLVE, n * w * nrhs,
+                    es * (n * w / 2.0 + 2.0 * n * nrhs));
 }

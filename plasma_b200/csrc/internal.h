@@ -133,6 +133,12 @@ void plasma_cuda_lapack_to_tile(cudaStream_t s, plasma_devstat_t *st,
 void plasma_cuda_tile_to_lapack(cudaStream_t s, plasma_devstat_t *st,
                                 plasma_desc_t A, plasma_enum_t uplo,
                                 void *pA, int lda);
+/* LAPACK band storage (ldab >= kd+1) <-> band tile descriptor of lower or
+ * upper storage (reference compute/pzpb2desc.c, pzdesc2pb.c). */
+void plasma_cuda_band_to_tile(cudaStream_t s, plasma_devstat_t *st,
+                              plasma_desc_t A, const void *pAB, int ldab);
+void plasma_cuda_tile_to_band(cudaStream_t s, plasma_devstat_t *st,
+                              plasma_desc_t A, void *pAB, int ldab);
 
 /* All diagonal-tile inverses W_k = inv(L_kk) (lower logical view) into W
  * (A.mt tiles of A.mb x A.mb, column-major). */
@@ -341,6 +347,12 @@ void plasma_pXpotrf_arrivals(plasma_context_t *plasma, plasma_enum_t uplo,
 void plasma_pXpotrs(plasma_context_t *plasma, plasma_enum_t uplo,
                     plasma_desc_t A, plasma_desc_t B,
                     plasma_sequence_t *sequence, plasma_request_t *request);
+/* Band Cholesky and the band solves on a band descriptor (compute/pbtrf.c). */
+void plasma_pXpbtrf(plasma_context_t *plasma, plasma_enum_t uplo, plasma_desc_t A,
+                    plasma_sequence_t *sequence, plasma_request_t *request, int call);
+void plasma_pXpbtrs(plasma_context_t *plasma, plasma_enum_t uplo, plasma_desc_t A,
+                    plasma_desc_t B, plasma_sequence_t *sequence, plasma_request_t *request);
+void plasma_tune_trsm(plasma_context_t *plasma, plasma_enum_t dtyp, int m, int n);
 
 #ifdef __cplusplus
 }

@@ -5,7 +5,10 @@ The workloads are the synthetic SPD systems of the benchmark configurations:
     (seed 42 for the CPU parity case n = 2048, seed 7 for n in {8192 .. 32768});
   * prescribed spectrum: A = Q diag(lambda) Q^T, Q from Householder QR of an
     N(0,1) matrix, lambda log-spaced from 1 to 1/kappa (seed 11);
-  * Gaussian likelihood: A = G G^T / n + I (seed 3).
+  * Gaussian likelihood: A = G G^T / n + I (seed 3);
+  * band: the diagonally dominant matrix cut to the band |i - j| <= kd, the
+    reference tester's band inputs (test/test_zpbsv.c:90-106), with its
+    LAPACK band storage.
 numpy's PCG64 streams are stable across numpy versions, so the same seed
 gives the same bytes on every machine.
 """
@@ -53,3 +56,39 @@ def likelihood(n, nrhs, seed=3):
 def probe_vector(n):
     """Fixed vector used for checksums L @ v of large factors."""
     return np.cos(np.arange(n, dtype=np.float64) * 0.37) + 0.5
+
+
+def band(n, kd, nrhs, seed, dtype=np.float64):
+    """Symmetric positive definite band matrix of bandwidth kd: A (full,
+    Fortran order), its LAPACK band storage for lower (AB(i-j, j)) and upper
+    (AB(kd+i-j, j)) triangles, both (kd+1) x n, and B."""
+    a, b = diag_dominant(n, nrhs, seed, dtype)
+    i, j = np.indices((n, n))
+    a = np.asfortranarray(np.where(np.abs(i - j) <= kd, a, 0).astype(dtype))
+    return a, to_band(a, kd, lower=True), to_band(a, kd, lower=False), b
+
+
+def to_band(a, kd, lower, ldab=None):
+    """LAPACK band storage of the lower or upper band of a (ldab x n,
+    Fortran order; rows past kd+1 and the corner positions are zero)."""
+    n = a.shape[0]
+    ldab = kd + 1 if ldab is None else ldab
+    ab = np.zeros((ldab, n), dtype=a.dtype, order="F")
+    for d in range(kd + 1):
+        if lower:
+            ab[d, :n - d] = np.diagonal(a, -d)
+        else:
+            ab[kd - d, d:] = np.diagonal(a, d)
+    return ab
+
+
+def from_band(ab, kd, lower):
+    """The triangle of a band matrix from its LAPACK band storage."""
+    n = ab.shape[1]
+    a = np.zeros((n, n), dtype=ab.dtype)
+    for d in range(kd + 1):
+        if lower:
+            a += np.diag(ab[d, :n - d], -d)
+        else:
+            a += np.diag(ab[kd - d, d:], d)
+    return a

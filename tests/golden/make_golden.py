@@ -81,6 +81,24 @@ def main():
             tri = np.tril if lower else np.triu
             d[f"potri{n}_{tag}_factor"] = tri(c)
             d[f"potri{n}_{tag}_inv"] = tri(inv)
+    # band Cholesky (dpbtrf) and band solve (dpbtrs): the reference tester
+    # test/test_zpbsv.c:167-214 and test_zpbtrf.c:155-214 check the residual
+    # and, on failure, LAPACKE_zpbsv's info
+    # (inputs are rebuilt from gen.band with the same seed)
+    for n, kd in ((7, 2), (64, 10), (100, 33), (130, 0), (96, 95)):
+        a, abl, abu, b = gen.band(n, kd, 2, seed=5000 + n + kd)
+        for lower, tag, ab in ((1, "L", abl), (0, "U", abu)):
+            c, info = lapack.dpbtrf(ab, lower=lower)
+            x, info_x = lapack.dpbtrs(c, b, lower=lower)
+            assert info == 0 and info_x == 0
+            d[f"band{n}_{kd}_{tag}_factor"] = c
+            d[f"band{n}_{kd}_{tag}_X"] = x
+    for n, kd, col in ((100, 9, 41), (300, 40, 0)):
+        a, abl, abu, _ = gen.band(n, kd, 1, seed=6000 + n)
+        a = gen.zerocol(a, col)
+        for lower, tag in ((1, "L"), (0, "U")):
+            _, info = lapack.dpbtrf(gen.to_band(a, kd, lower=bool(lower)), lower=lower)
+            d[f"bandinfo{n}_{kd}_{tag}"] = np.array(info)
     np.savez_compressed(OUT, **d)
     print("wrote", OUT, os.path.getsize(OUT), "bytes")
 

@@ -277,3 +277,110 @@ def test_potri_poinv_argument_codes(hostonly):
         assert fn(pb.PlasmaUpper, 4, None, 3) == -4
         assert fn(pb.PlasmaLower, 0, None, 1) == 0
         assert fn(pb.PlasmaLower, 4, None, 4) == pb.PlasmaErrorEnvironment
+
+
+def test_band_argument_codes(hostonly):
+    """plasma_{d,s}pbtrf: -1 uplo, -2 n, -3 kd, -5 ldab (compute/zpbtrf.c:86-105);
+    pbtrs: -1, -2, kd -4, nrhs -5, ldab -7, ldb -10 (compute/zpbtrs.c:94-118);
+    pbsv: -1, -2, -3, -4, ldab -6, ldb -8 (compute/zpbsv.c:105-129); the
+    quick returns; no device -> Environment."""
+    L = hostonly
+    lo = pb.PlasmaLower
+    for p in ("d", "s"):
+        trf = getattr(L, f"plasma_{p}pbtrf")
+        trs = getattr(L, f"plasma_{p}pbtrs")
+        sv = getattr(L, f"plasma_{p}pbsv")
+        assert trf(0, 8, 2, None, 3) == -1
+        assert trf(lo, -1, 2, None, 3) == -2
+        assert trf(lo, 8, -1, None, 3) == -3
+        assert trf(lo, 8, 2, None, 2) == -5
+        assert trf(lo, 0, 2, None, 3) == 0
+        assert trf(lo, 8, 2, None, 3) == pb.PlasmaErrorEnvironment
+        assert trs(0, 8, 2, 1, None, 3, None, 8) == -1
+        assert trs(lo, -1, 2, 1, None, 3, None, 8) == -2
+        assert trs(lo, 8, -1, 1, None, 3, None, 8) == -4
+        assert trs(lo, 8, 2, -1, None, 3, None, 8) == -5
+        assert trs(lo, 8, 2, 1, None, 2, None, 8) == -7
+        assert trs(lo, 8, 2, 1, None, 3, None, 7) == -10
+        assert trs(lo, 0, 2, 0, None, 3, None, 1) == 0
+        assert sv(0, 8, 2, 1, None, 3, None, 8) == -1
+        assert sv(lo, -1, 2, 1, None, 3, None, 8) == -2
+        assert sv(lo, 8, -1, 1, None, 3, None, 8) == -3
+        assert sv(lo, 8, 2, -1, None, 3, None, 8) == -4
+        assert sv(lo, 8, 2, 1, None, 2, None, 8) == -6
+        assert sv(lo, 8, 2, 1, None, 3, None, 7) == -8
+        assert sv(lo, 8, 2, 0, None, 3, None, 8) == 0
+
+
+def band_desc(L, uplo, n, kd, nb):
+    """The band descriptor the LAPACK-layout band routines build
+    (compute/zpbtrf.c:117-124)."""
+    d = pb.plasma_desc_t()
+    lm = nb * (1 + (kd + nb - 1) // nb)
+    rc = L.plasma_desc_general_band_init(pb.PlasmaRealDouble, uplo, None, nb, nb, lm, n,
+                                         0, 0, n, n, kd, kd, ctypes.byref(d))
+    assert rc == 0
+    return d
+
+
+def band_offset(d, m, n):
+    """plasma_tile_offset of a band descriptor (include/plasma_descriptor.h),
+    restated: the general formula at stored tile row (kut-1) + m - n."""
+    row, col = d.kut - 1 + m - n, n + d.j // d.nb
+    lm1, ln1 = d.gm // d.mb, d.gn // d.nb
+    assert 0 <= row < lm1
+    return d.mb * d.nb * (row + lm1 * col) if col < ln1 else d.A12 + d.mb * (d.gn % d.nb) * row
+
+
+@pytest.mark.parametrize("n,kd,nb", [(1000, 300, 128), (1000, 0, 128), (300, 299, 64),
+                                     (4096, 256, 256), (777, 1, 32)])
+@pytest.mark.parametrize("uplo", [pb.PlasmaLower, pb.PlasmaUpper])
+def test_band_descriptor_covers_the_walk(hostonly, n, kd, nb, uplo):
+    """The band descriptor's tile counts (control/descriptor.c:199-211) and,
+    for every tile the band factorization and solves touch (tile rows
+    [k, k+kt) of column k, the window [k+1, k+kt)^2), a stored location
+    inside the allocation, distinct per tile."""
+    L = hostonly
+    d = band_desc(L, uplo, n, kd, nb)
+    assert d.type == pb.PlasmaGeneralBand and d.uplo == uplo
+    kt = 1 + -(-kd // nb)
+    assert (d.klt, d.kut) == ((kt, 1) if uplo == pb.PlasmaLower else (1, kt))
+    assert L.plasma_desc_check(d) == 0
+    assert L.plasma_desc_general_band_check(d) == 0
+    size = L.plasma_desc_storage_bytes(d) // 8
+    assert size == d.gm * d.gn
+    seen = {}
+    for k in range(d.mt):
+        r = min(d.mt, k + kt)
+        for m in range(k, r):
+            for c in range(k, m + 1):
+                # logical lower tile (m, c) is stored at (m, c) or (c, m)
+                t = (m, c) if uplo == pb.PlasmaLower else (c, m)
+                off = band_offset(d, *t)
+                rows = d.mb
+                cols = nb if t[1] < d.gn // nb else d.gn % nb
+                assert 0 <= off and off + rows * cols <= size, (t, off, size)
+                assert seen.setdefault(off, t) == t
+    # views cut at r tiles keep the stored tiles where they were
+    assert len(seen) == sum(min(kt, d.mt - k) for k in range(d.mt))
+
+
+def test_band_descriptor_check_errors(hostonly):
+    L = hostonly
+    d = band_desc(L, pb.PlasmaLower, 100, 10, 16)
+    assert L.plasma_desc_check(d) == 0
+    # a band wider than the matrix (the reference rejects kd >= n)
+    assert L.plasma_desc_general_band_init(pb.PlasmaRealDouble, pb.PlasmaLower, None, 16,
+                                           16, 32, 10, 0, 0, 10, 10, 10, 10,
+                                           ctypes.byref(d)) == 0
+    assert L.plasma_desc_check(d) == pb.PlasmaErrorIllegalValue
+    # too few stored tile rows for the band
+    assert L.plasma_desc_general_band_init(pb.PlasmaRealDouble, pb.PlasmaLower, None, 16,
+                                           16, 16, 100, 0, 0, 100, 100, 10, 10,
+                                           ctypes.byref(d)) == 0
+    assert L.plasma_desc_check(d) == pb.PlasmaErrorIllegalValue
+    # stored rows not a multiple of the tile height
+    assert L.plasma_desc_general_band_init(pb.PlasmaRealDouble, pb.PlasmaLower, None, 16,
+                                           16, 40, 100, 0, 0, 100, 100, 10, 10,
+                                           ctypes.byref(d)) == 0
+    assert L.plasma_desc_check(d) == pb.PlasmaErrorIllegalValue

@@ -164,3 +164,50 @@ def test_potri_zero_diagonal_info():
     keep = f.copy()
     assert oracle.potri(oracle.LOWER, f) == 18
     np.testing.assert_array_equal(f, keep)
+
+
+BANDS = [(7, 2), (64, 10), (100, 33), (130, 0), (96, 95)]
+
+
+@pytest.mark.parametrize("n,kd", BANDS)
+@pytest.mark.parametrize("tag", ["L", "U"])
+@pytest.mark.parametrize("nb", [4, 16, 32])
+def test_pbtrf_pbtrs_against_lapack(golden, n, kd, tag, nb):
+    """The oracle's band tile Cholesky and band solves against LAPACK dpbtrf
+    and dpbtrs: the factor within 50 eps (relative Frobenius), the reference
+    tester's residual ||B - A X||_inf / (n ||A||_F ||X||_inf) < 50 eps
+    (test/test_zpbsv.c:180-202), and the solution against LAPACK's."""
+    a, abl, abu, b = gen.band(n, kd, 2, seed=5000 + n + kd)
+    lower = tag == "L"
+    ab = np.asfortranarray((abl if lower else abu).copy())
+    uplo = LO if lower else UP
+    assert oracle.pbtrf(uplo, ab, kd, nb) == 0
+    ref = golden[f"band{n}_{kd}_{tag}_factor"]
+    assert np.linalg.norm(ab - ref) / np.linalg.norm(ref) < 50 * EPS
+    x = np.asfortranarray(b.copy())
+    assert oracle.pbtrs(uplo, ab, kd, x, nb) == 0
+    r = np.abs(b - a @ x).max() / (n * np.linalg.norm(a) * np.abs(x).max())
+    assert r < TOL * EPS
+    xr = golden[f"band{n}_{kd}_{tag}_X"]
+    assert np.abs(x - xr).max() / np.abs(xr).max() < 1e3 * EPS
+
+
+@pytest.mark.parametrize("n,kd,col", [(100, 9, 41), (300, 40, 0)])
+@pytest.mark.parametrize("tag", ["L", "U"])
+def test_pbtrf_info_matches_lapack(golden, n, kd, col, tag):
+    """A zeroed row and column: the oracle's info equals LAPACK dpbtrf's and
+    the band array is left as it was (test/test_zpbsv.c:108-114, :207-214)."""
+    a, _, _, _ = gen.band(n, kd, 1, seed=6000 + n)
+    a = gen.zerocol(a, col)
+    lower = tag == "L"
+    ab = gen.to_band(a, kd, lower=lower)
+    keep = ab.copy()
+    info = oracle.pbtrf(LO if lower else UP, ab, kd, 16)
+    assert info == int(golden[f"bandinfo{n}_{kd}_{tag}"]) > 0
+    np.testing.assert_array_equal(ab, keep)
+
+
+def test_band_storage_round_trip():
+    a, abl, abu, _ = gen.band(50, 7, 1, seed=1)
+    np.testing.assert_array_equal(gen.from_band(abl, 7, True), np.tril(a))
+    np.testing.assert_array_equal(gen.from_band(abu, 7, False), np.triu(a))
