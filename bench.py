@@ -50,6 +50,10 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-dposv", action="store_true")
+    p.add_argument("--band-nb", default="0",
+                   help="band workload: comma-separated tile sizes (0 = tuned)")
+    p.add_argument("--band-kd", default="256,1024,4096",
+                   help="band workload: comma-separated bandwidths")
     p.add_argument("--batch-count", type=int, default=4096,
                    help="matrices of the batched workload")
     p.add_argument("--workload", default="dsposv", choices=["dsposv", "adjoint", "batched", "inverse",
@@ -372,30 +376,50 @@ def run_band(args):
     L = pb.lib()
     assert L.plasma_init() == 0
     n, rows = 32768, []
-    for kd in (256, 1024, 4096):
+    for kd in [int(v) for v in args.band_kd.split(",")]:
         g = torch.Generator(device="cuda").manual_seed(9)
         # column-major (kd+1) x n storage = row-major n x (kd+1)
         AB0 = torch.rand(n, kd + 1, generator=g, device="cuda", dtype=torch.float64) - 0.5
         AB0[:, 0] += 2 * kd + 1
-        for d in range(1, kd + 1):
-            AB0[n - d:, d] = 0.0
+        # entry (d, j) of the band storage is A(j+d, j): zero past the matrix
+        corner = (torch.arange(n, device="cuda")[:, None]
+                  + torch.arange(kd + 1, device="cuda")[None, :]) >= n
+        AB0[corner] = 0.0
         b0 = torch.rand(n, generator=g, device="cuda", dtype=torch.float64) * 2 - 1
-        for dt, fn in ((torch.float64, "d"), (torch.float32, "s")):
+        for dt, fn, nb in [(dt, fn, int(v)) for dt, fn in ((torch.float64, "d"),
+                                                          (torch.float32, "s"))
+                           for v in args.band_nb.split(",")]:
+            if nb > 0:
+                L.plasma_set(pb.PlasmaTuning, pb.PlasmaDisabled)
+                L.plasma_set(pb.PlasmaNb, nb)
+            else:
+                L.plasma_set(pb.PlasmaTuning, pb.PlasmaEnabled)
             AB1, b1 = AB0.to(dt), b0.to(dt)
-            times = []
+            times, trf = [], []
             for rep in range(args.warmup + args.steps):
-                AB, x = AB1.clone(), b1.clone()
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                torch.cuda.synchronize()
-                e0.record()
-                rc = getattr(L, f"plasma_{fn}pbsv")(pb.PlasmaLower, n, kd, 1, AB.data_ptr(),
-                                                    kd + 1, x.data_ptr(), n)
-                e1.record()
-                torch.cuda.synchronize()
-                assert rc == 0, rc
-                if rep >= args.warmup:
-                    times.append(e0.elapsed_time(e1))
+                for factor_only in (False, True):
+                    AB, x = AB1.clone(), b1.clone()
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    torch.cuda.synchronize()
+                    e0.record()
+                    if factor_only:
+                        rc = getattr(L, f"plasma_{fn}pbtrf")(pb.PlasmaLower, n, kd,
+                                                             AB.data_ptr(), kd + 1)
+                    else:
+                        rc = getattr(L, f"plasma_{fn}pbsv")(pb.PlasmaLower, n, kd, 1,
+                                                            AB.data_ptr(), kd + 1,
+                                                            x.data_ptr(), n)
+                    e1.record()
+                    torch.cuda.synchronize()
+                    assert rc == 0, rc
+                    if rep >= args.warmup:
+                        (trf if factor_only else times).append(e0.elapsed_time(e1))
+            AB, x = AB1.clone(), b1.clone()
+            assert getattr(L, f"plasma_{fn}pbsv")(pb.PlasmaLower, n, kd, 1, AB.data_ptr(),
+                                                  kd + 1, x.data_ptr(), n) == 0
+            nb_used = ctypes.c_int()
+            L.plasma_get(pb.PlasmaNb, ctypes.byref(nb_used))
             xd = x.double()
             ax = AB0[:, 0] * xd
             for d in range(1, kd + 1):
@@ -405,8 +429,9 @@ def run_band(args):
             res = ((b0 - ax).abs().max() / (n * anorm * xd.abs().max())).item()
             ms = min(times)
             flops = n * (kd * kd + 3.0 * kd) + 4.0 * n * kd
-            rows.append({"routine": f"{fn}pbsv", "n": n, "kd": kd, "ms": ms,
-                         "gflops": flops / ms / 1e6, "tester_residual": res})
+            rows.append({"routine": f"{fn}pbsv", "n": n, "kd": kd, "nb": nb_used.value,
+                         "ms": ms, "pbtrf_ms": min(trf), "gflops": flops / ms / 1e6,
+                         "tester_residual": res})
             del AB, AB1, x
     print(json.dumps({"workload": "band", "metric": "time of the SPD band solve "
                       "(pbsv = pbtrf + pbtrs), device-resident AB, uplo = L, nrhs = 1",

@@ -356,8 +356,6 @@ void plasma_omp_Xlapack2desc(const void *pA, int lda, plasma_desc_t A,
 void plasma_omp_Xdesc2lapack(plasma_desc_t A, void *pA, int lda,
                              plasma_enum_t uplo, plasma_sequence_t *sequence,
                              plasma_request_t *request);
-void plasma_tune_potrf(plasma_context_t *plasma, plasma_enum_t dtyp, int n);
-
 /* The band tile copy of AB in the context's kept slot (the reference
  * allocates it per call with plasma_desc_general_band_create). */
 static int band_desc(plasma_context_t *plasma, plasma_enum_t prec, plasma_enum_t uplo,
@@ -416,12 +414,8 @@ static int Xband(plasma_enum_t prec, int op, plasma_enum_t uplo, int n, int kd, 
         return PlasmaSuccess;
     if (plasma->device < 0)
         return PlasmaErrorEnvironment;
-    if (plasma->tuning) {
-        if (op == OP_TRS)
-            plasma_tune_trsm(plasma, prec, n, n);
-        else
-            plasma_tune_potrf(plasma, prec, n);
-    }
+    if (plasma->tuning)
+        plasma_tune_pbtrf(plasma, prec, n, kd);
 
     plasma_desc_t AB, B;
     int retval = band_desc(plasma, prec, uplo, n, kd, &AB);

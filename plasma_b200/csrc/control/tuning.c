@@ -49,6 +49,22 @@ void plasma_tune_potrf(plasma_context_t *plasma, plasma_enum_t dtyp, int n)
         plasma->nb = nb;
 }
 
+/* Band factorization and solves (the reference's plasma_tune_pbtrf,
+ * control/tuning.c:347-354, pbtrf_nb = 256 in tuning/default.lua:120-122).
+ * Here the band walk is a chain of n/nb dependent tile steps, and what a
+ * step costs grows with nb faster than the step count falls: measured on
+ * B200 at n = 32768, kd in {256, 1024, 4096}, nb = 128 is the fastest in
+ * FP64 at every kd and in FP32 up to kd = 1024; FP32 at kd = 4096 prefers
+ * 256 (its trailing windows are large enough to keep the SMs busy). */
+void plasma_tune_pbtrf(plasma_context_t *plasma, plasma_enum_t dtyp, int n, int kd)
+{
+    (void)n;
+    const char *env = getenv("PLASMA_TUNING_DISABLE");
+    if (env && env[0] == '1')
+        return;
+    plasma->nb = (dtyp == PlasmaRealFloat && kd >= 2048) ? 256 : 128;
+}
+
 void plasma_tune_trsm(plasma_context_t *plasma, plasma_enum_t dtyp, int m,
                       int n)
 {

@@ -20,6 +20,29 @@ namespace {
 constexpr int kCols = 16;        // right-hand sides per CTA
 constexpr int kThreads = 256;
 
+// out(i, 0:kCols) = sum over c in [cb, ce) of row[c] * Ys[c][0:kCols] for a
+// row of the operator that is contiguous in memory, one warp per row: the
+// lanes stride along the row (coalesced) and the partial sums are reduced
+// across the warp; lane 0 ends with the sums.
+template <typename T>
+__device__ __forceinline__ void warp_row(const T *row, int cb, int ce,
+                                         const T (*Ys)[kCols + 1], T (&acc)[kCols])
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int j = 0; j < kCols; j++) acc[j] = T(0);
+    for (int c = cb + lane; c < ce; c += 32) {
+        const T v = row[c];
+#pragma unroll
+        for (int j = 0; j < kCols; j++) acc[j] += v * Ys[c][j];
+    }
+#pragma unroll
+    for (int j = 0; j < kCols; j++)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
+}
+
 // out(k) = op(W_k) * B(k, chunk), op = identity (forward) or transpose.
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
@@ -42,14 +65,28 @@ k_diag_apply(plasma_desc_t B, int k, const T *W, int nbw, int trans,
         Bs[r][c] = b[(size_t)(c0 + c) * ldb + r];
     }
     __syncthreads();
+    if (trans) {
+        // backward: out_i = sum_{c >= i} W(c,i) B(c,:); column i of W_k is
+        // contiguous, so a warp per row
+        for (int i = threadIdx.x >> 5; i < rows; i += kThreads / 32) {
+            T acc[kCols];
+            warp_row(w + (size_t)i * nbw, i, rows, Bs, acc);
+            if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+                for (int j = 0; j < kCols; j++)
+                    if (j < cols) b[(size_t)(c0 + j) * ldb + i] = acc[j];
+            }
+        }
+        return;
+    }
     for (int i = threadIdx.x; i < rows; i += kThreads) {
         T acc[kCols];
 #pragma unroll
         for (int j = 0; j < kCols; j++) acc[j] = T(0);
-        // W_k is lower: forward uses row i (c <= i), backward column i (c >= i)
-        int cb = trans ? i : 0, ce = trans ? rows : i + 1;
-        for (int c = cb; c < ce; c++) {
-            T wv = trans ? w[(size_t)i * nbw + c] : w[(size_t)c * nbw + i];
+        // forward: out_i = sum_{c <= i} W(i,c) B(c,:), W_k lower, coalesced
+        // across the threads' rows
+        for (int c = 0; c <= i; c++) {
+            T wv = w[(size_t)c * nbw + i];
 #pragma unroll
             for (int j = 0; j < kCols; j++) acc[j] += wv * Bs[c][j];
         }
@@ -86,6 +123,20 @@ k_solve_update(plasma_desc_t A, int uplo, plasma_desc_t B, int k, int mlo,
     __syncthreads();
     // forward: L(m,k) (logical lower tile); backward: L(k,m)^T
     TileView<T> L = trans ? tile_view<T>(A, uplo, k, m) : tile_view<T>(A, uplo, m, k);
+    if (trans != L.trans) {
+        // element (i,c) of the operator is L.p[i*ld + c]: rows contiguous,
+        // a warp per row (backward on lower storage, forward on upper)
+        for (int i = threadIdx.x >> 5; i < mr; i += kThreads / 32) {
+            T acc[kCols];
+            warp_row(L.p + (size_t)i * L.ld, 0, kr, Ys, acc);
+            if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+                for (int j = 0; j < kCols; j++)
+                    if (j < cols) b[(size_t)(c0 + j) * ldb + i] -= acc[j];
+            }
+        }
+        return;
+    }
     for (int i = threadIdx.x; i < mr; i += kThreads) {
         T acc[kCols];
 #pragma unroll

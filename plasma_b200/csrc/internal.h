@@ -353,6 +353,7 @@ void plasma_pXpbtrf(plasma_context_t *plasma, plasma_enum_t uplo, plasma_desc_t 
 void plasma_pXpbtrs(plasma_context_t *plasma, plasma_enum_t uplo, plasma_desc_t A,
                     plasma_desc_t B, plasma_sequence_t *sequence, plasma_request_t *request);
 void plasma_tune_trsm(plasma_context_t *plasma, plasma_enum_t dtyp, int m, int n);
+void plasma_tune_pbtrf(plasma_context_t *plasma, plasma_enum_t dtyp, int n, int kd);
 
 #ifdef __cplusplus
 }
