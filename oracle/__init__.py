@@ -33,6 +33,17 @@ def lib():
             getattr(L, f"{p}oracle_pbtrs").argtypes = [ci, ci, ci, ci, vp, ci, vp, ci, ci]
             for f in ("potrf", "potrs", "posv", "potri", "pbtrf", "pbtrs"):
                 getattr(L, f"{p}oracle_{f}").restype = ci
+        for p in ("d", "s"):
+            getattr(L, f"{p}oracle_getrf").argtypes = [ci, vp, ci, vp, ci]
+            getattr(L, f"{p}oracle_getrs").argtypes = [ci, ci, vp, ci, vp, vp, ci]
+            getattr(L, f"{p}oracle_gesv").argtypes = [ci, ci, vp, ci, vp, vp, ci, ci]
+            for f in ("getrf", "getrs", "gesv"):
+                getattr(L, f"{p}oracle_{f}").restype = ci
+        L.oracle_dsgesv.argtypes = [ci, ci, vp, ci, vp, vp, ci, vp, ci,
+                                    ctypes.POINTER(ci), ci]
+        L.oracle_dsgesv.restype = ci
+        L.oracle_dlange_inf.argtypes = [ci, vp, ci]
+        L.oracle_dlange_inf.restype = ctypes.c_double
         L.oracle_dsposv.argtypes = [ci, ci, ci, vp, ci, vp, ci, vp, ci,
                                     ctypes.POINTER(ci), ci]
         L.oracle_dsposv.restype = ci
@@ -99,6 +110,39 @@ def dsposv(uplo, a, b, x, nb):
     info = lib().oracle_dsposv(uplo, n, nrhs, _p(a), a.shape[0], _p(b), b.shape[0],
                                _p(x), x.shape[0], ctypes.byref(it), nb)
     return info, it.value
+
+
+def getrf(a, nb):
+    """In-place LU with partial pivoting of the Fortran-ordered square a;
+    returns (info, ipiv) with LAPACK's 1-based pivots."""
+    import numpy as np
+    n = a.shape[0]
+    ipiv = np.zeros(max(n, 1), dtype=np.int32)
+    info = getattr(lib(), f"{_prefix(a)}oracle_getrf")(n, _p(a), a.shape[0], _p(ipiv), nb)
+    return info, ipiv[:n]
+
+
+def getrs(a, ipiv, b):
+    import numpy as np
+    n, nrhs = b.shape
+    ipiv = np.ascontiguousarray(ipiv, dtype=np.int32)
+    return getattr(lib(), f"{_prefix(a)}oracle_getrs")(n, nrhs, _p(a), a.shape[0],
+                                                       _p(ipiv), _p(b), b.shape[0])
+
+
+def dsgesv(a, b, x, nb):
+    """FP32 LU + FP64 refinement (FP64 LU fallback); returns (info, iter, ipiv)."""
+    import numpy as np
+    n, nrhs = b.shape
+    it = ctypes.c_int(0)
+    ipiv = np.zeros(max(n, 1), dtype=np.int32)
+    info = lib().oracle_dsgesv(n, nrhs, _p(a), a.shape[0], _p(ipiv), _p(b), b.shape[0],
+                               _p(x), x.shape[0], ctypes.byref(it), nb)
+    return info, it.value, ipiv[:n]
+
+
+def lange_inf(a):
+    return lib().oracle_dlange_inf(a.shape[0], _p(a), a.shape[0])
 
 
 def lansy_inf(uplo, a):

@@ -11,6 +11,8 @@
  *                        :43-107 (Left, Upper)
  *   band tile Cholesky   compute/pzpbtrf.c:37-118, and the band solves
  *                        (compute/pztbsm.c) as the tile solve cut to the band
+ *   LU with partial pivoting compute/pzgetrf.c:37-232 (panel kernel
+ *                        core_blas/core_zgetrf.c), the solve of zgetrs.c
  *   the LAPACK/BLAS tile kernels the reference calls through CBLAS/LAPACKE
  *   (core_blas/core_zpotrf.c:54-63, core_ztrsm.c:87-100, core_zsyrk.c,
  *   core_zgemm.c:89-102), written out from the published LAPACK algorithms
@@ -470,6 +472,123 @@ static void P(tiles_to_band)(const P(tiles_t) *T, int uplo, int kd, REAL *AB, in
                 TL(T, m, k)[(size_t)(j - k * nb) * P(tile_rows)(T, m) + (i - m * nb)];
         }
     }
+}
+
+/* ---------------- LU with partial pivoting ------------------------------ */
+
+/* The reference's tile LU (compute/pzgetrf.c:37-232, panel kernel
+ * core_blas/core_zgetrf.c:20-238) on column-major A (n x n, lda): for each
+ * block column of width nb, the panel (all rows from the block's first row
+ * down) is factored column by column -- pivot search over the whole panel
+ * column (the first entry of largest magnitude, as LAPACK's idamax), row
+ * interchange, the column divided by the pivot (multiplied by its reciprocal
+ * when |pivot| < sfmin, core_zgetrf.c:125-145), rank-1 update of the panel's
+ * other columns -- then the columns right of the panel get a unit-lower
+ * solve on the block row and the GEMM update below it.  Interchanges are
+ * applied to whole rows at once; the reference defers those left of the
+ * panel to the end (:196-228), and interchanges move values without
+ * arithmetic, so the factors are the same.  ipiv is 1-based, as LAPACK's.
+ * Returns info = the first zero pivot (1-based); like the reference, whose
+ * failed sequence skips every later task, the factorization stops at the
+ * panel that holds it. */
+static int P(p_getrf)(int n, REAL *A, int lda, int *ipiv, int nb)
+{
+#define GE(i, j) A[(size_t)(j) * lda + (i)]
+    const REAL sfmin = sizeof(REAL) == 4 ? (REAL)FLT_MIN : (REAL)DBL_MIN;
+    for (int k0 = 0; k0 < n; k0 += nb) {
+        const int kb = n - k0 < nb ? n - k0 : nb;
+        for (int j = k0; j < k0 + kb; j++) {
+            int jp = j;
+            REAL best = (REAL)fabs((double)GE(j, j));
+            for (int i = j + 1; i < n; i++) {
+                REAL v = (REAL)fabs((double)GE(i, j));
+                if (v > best) { best = v; jp = i; }
+            }
+            ipiv[j] = jp + 1;
+            if (best == (REAL)0)
+                return j + 1;
+            if (jp != j)
+                for (int c = 0; c < n; c++) {
+                    REAL t = GE(j, c); GE(j, c) = GE(jp, c); GE(jp, c) = t;
+                }
+            const REAL piv = GE(j, j);
+            if ((REAL)fabs((double)piv) >= sfmin) {
+                for (int i = j + 1; i < n; i++) GE(i, j) /= piv;
+            } else {
+                const REAL r = (REAL)1 / piv;
+                for (int i = j + 1; i < n; i++) GE(i, j) *= r;
+            }
+            #pragma omp parallel for schedule(static)
+            for (int c = j + 1; c < k0 + kb; c++) {
+                const REAL u = GE(j, c);
+                for (int i = j + 1; i < n; i++) GE(i, c) -= GE(i, j) * u;
+            }
+        }
+        /* block row: unit-lower solve; below it: GEMM */
+        #pragma omp parallel for schedule(dynamic, 4)
+        for (int c = k0 + kb; c < n; c++) {
+            for (int l = k0; l < k0 + kb; l++) {
+                const REAL u = GE(l, c);
+                for (int i = l + 1; i < k0 + kb; i++) GE(i, c) -= GE(i, l) * u;
+            }
+            for (int l = k0; l < k0 + kb; l++) {
+                const REAL u = GE(l, c);
+                for (int i = k0 + kb; i < n; i++) GE(i, c) -= GE(i, l) * u;
+            }
+        }
+    }
+    return 0;
+#undef GE
+}
+
+/* plasma_getrs (compute/zgetrs.c): the interchanges on B (geswp), then the
+ * unit-lower and the upper solves (pztrsm) */
+static void P(p_getrs)(int n, int nrhs, const REAL *A, int lda, const int *ipiv,
+                       REAL *B, int ldb)
+{
+    #pragma omp parallel for schedule(static)
+    for (int c = 0; c < nrhs; c++) {
+        REAL *b = B + (size_t)c * ldb;
+        for (int j = 0; j < n; j++) {
+            int p = ipiv[j] - 1;
+            if (p != j) { REAL t = b[j]; b[j] = b[p]; b[p] = t; }
+        }
+        for (int l = 0; l < n; l++) {
+            const REAL u = b[l];
+            const REAL *a = A + (size_t)l * lda;
+            for (int i = l + 1; i < n; i++) b[i] -= a[i] * u;
+        }
+        for (int l = n - 1; l >= 0; l--) {
+            const REAL *a = A + (size_t)l * lda;
+            b[l] /= a[l];
+            const REAL u = b[l];
+            for (int i = 0; i < l; i++) b[i] -= a[i] * u;
+        }
+    }
+}
+
+int P(oracle_getrf)(int n, REAL *A, int lda, int *ipiv, int nb)
+{
+    if (n == 0) return 0;
+    return P(p_getrf)(n, A, lda, ipiv, nb);
+}
+
+int P(oracle_getrs)(int n, int nrhs, const REAL *A, int lda, const int *ipiv,
+                    REAL *B, int ldb)
+{
+    if (n == 0 || nrhs == 0) return 0;
+    P(p_getrs)(n, nrhs, A, lda, ipiv, B, ldb);
+    return 0;
+}
+
+int P(oracle_gesv)(int n, int nrhs, REAL *A, int lda, int *ipiv, REAL *B, int ldb,
+                   int nb)
+{
+    if (n == 0 || nrhs == 0) return 0;
+    int info = P(p_getrf)(n, A, lda, ipiv, nb);
+    if (info == 0)
+        P(p_getrs)(n, nrhs, A, lda, ipiv, B, ldb);
+    return info;
 }
 
 /* ---------------- LAPACK-layout entry points ---------------------------- */

@@ -8,7 +8,10 @@ The workloads are the synthetic SPD systems of the benchmark configurations:
   * Gaussian likelihood: A = G G^T / n + I (seed 3);
   * band: the diagonally dominant matrix cut to the band |i - j| <= kd, the
     reference tester's band inputs (test/test_zpbsv.c:90-106), with its
-    LAPACK band storage.
+    LAPACK band storage;
+  * general (LU): A = U[-0.5, 0.5] with no diagonal boost, so that partial
+    pivoting interchanges rows, or U diag(sigma) V^T with sigma log-spaced
+    1 .. 1/kappa (the mixed-precision LU inputs).
 numpy's PCG64 streams are stable across numpy versions, so the same seed
 gives the same bytes on every machine.
 """
@@ -92,3 +95,20 @@ def from_band(ab, kd, lower):
         else:
             a += np.diag(ab[kd - d, d:], d)
     return a
+
+
+def general(n, nrhs, seed, dtype=np.float64):
+    """Nonsymmetric A ~ U[-0.5, 0.5] and B ~ U[-1, 1] (Fortran order)."""
+    rng = np.random.default_rng(seed)
+    a = rng.uniform(-0.5, 0.5, size=(n, n))
+    b = rng.uniform(-1.0, 1.0, size=(n, nrhs))
+    return np.asfortranarray(a.astype(dtype)), np.asfortranarray(b.astype(dtype))
+
+
+def general_spectrum(n, kappa, seed=13):
+    """A = U diag(sigma) V^T with sigma log-spaced 1 .. 1/kappa."""
+    rng = np.random.default_rng(seed)
+    u, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    v, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    sig = np.logspace(0.0, -np.log10(kappa), n)
+    return np.asfortranarray((u * sig) @ v.T)

@@ -99,6 +99,28 @@ def main():
         for lower, tag in ((1, "L"), (0, "U")):
             _, info = lapack.dpbtrf(gen.to_band(a, kd, lower=bool(lower)), lower=lower)
             d[f"bandinfo{n}_{kd}_{tag}"] = np.array(info)
+    # LU with partial pivoting (dgetrf, 1-based pivots), dgesv solutions,
+    # dgetrf's info for a zero column; the reference's getrf tester compares
+    # with LAPACKE_zgetrf (test/test_zgetrf.c:116-138), gesv and dcgesv check
+    # the residual (test_zgesv.c, test_zcgesv.c:133-170)
+    for n in (7, 64, 100, 150):
+        a, b = gen.general(n, 2, seed=9000 + n)
+        lu, piv, info = lapack.dgetrf(a)
+        _, _, x, info_x = lapack.dgesv(a, b)
+        assert info == 0 and info_x == 0
+        d[f"lu{n}_LU"] = lu
+        d[f"lu{n}_ipiv"] = (piv + 1).astype(np.int32)
+        d[f"lu{n}_X"] = x
+    for n, col in ((64, 20), (100, 0)):
+        a, _ = gen.general(n, 1, seed=9100 + n)
+        a[:, col] = 0.0
+        _, _, info = lapack.dgetrf(a)
+        d[f"luinfo{n}_{col}"] = np.array(info)
+    for kappa in (1e2, 1e12):
+        a = gen.general_spectrum(100, kappa)
+        b = np.asfortranarray(np.cos(np.arange(200.0)).reshape(100, 2))
+        _, _, x, info = lapack.dgesv(a, b)
+        d[f"gesv_kappa{kappa:.0e}_X"] = x
     np.savez_compressed(OUT, **d)
     print("wrote", OUT, os.path.getsize(OUT), "bytes")
 

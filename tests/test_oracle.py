@@ -211,3 +211,68 @@ def test_band_storage_round_trip():
     a, abl, abu, _ = gen.band(50, 7, 1, seed=1)
     np.testing.assert_array_equal(gen.from_band(abl, 7, True), np.tril(a))
     np.testing.assert_array_equal(gen.from_band(abu, 7, False), np.triu(a))
+
+
+@pytest.mark.parametrize("n", [7, 64, 100, 150])
+@pytest.mark.parametrize("nb", [1, 16, 32, 256])
+def test_getrf_against_lapack(golden, n, nb):
+    """The oracle's LU with partial pivoting against LAPACK dgetrf: the same
+    pivots, and the reference tester's factor check (test/test_zgetrf.c:
+    116-138), ||LU - LU_lapack||_F / ||A||_F / sqrt(n n) < 50 eps."""
+    a, b = gen.general(n, 2, seed=9000 + n)
+    f = np.asfortranarray(a.copy())
+    info, ipiv = oracle.getrf(f, nb)
+    assert info == 0
+    np.testing.assert_array_equal(ipiv, golden[f"lu{n}_ipiv"])
+    err = np.linalg.norm(f - golden[f"lu{n}_LU"]) / np.linalg.norm(a) / n
+    assert err < TOL * EPS
+    # P A = L U
+    lo = np.tril(f, -1) + np.eye(n)
+    pa = a.copy()
+    for j, p in enumerate(ipiv - 1):
+        pa[[j, p]] = pa[[p, j]]
+    assert np.linalg.norm(pa - lo @ np.triu(f)) / np.linalg.norm(a) < n * EPS * 10
+    # the solve (compute/zgetrs.c) against dgesv, and the tester's residual
+    x = np.asfortranarray(b.copy())
+    assert oracle.getrs(f, ipiv, x) == 0
+    assert solve_residual(a, x, b) < TOL * EPS
+    np.testing.assert_allclose(x, golden[f"lu{n}_X"], rtol=1e-10, atol=1e-12)
+
+
+@pytest.mark.parametrize("n,col", [(64, 20), (100, 0)])
+def test_getrf_info_matches_lapack(golden, n, col):
+    """A zero column: the first zero pivot, as LAPACK dgetrf reports it."""
+    a, _ = gen.general(n, 1, seed=9100 + n)
+    a[:, col] = 0.0
+    info, _ = oracle.getrf(np.asfortranarray(a), 16)
+    assert info == int(golden[f"luinfo{n}_{col}"]) > 0
+
+
+@pytest.mark.parametrize("kappa,iters", [(1e2, (1, 5)), (1e12, (-31, -31))])
+def test_dsgesv_against_lapack(golden, kappa, iters):
+    """FP32 LU + FP64 refinement (compute/zcgesv.c:363-532): converges at
+    kappa = 1e2, falls back to the FP64 LU at kappa = 1e12; the tester's
+    residual (test/test_zcgesv.c:150-170) and the dgesv solution."""
+    n = 100
+    a = gen.general_spectrum(n, kappa)
+    b = np.asfortranarray(np.cos(np.arange(200.0)).reshape(n, 2))
+    x = np.zeros((n, 2), order="F")
+    a0, b0 = a.copy(), b.copy()
+    info, it, _ = oracle.dsgesv(a, b, x, 32)
+    assert info == 0
+    assert iters[0] <= it <= iters[1]
+    np.testing.assert_array_equal(a, a0)
+    np.testing.assert_array_equal(b, b0)
+    assert solve_residual(a, x, b) < TOL * EPS
+    xr = golden[f"gesv_kappa{kappa:.0e}_X"]
+    assert np.abs(x - xr).max() / np.abs(xr).max() < 10 * kappa * n * EPS
+
+
+def test_dsgesv_fp32_overflow_falls_back():
+    n = 50
+    a, b = gen.general(n, 1, seed=77)
+    a = a * 1e39
+    x = np.zeros((n, 1), order="F")
+    info, it, _ = oracle.dsgesv(np.asfortranarray(a), b, x, 16)
+    assert info == 0 and it == -31
+    assert solve_residual(a, x, b) < TOL * EPS
