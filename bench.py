@@ -57,7 +57,7 @@ def parse():
     p.add_argument("--batch-count", type=int, default=4096,
                    help="matrices of the batched workload")
     p.add_argument("--workload", default="dsposv", choices=["dsposv", "adjoint", "batched", "inverse",
-                                                     "band"],
+                                                     "band", "lu"],
                    help="dsposv: the headline; adjoint / batched: the differentiation "
                         "and batched-solve configurations, one JSON line each")
     return p.parse_args()
@@ -441,6 +441,52 @@ def run_band(args):
     return 0
 
 
+def run_lu(args):
+    """plasma_dsgesv (FP32 LU with partial pivoting + FP64 refinement) on a
+    device-resident general A = U[-0.5, 0.5] (seed 9), n = 4096, one
+    right-hand side b ~ U[-1, 1].  GFLOP/s counts LAPACK's dgetrf + dgetrs
+    flops (2n^3/3 + 2n^2); the error is the reference tester's residual
+    ||b - A x||_inf / (n ||A||_inf ||x||_inf)."""
+    import torch
+    import plasma_b200 as pb
+    L = pb.lib()
+    assert L.plasma_init() == 0
+    rows = []
+    for n in (4096,):
+        g = torch.Generator(device="cuda").manual_seed(9)
+        A = torch.rand(n, n, generator=g, device="cuda", dtype=torch.float64) - 0.5
+        b = torch.rand(n, generator=g, device="cuda", dtype=torch.float64) * 2 - 1
+        x = torch.zeros(n, device="cuda", dtype=torch.float64)
+        piv = np.zeros(n, dtype=np.int32)
+        it = ctypes.c_int()
+        times = []
+        for rep in range(args.warmup + args.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            rc = L.plasma_dsgesv(n, 1, A.data_ptr(), n, piv.ctypes.data, b.data_ptr(), n,
+                                 x.data_ptr(), n, ctypes.byref(it))
+            e1.record()
+            torch.cuda.synchronize()
+            assert rc == 0, rc
+            if rep >= args.warmup:
+                times.append(e0.elapsed_time(e1))
+        # A holds the transpose of the column-major matrix: A_cm = A.T
+        r = b - A.T @ x
+        res = (r.abs().max() / (n * A.abs().sum(dim=0).max() * x.abs().max())).item()
+        ms = min(times)
+        rows.append({"routine": "dsgesv", "n": n, "ms": ms, "iter": it.value,
+                     "gflops": (2 * n ** 3 / 3 + 2 * n ** 2) / ms / 1e6,
+                     "tester_residual": res})
+    print(json.dumps({"workload": "lu", "metric": "time of the LU-based mixed-precision "
+                      "solve (dsgesv), device-resident A, nrhs = 1",
+                      "unit": "ms", "steps": args.steps, "warmup": args.warmup,
+                      "results": rows}), flush=True)
+    L.plasma_finalize()
+    return 0
+
+
 def run_batched(args):
     """4096 SPD systems, n uniform in [16, 512] (seed 5), A = G G^T / n + 0.1 I,
     b ~ N(0,1), FP64 and FP32: one batched posv (factor + solve) launch per
@@ -530,6 +576,8 @@ def main():
         return run_inverse(args)
     if args.workload == "band":
         return run_band(args)
+    if args.workload == "lu":
+        return run_lu(args)
     if args.workload == "batched":
         return run_batched(args)
     if args.impl == "reference":

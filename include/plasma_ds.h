@@ -1,7 +1,7 @@
 /*
- * plasma_ds.h -- mixed-precision SPD solver (low-precision factor + FP64
- * iterative refinement), the d/s instance of the reference's zc template
- * include/plasma_zc.h:33-37,66-72.
+ * plasma_ds.h -- mixed-precision solvers (low-precision factor + FP64
+ * iterative refinement): SPD (Cholesky) and general (LU), the d/s instance
+ * of the reference's zc template include/plasma_zc.h:27-37,58-72.
  */
 #ifndef PLASMA_DS_H
 #define PLASMA_DS_H
@@ -38,6 +38,27 @@ void plasma_omp_dsposv(plasma_enum_t uplo,
                        plasma_desc_t A, plasma_desc_t B, plasma_desc_t X,
                        plasma_desc_t As, plasma_desc_t Xs, plasma_desc_t R,
                        double *W, double *Rnorm, double *Xnorm, int *iter,
+                       plasma_sequence_t *sequence, plasma_request_t *request);
+
+/*
+ * reference compute/zcgesv.c:106-271.  Solves A X = B for a general square
+ * A by an FP32 LU with partial pivoting and FP64 iterative refinement; A and
+ * B are not modified, X receives the solution and ipiv (n entries, host
+ * memory) the pivots of the factorization used.  *iter as for dsposv
+ * (-31: the FP64 LU was used).
+ */
+int plasma_dsgesv(int n, int nrhs, double *pA, int lda, int *ipiv,
+                  double *pB, int ldb, double *pX, int ldx, int *iter);
+
+/*
+ * reference compute/zcgesv.c:363-532.  A, B, X, R FP64 and As, Xs FP32
+ * general descriptors of one tiling (device memory); ipiv host memory (n
+ * entries); work may be NULL (the norms live on the device), Rnorm and
+ * Xnorm receive the last columnwise norms when refinement converged.
+ */
+void plasma_omp_dsgesv(plasma_desc_t A, int *ipiv, plasma_desc_t B, plasma_desc_t X,
+                       plasma_desc_t As, plasma_desc_t Xs, plasma_desc_t R,
+                       double *work, double *Rnorm, double *Xnorm, int *iter,
                        plasma_sequence_t *sequence, plasma_request_t *request);
 
 #ifdef __cplusplus

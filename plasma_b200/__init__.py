@@ -183,6 +183,10 @@ _SIGNATURES = [
     ("plasma_omp_sdesc2pb", None, [_DESC, c_void_p, c_int, _SEQ, _REQ]),
     ("plasma_omp_dposv", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
     ("plasma_omp_sposv", None, [c_int, _DESC, _DESC, _SEQ, _REQ]),
+    ("plasma_dsgesv", c_int, [c_int, c_int, c_void_p, c_int, c_void_p, c_void_p, c_int,
+                              c_void_p, c_int, POINTER(c_int)]),
+    ("plasma_omp_dsgesv", None, [_DESC, c_void_p, _DESC, _DESC, _DESC, _DESC, _DESC,
+                                 c_void_p, c_void_p, c_void_p, POINTER(c_int), _SEQ, _REQ]),
     ("plasma_omp_dsposv", None, [c_int, _DESC, _DESC, _DESC, _DESC, _DESC, _DESC,
                                  c_void_p, c_void_p, c_void_p, POINTER(c_int),
                                  _SEQ, _REQ]),

@@ -347,6 +347,23 @@ void plasma_pXpotrf_arrivals(plasma_context_t *plasma, plasma_enum_t uplo,
 void plasma_pXpotrs(plasma_context_t *plasma, plasma_enum_t uplo,
                     plasma_desc_t A, plasma_desc_t B,
                     plasma_sequence_t *sequence, plasma_request_t *request);
+/* LU with partial pivoting (cuda/getrf.cu): the panel of tile column k
+ * (pivots into ipiv, 1-based global rows; a zero pivot records info =
+ * row + 1 and ends the kernel), the interchanges of rows [j0, j1) on columns
+ * [c0, c1), the inverses of the unit-lower and upper parts of diagonal tiles
+ * [k0, k1) (nb x nb each at W + k*nb*nb), ||A||_inf of a general matrix and
+ * the columnwise max |.| of an n x nrhs matrix (device doubles). */
+void plasma_cuda_getrf_panel(cudaStream_t s, plasma_devstat_t *st, int call,
+                             plasma_desc_t A, int k, int *ipiv);
+void plasma_cuda_laswp(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t D,
+                       const int *ipiv, int j0, int j1, int c0, int c1);
+void plasma_cuda_trtri_lu(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t A,
+                          int k0, int k1, void *WL, void *WU);
+void plasma_cuda_lange_inf(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t A,
+                           double *dnorm);
+void plasma_cuda_colmax(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t D,
+                        double *out);
+
 /* Band Cholesky and the band solves on a band descriptor (compute/pbtrf.c). */
 void plasma_pXpbtrf(plasma_context_t *plasma, plasma_enum_t uplo, plasma_desc_t A,
                     plasma_sequence_t *sequence, plasma_request_t *request, int call);

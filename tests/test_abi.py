@@ -384,3 +384,21 @@ def test_band_descriptor_check_errors(hostonly):
                                            16, 40, 100, 0, 0, 100, 100, 10, 10,
                                            ctypes.byref(d)) == 0
     assert L.plasma_desc_check(d) == pb.PlasmaErrorIllegalValue
+
+
+def test_dsgesv_argument_codes(hostonly):
+    """plasma_dsgesv: -1 n, -2 nrhs, -4 lda, -7 ldb, -9 ldx (compute/zcgesv.c:
+    119-138), iter = 0 and success on quick return, no device -> Environment."""
+    L = hostonly
+    it = ctypes.c_int(5)
+    piv = (ctypes.c_int * 8)()
+    assert L.plasma_dsgesv(-1, 1, None, 1, piv, None, 1, None, 1, ctypes.byref(it)) == -1
+    assert L.plasma_dsgesv(8, -1, None, 8, piv, None, 8, None, 8, ctypes.byref(it)) == -2
+    assert L.plasma_dsgesv(8, 1, None, 7, piv, None, 8, None, 8, ctypes.byref(it)) == -4
+    assert L.plasma_dsgesv(8, 1, None, 8, piv, None, 7, None, 8, ctypes.byref(it)) == -7
+    assert L.plasma_dsgesv(8, 1, None, 8, piv, None, 8, None, 7, ctypes.byref(it)) == -9
+    it.value = 5
+    assert L.plasma_dsgesv(8, 0, None, 8, piv, None, 8, None, 8, ctypes.byref(it)) == 0
+    assert it.value == 0
+    assert L.plasma_dsgesv(8, 1, None, 8, piv, None, 8, None, 8,
+                           ctypes.byref(it)) == pb.PlasmaErrorEnvironment
