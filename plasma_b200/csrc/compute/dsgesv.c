@@ -17,7 +17,8 @@
  * first zero pivot of the FP64 factorization.
  *
  * The LU walk (plasma_pXgetrf), per tile column k on the context stream:
- *   PANEL(k)            k_getrf_panel: pivots and multipliers of column k
+ *   PANEL(k)            k_lu_pivot / k_lu_update per column: pivots and
+ *                       multipliers of tile column k
  *   LASWP(k)            the panel's interchanges on the other columns
  *   TRTRI(k)            inverses of the unit-lower and upper diagonal tile
  *   block row           A(k, k+1:) <- inv(L_kk) A(k, k+1:)   (GEMM on views)
@@ -76,6 +77,7 @@ typedef struct {
     plasma_desc_t Wu;      /* ... and of WU                         */
     void *tmp;             /* nb x max(n, nrhs) block row            */
     size_t tmp_cols;
+    void *parts;           /* per-CTA pivot candidates of the panel  */
 } lu_work_t;
 
 static int lu_work(plasma_context_t *plasma, plasma_desc_t A, int ncols, lu_work_t *w)
@@ -85,8 +87,10 @@ static int lu_work(plasma_context_t *plasma, plasma_desc_t A, int ncols, lu_work
     char *buf = (char *)plasma_scratch(plasma, PLASMA_SLOT_WORK, 2 * A.mt * nbsq * es + 256);
     const size_t cols = (size_t)(ncols > A.n ? ncols : A.n);
     void *tmp = plasma_scratch(plasma, PLASMA_SLOT_ADJOINT, (size_t)A.mb * cols * es + 256);
-    if (buf == NULL || tmp == NULL)
+    void *parts = plasma_scratch(plasma, PLASMA_SLOT_MIXED, plasma_cuda_getrf_parts_bytes(A));
+    if (buf == NULL || tmp == NULL || parts == NULL)
         return 0;
+    w->parts = parts;
     w->WL = buf;
     w->WU = buf + A.mt * nbsq * es;
     plasma_desc_general_init(A.precision, w->WL, A.mb, A.mb, A.mb, A.mt * A.mb, 0, 0,
@@ -126,7 +130,7 @@ static void plasma_pXgetrf(plasma_context_t *plasma, plasma_desc_t A, int *dpiv,
     for (int k = 0; k < mt; k++) {
         const int kb = plasma_tile_nview(A, k);
         const int r0 = k * A.mb, c1 = r0 + kb;
-        plasma_cuda_getrf_panel(S, st, call, A, k, dpiv);
+        plasma_cuda_getrf_panel(S, st, call, A, k, dpiv, w->parts);
         plasma_cuda_laswp(S, st, A, dpiv, r0, r0 + kb, 0, r0);
         plasma_cuda_laswp(S, st, A, dpiv, r0, r0 + kb, c1, A.n);
         plasma_cuda_trtri_lu(S, st, A, k, k + 1, w->WL, w->WU);

@@ -7,11 +7,11 @@
 // core_zgetrf.c:20-238) -- then applies the panel's interchanges to the other
 // columns (geswp), solves the block row with the unit-lower diagonal tile
 // (trsm) and updates the trailing matrix (gemm).  Here:
-//   k_getrf_panel   the panel of one tile column in one CTA: the rows of the
-//                   panel are strided over 1024 threads, the pivot is found
-//                   by a warp-shuffle then shared-memory max reduction (the
-//                   first entry of largest magnitude, as LAPACK's idamax),
-//                   and each thread applies the rank-1 update to its rows;
+//   k_lu_pivot,     the panel of one tile column, two launches per column:
+//   k_lu_update     the pivot (the first entry of largest magnitude, as
+//                   LAPACK's idamax) from per-CTA candidates and the row
+//                   interchange in one CTA, then scaling, rank-1 update and
+//                   the next column's candidates with a thread per panel row;
 //   k_laswp         the interchanges of a range of rows applied to a range of
 //                   columns, one thread per column (interchanges of one
 //                   column are sequential, columns are independent);
@@ -28,8 +28,6 @@
 #include <limits.h>
 
 namespace {
-
-constexpr int kPanelThreads = 1024;
 
 template <typename T> __device__ __forceinline__ T tiny();
 template <> __device__ __forceinline__ float tiny<float>() { return FLT_MIN; }
@@ -52,75 +50,111 @@ __device__ __forceinline__ void max_pick(T &v, int &i, T ov, int oi)
     if (ov > v || (ov == v && oi < i)) { v = ov; i = oi; }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kPanelThreads)
-k_getrf_panel(plasma_desc_t A, int k, int *ipiv, plasma_devstat_t *st, int call)
-{
-    __shared__ T s_val[kPanelThreads / 32];
-    __shared__ int s_idx[kPanelThreads / 32];
-    __shared__ int s_piv, s_zero;
-    if (plasma_failed(st)) return;
-    const int r0 = k * A.mb;                       // first row of the panel
-    const int M = A.m - r0;                        // panel rows
-    const int kb = min(plasma_tile_nview(A, k), M);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int nwarps = blockDim.x >> 5;
+// The panel of tile column k, one column j at a time, in two launches:
+//   k_lu_pivot   (one CTA) reduces the per-CTA candidates of column j to the
+//                pivot p (first largest magnitude), records ipiv, records
+//                info on an exact zero pivot, and swaps rows j and p across
+//                the panel's columns;
+//   k_lu_update  (a thread per panel row) scales column j below the pivot,
+//                applies the rank-1 update to the rest of the panel and, in
+//                the same pass, leaves each CTA's candidate for column j+1
+//                (j = -1: only the candidates of column 0).
+// Rows r of the panel count from the first row of tile row k.
+constexpr int kRows = 256;      // panel rows per CTA of k_lu_update
 
-    for (int j = 0; j < kb; j++) {
-        // pivot search down column j from row j
-        T bv = T(-1);
-        int bi = INT_MAX;
-        for (int r = j + tid; r < M; r += blockDim.x)
-            max_pick(bv, bi, (T)fabs(*panel_at<T>(A, k, r, j)), r);
+template <typename T>
+__device__ __forceinline__ void block_best(T &bv, int &bi, T *s_val, int *s_idx)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        max_pick(bv, bi, __shfl_xor_sync(0xffffffffu, bv, o),
+                 __shfl_xor_sync(0xffffffffu, bi, o));
+    if (lane == 0) {
+        s_val[warp] = bv;
+        s_idx[warp] = bi;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        bv = lane < nw ? s_val[lane] : T(-1);
+        bi = lane < nw ? s_idx[lane] : INT_MAX;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1)
             max_pick(bv, bi, __shfl_xor_sync(0xffffffffu, bv, o),
                      __shfl_xor_sync(0xffffffffu, bi, o));
-        if (lane == 0) {
-            s_val[warp] = bv;
-            s_idx[warp] = bi;
-        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRows)
+k_lu_update(plasma_desc_t A, int k, int j, int kb, T *pval, int *pidx,
+            const plasma_devstat_t *st)
+{
+    __shared__ T s_u[512];
+    __shared__ T s_val[kRows / 32];
+    __shared__ int s_idx[kRows / 32];
+    if (plasma_failed(st)) return;
+    const int M = A.m - k * A.mb;
+    const int r = blockIdx.x * kRows + threadIdx.x;
+    const bool mine = r < M && r > j;
+    if (j >= 0) {
+        // the pivot row's remaining entries, shared by the CTA
+        for (int c = j + 1 + (int)threadIdx.x; c < kb; c += kRows)
+            s_u[c - j - 1] = *panel_at<T>(A, k, j, c);
         __syncthreads();
-        if (warp == 0) {
-            bv = lane < nwarps ? s_val[lane] : T(-1);
-            bi = lane < nwarps ? s_idx[lane] : INT_MAX;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1)
-                max_pick(bv, bi, __shfl_xor_sync(0xffffffffu, bv, o),
-                         __shfl_xor_sync(0xffffffffu, bi, o));
-            if (lane == 0) {
-                // a column of NaNs has no larger entry: keep the diagonal one
-                const int p = bi == INT_MAX ? j : bi;
-                s_piv = p;
-                s_zero = *panel_at<T>(A, k, p, j) == T(0);
-                ipiv[r0 + j] = r0 + p + 1;
-                if (s_zero)
-                    plasma_fail(st, r0 + j + 1, call);
-            }
-        }
-        __syncthreads();
-        if (s_zero)
-            return;                                   // the whole CTA leaves
-        const int p = s_piv;
-        if (p != j)
-            for (int c = tid; c < kb; c += blockDim.x) {
-                T *a = panel_at<T>(A, k, j, c), *b = panel_at<T>(A, k, p, c);
-                const T t = *a;
-                *a = *b;
-                *b = t;
-            }
-        __syncthreads();
-        const T piv = *panel_at<T>(A, k, j, j);
-        const bool normal = (T)fabs(piv) >= tiny<T>();
-        const T rpiv = T(1) / piv;
-        for (int r = j + 1 + tid; r < M; r += blockDim.x) {
+        if (mine) {
+            const T piv = *panel_at<T>(A, k, j, j);
             T *lr = panel_at<T>(A, k, r, j);
-            const T l = normal ? *lr / piv : *lr * rpiv;
+            const T l = (T)fabs(piv) >= tiny<T>() ? *lr / piv : *lr * (T(1) / piv);
             *lr = l;
             for (int c = j + 1; c < kb; c++)
-                *panel_at<T>(A, k, r, c) -= l * *panel_at<T>(A, k, j, c);
+                *panel_at<T>(A, k, r, c) -= l * s_u[c - j - 1];
         }
-        __syncthreads();
+    }
+    if (j + 1 >= kb) return;                         // no next column
+    T bv = T(-1);
+    int bi = INT_MAX;
+    if (r < M && r >= j + 1)
+        max_pick(bv, bi, (T)fabs(*panel_at<T>(A, k, r, j + 1)), r);
+    block_best(bv, bi, s_val, s_idx);
+    if (threadIdx.x == 0) {
+        pval[blockIdx.x] = bv;
+        pidx[blockIdx.x] = bi;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRows)
+k_lu_pivot(plasma_desc_t A, int k, int j, int kb, const T *pval, const int *pidx,
+           int nparts, int *ipiv, plasma_devstat_t *st, int call)
+{
+    __shared__ T s_val[kRows / 32];
+    __shared__ int s_idx[kRows / 32];
+    __shared__ int s_piv, s_zero;
+    if (plasma_failed(st)) return;
+    T bv = T(-1);
+    int bi = INT_MAX;
+    for (int q = threadIdx.x; q < nparts; q += kRows)
+        max_pick(bv, bi, pval[q], pidx[q]);
+    block_best(bv, bi, s_val, s_idx);
+    if (threadIdx.x == 0) {
+        // a column of NaNs has no larger entry: keep the diagonal one
+        const int p = bi == INT_MAX ? j : bi;
+        s_piv = p;
+        s_zero = *panel_at<T>(A, k, p, j) == T(0);
+        ipiv[k * A.mb + j] = k * A.mb + p + 1;
+        if (s_zero)
+            plasma_fail(st, k * A.mb + j + 1, call);
+    }
+    __syncthreads();
+    const int p = s_piv;
+    if (s_zero || p == j) return;
+    for (int c = threadIdx.x; c < kb; c += kRows) {
+        T *a = panel_at<T>(A, k, j, c), *b = panel_at<T>(A, k, p, c);
+        const T t = *a;
+        *a = *b;
+        *b = t;
     }
 }
 
@@ -225,18 +259,43 @@ k_colmax(plasma_desc_t D, double *out, const plasma_devstat_t *st)
 
 }  // namespace
 
+// parts: room for ceil((A.m - k*mb) / 256) candidate pairs (values of the
+// precision of A, then ints).
 extern "C" void plasma_cuda_getrf_panel(cudaStream_t s, plasma_devstat_t *st, int call,
-                                        plasma_desc_t A, int k, int *ipiv)
+                                        plasma_desc_t A, int k, int *ipiv, void *parts)
 {
-    PLASMA_COUNT_LAUNCH();
-    const double M = A.m - k * A.mb, kb = plasma_tile_nview(A, k);
+    const int M = A.m - k * A.mb;
+    const int kb = min(plasma_tile_nview(A, k), M);
+    if (kb <= 0) return;
+    const int G = (M + kRows - 1) / kRows;
+    const size_t es = plasma_element_size(A.precision);
+    int *pidx = (int *)((char *)parts + (((size_t)G * es + 15) & ~(size_t)15));
     int prof = plasma_prof_begin(s);
-    if (A.precision == PlasmaRealDouble)
-        k_getrf_panel<double><<<1, kPanelThreads, 0, s>>>(A, k, ipiv, st, call);
-    else
-        k_getrf_panel<float><<<1, kPanelThreads, 0, s>>>(A, k, ipiv, st, call);
-    plasma_prof_end(prof, s, PLASMA_KCLASS_POTRF, M * kb * kb - kb * kb * kb / 3.0,
-                    2.0 * M * kb * plasma_element_size(A.precision));
+    for (int j = -1; j < kb; j++) {
+        if (j >= 0) {
+            PLASMA_COUNT_LAUNCH();
+            if (A.precision == PlasmaRealDouble)
+                k_lu_pivot<double><<<1, kRows, 0, s>>>(A, k, j, kb, (const double *)parts,
+                                                       pidx, G, ipiv, st, call);
+            else
+                k_lu_pivot<float><<<1, kRows, 0, s>>>(A, k, j, kb, (const float *)parts,
+                                                      pidx, G, ipiv, st, call);
+        }
+        PLASMA_COUNT_LAUNCH();
+        if (A.precision == PlasmaRealDouble)
+            k_lu_update<double><<<G, kRows, 0, s>>>(A, k, j, kb, (double *)parts, pidx, st);
+        else
+            k_lu_update<float><<<G, kRows, 0, s>>>(A, k, j, kb, (float *)parts, pidx, st);
+    }
+    plasma_prof_end(prof, s, PLASMA_KCLASS_POTRF,
+                    (double)M * kb * kb - (double)kb * kb * kb / 3.0,
+                    2.0 * (double)M * kb * es);
+}
+
+extern "C" size_t plasma_cuda_getrf_parts_bytes(plasma_desc_t A)
+{
+    const size_t G = (size_t)(A.m + kRows - 1) / kRows;
+    return ((G * 8 + 15) & ~(size_t)15) + G * sizeof(int) + 64;
 }
 
 extern "C" void plasma_cuda_laswp(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t D,

@@ -349,12 +349,14 @@ void plasma_pXpotrs(plasma_context_t *plasma, plasma_enum_t uplo,
                     plasma_sequence_t *sequence, plasma_request_t *request);
 /* LU with partial pivoting (cuda/getrf.cu): the panel of tile column k
  * (pivots into ipiv, 1-based global rows; a zero pivot records info =
- * row + 1 and ends the kernel), the interchanges of rows [j0, j1) on columns
+ * row + 1 and ends the walk; two launches per column), the interchanges of rows [j0, j1) on columns
  * [c0, c1), the inverses of the unit-lower and upper parts of diagonal tiles
  * [k0, k1) (nb x nb each at W + k*nb*nb), ||A||_inf of a general matrix and
  * the columnwise max |.| of an n x nrhs matrix (device doubles). */
 void plasma_cuda_getrf_panel(cudaStream_t s, plasma_devstat_t *st, int call,
-                             plasma_desc_t A, int k, int *ipiv);
+                             plasma_desc_t A, int k, int *ipiv, void *parts);
+/* bytes of the `parts` workspace of plasma_cuda_getrf_panel for A */
+size_t plasma_cuda_getrf_parts_bytes(plasma_desc_t A);
 void plasma_cuda_laswp(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t D,
                        const int *ipiv, int j0, int j1, int c0, int c1);
 void plasma_cuda_trtri_lu(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t A,
