@@ -56,11 +56,13 @@ __device__ __forceinline__ void max_pick(T &v, int &i, T ov, int oi)
 //                info on an exact zero pivot, and swaps rows j and p across
 //                the panel's columns;
 //   k_lu_update  (a thread per panel row) scales column j below the pivot,
-//                applies the rank-1 update to the rest of the panel and, in
-//                the same pass, leaves each CTA's candidate for column j+1
-//                (j = -1: only the candidates of column 0).
+//                applies the rank-1 update to the rest of its sub-block of
+//                kIB columns and, in the same pass, leaves each CTA's
+//                candidate for the next column (j = -1: candidates only);
+//   k_lu_trsm_block  the sub-block's rows of the panel's later columns.
 // Rows r of the panel count from the first row of tile row k.
 constexpr int kRows = 256;      // panel rows per CTA of k_lu_update
+constexpr int kIB = 32;         // columns of a panel sub-block
 
 template <typename T>
 __device__ __forceinline__ void block_best(T &bv, int &bi, T *s_val, int *s_idx)
@@ -88,39 +90,57 @@ __device__ __forceinline__ void block_best(T &bv, int &bi, T *s_val, int *s_idx)
 
 template <typename T>
 __global__ void __launch_bounds__(kRows)
-k_lu_update(plasma_desc_t A, int k, int j, int kb, T *pval, int *pidx,
+k_lu_update(plasma_desc_t A, int k, int j, int ce, int next, T *pval, int *pidx,
             const plasma_devstat_t *st)
 {
-    __shared__ T s_u[512];
+    __shared__ T s_u[kIB];
     __shared__ T s_val[kRows / 32];
     __shared__ int s_idx[kRows / 32];
     if (plasma_failed(st)) return;
     const int M = A.m - k * A.mb;
     const int r = blockIdx.x * kRows + threadIdx.x;
-    const bool mine = r < M && r > j;
     if (j >= 0) {
-        // the pivot row's remaining entries, shared by the CTA
-        for (int c = j + 1 + (int)threadIdx.x; c < kb; c += kRows)
+        // the pivot row's entries in the rest of the sub-block (ce - j - 1
+        // < kIB of them), shared by the CTA
+        for (int c = j + 1 + (int)threadIdx.x; c < ce; c += kRows)
             s_u[c - j - 1] = *panel_at<T>(A, k, j, c);
         __syncthreads();
-        if (mine) {
+        if (r < M && r > j) {
             const T piv = *panel_at<T>(A, k, j, j);
             T *lr = panel_at<T>(A, k, r, j);
             const T l = (T)fabs(piv) >= tiny<T>() ? *lr / piv : *lr * (T(1) / piv);
             *lr = l;
-            for (int c = j + 1; c < kb; c++)
+            for (int c = j + 1; c < ce; c++)
                 *panel_at<T>(A, k, r, c) -= l * s_u[c - j - 1];
         }
     }
-    if (j + 1 >= kb) return;                         // no next column
+    if (next < 0) return;                            // no candidates wanted
     T bv = T(-1);
     int bi = INT_MAX;
-    if (r < M && r >= j + 1)
-        max_pick(bv, bi, (T)fabs(*panel_at<T>(A, k, r, j + 1)), r);
+    if (r < M && r >= next)
+        max_pick(bv, bi, (T)fabs(*panel_at<T>(A, k, r, next)), r);
     block_best(bv, bi, s_val, s_idx);
     if (threadIdx.x == 0) {
         pval[blockIdx.x] = bv;
         pidx[blockIdx.x] = bi;
+    }
+}
+
+// The rows [s0, ce) of the panel right of the sub-block, columns [ce, kb):
+// U12 <- inv(L11) U12 with L11 the unit-lower sub-block diagonal, a thread per
+// column (forward substitution down ce - s0 <= kIB rows).
+template <typename T>
+__global__ void __launch_bounds__(kRows)
+k_lu_trsm_block(plasma_desc_t A, int k, int s0, int ce, int kb, const plasma_devstat_t *st)
+{
+    if (plasma_failed(st)) return;
+    const int c = ce + blockIdx.x * kRows + threadIdx.x;
+    if (c >= kb) return;
+    for (int i = s0 + 1; i < ce; i++) {
+        T s = *panel_at<T>(A, k, i, c);
+        for (int l = s0; l < i; l++)
+            s -= *panel_at<T>(A, k, i, l) * *panel_at<T>(A, k, l, c);
+        *panel_at<T>(A, k, i, c) = s;
     }
 }
 
@@ -261,6 +281,12 @@ k_colmax(plasma_desc_t D, double *out, const plasma_devstat_t *st)
 
 // parts: room for ceil((A.m - k*mb) / 256) candidate pairs (values of the
 // precision of A, then ints).
+// The panel in sub-blocks of kIB columns (the blocked right-looking order of
+// LAPACK's dgetrf applied inside the panel): each column's rank-1 update
+// stops at the end of its sub-block; after the sub-block, its rows of the
+// panel's remaining columns are solved with the sub-block's unit-lower
+// diagonal and the rows below take one GEMM update.  Interchanges always
+// swap whole panel rows.
 extern "C" void plasma_cuda_getrf_panel(cudaStream_t s, plasma_devstat_t *st, int call,
                                         plasma_desc_t A, int k, int *ipiv, void *parts)
 {
@@ -270,22 +296,48 @@ extern "C" void plasma_cuda_getrf_panel(cudaStream_t s, plasma_devstat_t *st, in
     const int G = (M + kRows - 1) / kRows;
     const size_t es = plasma_element_size(A.precision);
     int *pidx = (int *)((char *)parts + (((size_t)G * es + 15) & ~(size_t)15));
+    const bool dp = A.precision == PlasmaRealDouble;
+    auto update = [&](int j, int ce, int next) {
+        PLASMA_COUNT_LAUNCH();
+        if (dp)
+            k_lu_update<double><<<G, kRows, 0, s>>>(A, k, j, ce, next, (double *)parts, pidx,
+                                                    st);
+        else
+            k_lu_update<float><<<G, kRows, 0, s>>>(A, k, j, ce, next, (float *)parts, pidx,
+                                                   st);
+    };
     int prof = plasma_prof_begin(s);
-    for (int j = -1; j < kb; j++) {
-        if (j >= 0) {
+    const int d0 = k * A.mb;                     // first row and column of the panel
+    for (int s0 = 0; s0 < kb; s0 += kIB) {
+        const int ce = min(kb, s0 + kIB);
+        update(-1, ce, s0);                      // candidates of column s0
+        for (int j = s0; j < ce; j++) {
             PLASMA_COUNT_LAUNCH();
-            if (A.precision == PlasmaRealDouble)
+            if (dp)
                 k_lu_pivot<double><<<1, kRows, 0, s>>>(A, k, j, kb, (const double *)parts,
                                                        pidx, G, ipiv, st, call);
             else
                 k_lu_pivot<float><<<1, kRows, 0, s>>>(A, k, j, kb, (const float *)parts,
                                                       pidx, G, ipiv, st, call);
+            update(j, ce, j + 1 < ce ? j + 1 : -1);
         }
-        PLASMA_COUNT_LAUNCH();
-        if (A.precision == PlasmaRealDouble)
-            k_lu_update<double><<<G, kRows, 0, s>>>(A, k, j, kb, (double *)parts, pidx, st);
-        else
-            k_lu_update<float><<<G, kRows, 0, s>>>(A, k, j, kb, (float *)parts, pidx, st);
+        if (ce < kb) {
+            PLASMA_COUNT_LAUNCH();
+            const unsigned g = (unsigned)((kb - ce + kRows - 1) / kRows);
+            if (dp)
+                k_lu_trsm_block<double><<<g, kRows, 0, s>>>(A, k, s0, ce, kb, st);
+            else
+                k_lu_trsm_block<float><<<g, kRows, 0, s>>>(A, k, s0, ce, kb, st);
+            if (ce < M) {
+                plasma_view_t a{}, b{}, c{};
+                a.D = b.D = c.D = A;
+                a.r0 = d0 + ce;  a.c0 = d0 + s0;         // L21
+                b.r0 = d0 + s0;  b.c0 = d0 + ce;         // U12
+                c.r0 = d0 + ce;  c.c0 = d0 + ce;         // A22
+                plasma_cuda_gemm_view(s, st, M - ce, kb - ce, ce - s0, -1.0, a, b, 1.0, c, 0,
+                                      0);
+            }
+        }
     }
     plasma_prof_end(prof, s, PLASMA_KCLASS_POTRF,
                     (double)M * kb * kb - (double)kb * kb * kb / 3.0,
