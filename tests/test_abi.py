@@ -402,3 +402,76 @@ def test_dsgesv_argument_codes(hostonly):
     assert it.value == 0
     assert L.plasma_dsgesv(8, 1, None, 8, piv, None, 8, None, 8,
                            ctypes.byref(it)) == pb.PlasmaErrorEnvironment
+
+
+def _general(L, prec, m, n, nb=16):
+    d = pb.plasma_desc_t()
+    assert L.plasma_desc_general_init(prec, None, nb, nb, m, n, 0, 0, m, n,
+                                      ctypes.byref(d)) == 0
+    return d
+
+
+def test_omp_dsgesv_descriptor_checks(hostonly):
+    """plasma_omp_dsgesv refuses descriptors of the wrong precision, shape or
+    tiling before touching the device (IllegalValue in the sequence)."""
+    L = hostonly
+    D, S = pb.PlasmaRealDouble, pb.PlasmaRealFloat
+    n, nrhs = 40, 2
+    ok = dict(A=_general(L, D, n, n), B=_general(L, D, n, nrhs), X=_general(L, D, n, nrhs),
+              As=_general(L, S, n, n), Xs=_general(L, S, n, nrhs), R=_general(L, D, n, nrhs))
+    bad = [("As", _general(L, D, n, n)),            # FP64 where FP32 is expected
+           ("X", _general(L, D, n, nrhs + 1)),      # X wider than B
+           ("A", _general(L, D, n, n - 1)),         # A not square
+           ("R", _general(L, D, n, nrhs, nb=8))]    # another tiling
+    piv = (ctypes.c_int * n)()
+    for name, d in bad:
+        args = dict(ok)
+        args[name] = d
+        seq, req = pb.new_sequence()
+        it = ctypes.c_int(7)
+        L.plasma_omp_dsgesv(args["A"], piv, args["B"], args["X"], args["As"], args["Xs"],
+                            args["R"], None, None, None, ctypes.byref(it), ctypes.byref(seq),
+                            ctypes.byref(req))
+        assert seq.status == pb.PlasmaErrorIllegalValue, name
+        assert it.value == 0
+    # well-formed descriptors reach the device check
+    seq, req = pb.new_sequence()
+    it = ctypes.c_int(7)
+    L.plasma_omp_dsgesv(ok["A"], piv, ok["B"], ok["X"], ok["As"], ok["Xs"], ok["R"], None,
+                        None, None, ctypes.byref(it), ctypes.byref(seq), ctypes.byref(req))
+    assert seq.status == pb.PlasmaErrorEnvironment
+
+
+def test_omp_band_descriptor_checks(hostonly):
+    """The async band routines take band descriptors of the uplo triangle (or
+    general band storage) only; the layout converters refuse general band
+    storage and a too small ldab."""
+    L = hostonly
+    lo, up = pb.PlasmaLower, pb.PlasmaUpper
+    ab = band_desc(L, lo, 100, 10, 16)
+    ge = _general(L, pb.PlasmaRealDouble, 100, 100)
+    for fn, args in (("plasma_omp_dpbtrf", (up, ab)), ("plasma_omp_dpbtrf", (lo, ge)),
+                     ("plasma_omp_dpbsv", (up, ab, ge)), ("plasma_omp_dpbtrs", (lo, ge, ge))):
+        seq, req = pb.new_sequence()
+        getattr(L, fn)(*args, ctypes.byref(seq), ctypes.byref(req))
+        assert seq.status == pb.PlasmaErrorIllegalValue, (fn, args)
+    # the matching triangle gets as far as the device check
+    seq, req = pb.new_sequence()
+    L.plasma_omp_dpbtrf(lo, ab, ctypes.byref(seq), ctypes.byref(req))
+    assert seq.status == pb.PlasmaErrorEnvironment
+    buf = np.zeros((11, 100), order="F")
+    seq, req = pb.new_sequence()
+    L.plasma_omp_dpb2desc(buf.ctypes.data, 10, ab, ctypes.byref(seq), ctypes.byref(req))
+    assert seq.status == pb.PlasmaErrorIllegalValue              # ldab < kd + 1
+    gband = pb.plasma_desc_t()
+    assert L.plasma_desc_general_band_init(pb.PlasmaRealDouble, pb.PlasmaGeneral, None, 16, 16,
+                                           64, 100, 0, 0, 100, 100, 10, 10,
+                                           ctypes.byref(gband)) == 0
+    seq, req = pb.new_sequence()
+    L.plasma_omp_dpb2desc(buf.ctypes.data, 11, gband, ctypes.byref(seq), ctypes.byref(req))
+    assert seq.status == pb.PlasmaErrorNotSupported
+    # band storage cannot be allocated without a device
+    d = pb.plasma_desc_t()
+    assert L.plasma_desc_general_band_create(pb.PlasmaRealDouble, lo, 16, 16, 32, 100, 0, 0,
+                                             100, 100, 10, 10,
+                                             ctypes.byref(d)) == pb.PlasmaErrorEnvironment
