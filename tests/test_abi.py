@@ -22,9 +22,13 @@ import plasma_b200 as pb
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def declared_functions():
+def declared_functions(headers=None):
     names = set()
-    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+    if headers is None:
+        # plasma_core_blas.h belongs to libplasma_core_blas.so
+        headers = [h for h in glob.glob(os.path.join(ROOT, "include", "*.h"))
+                   if not h.endswith("plasma_core_blas.h")]
+    for h in headers:
         src = open(h).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
         for m in re.finditer(r"\b(plasma_\w+)\s*\(", src):
