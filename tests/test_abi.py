@@ -13,6 +13,7 @@ import ctypes
 import glob
 import os
 import re
+import subprocess
 
 import numpy as np
 import pytest
@@ -479,3 +480,57 @@ def test_omp_band_descriptor_checks(hostonly):
     assert L.plasma_desc_general_band_create(pb.PlasmaRealDouble, lo, 16, 16, 32, 100, 0, 0,
                                              100, 100, 10, 10,
                                              ctypes.byref(d)) == pb.PlasmaErrorEnvironment
+
+
+C_CALLER = r"""
+#include "plasma.h"
+#include <stdio.h>
+#include <stdlib.h>
+
+int main(void)
+{
+    /* the reference's calling sequence, host-only (no device): argument
+     * codes come back before any device work */
+    if (plasma_init() != 0) return 10;
+    double A[16] = {4, 1, 0, 0, 1, 4, 1, 0, 0, 1, 4, 1, 0, 0, 1, 4};
+    double B[4] = {1, 2, 3, 4}, X[4];
+    int iter = 5, ipiv[4];
+    int rc = 0;
+    rc |= plasma_dposv(999, 4, 1, A, 4, B, 4) != -1;
+    rc |= plasma_dpotrf(PlasmaLower, 4, A, 3) != -4;
+    rc |= plasma_dsposv(PlasmaLower, 4, 1, A, 4, B, 4, X, 3, &iter) != -9;
+    rc |= plasma_dsgesv(4, 1, A, 4, ipiv, B, 4, X, 4, &iter) != PlasmaErrorEnvironment;
+    rc |= plasma_dpbsv(PlasmaLower, 4, 1, 1, A, 1, B, 4) != -6;
+    plasma_desc_t D;
+    rc |= plasma_desc_general_init(PlasmaRealDouble, NULL, 2, 2, 4, 4, 0, 0, 4, 4, &D) != 0;
+    rc |= plasma_desc_check(D) != 0;
+    rc |= plasma_finalize() != 0;
+    printf("%s\n", rc ? "FAIL" : "ok");
+    return rc;
+}
+"""
+
+
+@pytest.mark.parametrize("compiler,ext", [("gcc", "c"), ("g++", "cpp")])
+def test_c_and_cxx_callers_compile_link_and_run(tmp_path, compiler, ext):
+    """A caller written against plasma.h compiles as C and as C++, links with
+    -lplasma_b200 (the INTEGRATION recipe) and gets the reference's argument
+    codes back (host-only mode, no device)."""
+    import shutil
+    if shutil.which(compiler) is None:
+        pytest.skip(f"{compiler} not available")
+    pb.lib()                      # the library is built
+    src = tmp_path / f"caller.{ext}"
+    src.write_text(C_CALLER)
+    exe = tmp_path / "caller"
+    libdir = os.path.join(ROOT, "plasma_b200")
+    cmd = [compiler, str(src), "-I", os.path.join(ROOT, "include"), "-L", libdir,
+           "-lplasma_b200", f"-Wl,-rpath,{libdir}", "-o", str(exe)]
+    if ext == "c":
+        cmd[1:1] = ["-std=c99", "-Wall", "-Werror"]
+    else:
+        cmd[1:1] = ["-Wall", "-Werror"]
+    subprocess.run(cmd, check=True)
+    env = dict(os.environ, PLASMA_ALLOW_NO_DEVICE="1")
+    out = subprocess.run([str(exe)], env=env, capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0 and out.stdout.strip() == "ok", (out.stdout, out.stderr)
