@@ -13,9 +13,12 @@ e2e        : the same, through plasma_dsposv with HOST buffers (H2D of A and
              b and D2H of x inside the timed region).
 roofline   : the dominant kernel (trailing update) of the timed region, timed
              by the library's own CUDA events on its launch stream.
-cpu_baseline / --impl reference : the CPU oracle (a C restatement of the
-             reference's tile algorithms, OpenMP tasks on all host cores) on
-             a bounded sample of the same workload (n = 8192).
+cpu_baseline / --impl reference : the reference PLASMA itself, built from
+             its sources into oracle/_ref (oracle/build_ref.sh) with
+             OpenBLAS 0.3.15 single-threaded and its OpenMP tasks on all host
+             cores, on the same n = 32768 system: one solve for
+             cpu_baseline, one solve per step for the reference arm, which
+             prints the same metric on the same workload.
 Multi-GPU: the path does not shard (one matrix per GPU); N GPUs run N
 independent replicas, timed as the max over ranks.
 """
@@ -46,7 +49,6 @@ def parse():
     p.add_argument("--mode", default="fp32", choices=["fp32", "tf32", "bf16", "auto"])
     p.add_argument("--refine", default="ir", choices=["ir", "gmres", "auto"])
     p.add_argument("--nb", type=int, default=0, help="0 = autotuned table")
-    p.add_argument("--cpu-n", type=int, default=8192)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-dposv", action="store_true")
@@ -63,6 +65,9 @@ def parse():
     return p.parse_args()
 
 
+# the benchmark's metric, printed verbatim by both arms
+METRIC = ("dsposv vs dposv time-to-FP64-backward-err at n=32768 on 1 B200; "
+          "GFLOP/s, % roofline")
 MODES = {"fp32": 0, "tf32": 1, "bf16": 2, "auto": 3}
 UPDATE_DRAM_BYTES_PER_TILE = {"fp32": 384465}
 REFINE = {"ir": 0, "gmres": 1, "auto": 2}
@@ -73,6 +78,15 @@ def dist_info():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return rank, world, local
+
+
+def workload_config(args, nb):
+    return {"workload": f"dsposv n={args.n} nrhs={args.nrhs} A=Q diag(lambda) Q^T "
+                        f"kappa={args.kappa:g} seed 11, b = A x_true (seed 12), uplo=L",
+            "factor": args.mode, "refinement": args.refine, "nb": nb,
+            "l2": f"inputs larger than L2 (A is {args.n * args.n * 8 / 1e9:.1f} GB)"
+                  if args.n * args.n * 8 > 126e6 else "A smaller than L2",
+            "parallelism": "replicas x1"}
 
 
 def flops_of(n, nrhs):
@@ -94,7 +108,8 @@ def make_system(n, nrhs, kappa, device, seed=11):
     g2 = torch.Generator(device=device).manual_seed(seed + 1)
     xt = torch.randn(nrhs, n, generator=g2, device=device, dtype=torch.float64)
     B = (A @ xt.T).T.contiguous()          # nrhs x n row-major = n x nrhs col-major
-    torch.cuda.synchronize()
+    if A.is_cuda:
+        torch.cuda.synchronize()
     return A.contiguous(), B, xt
 
 
@@ -187,30 +202,49 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(mhz)}
 
 
-def cpu_baseline(n, nrhs, kappa, threads=None):
-    """Oracle dsposv on the host cores on a bounded sample (n x n)."""
-    import oracle
-    import torch
-    if threads:
-        oracle.set_threads(threads)
-    dev = "cuda" if torch.cuda.is_available() else "cpu"
-    A, B, _ = make_system(n, nrhs, kappa, dev) if dev == "cuda" else (None, None, None)
-    if A is None:
-        import gen
-        a = gen.spectrum(n, kappa)
-        b = a @ np.random.default_rng(12).standard_normal((n, nrhs))
-    else:
-        a = np.asfortranarray(A.cpu().numpy())
-        b = np.asfortranarray(B.cpu().numpy().T)
-        del A, B
-    x = np.zeros((n, nrhs), order="F")
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def host_system(A, B):
+    """Column-major host copies of the device system (A symmetric, so its
+    row-major bytes are its column-major ones; B is nrhs x n row-major)."""
+    a = np.asfortranarray(A.cpu().numpy())
+    b = np.asfortranarray(B.cpu().numpy().T)
+    return a, b
+
+
+def reference_dsposv(a, b, nb, threads):
+    """One plasma_dsposv of the reference PLASMA itself (oracle/_ref: its own
+    sources, OpenBLAS 0.3.15 single-threaded, OpenMP tasks on `threads`
+    host cores) on host arrays; returns (seconds, info, iter)."""
+    from oracle import ref
+    ref.set_threads(threads)
+    x = np.zeros_like(b, order="F")
     t0 = time.perf_counter()
-    info, it = oracle.dsposv(oracle.LOWER, a, b, x, 256)
-    dt = time.perf_counter() - t0
+    info, it = ref.dsposv(ref.LOWER, a, b, x, nb)
+    return time.perf_counter() - t0, info, it
+
+
+def cpu_baseline(a, b, nb=256):
+    """The reference PLASMA on the host cores on one solve of the same
+    workload (the bounded sample: one dsposv of the benchmark's own system)."""
+    threads = os.cpu_count() or 1
+    n, nrhs = b.shape
+    dt, info, it = reference_dsposv(a, b, nb, threads)
     return {"value": flops_of(n, nrhs) / dt / 1e9, "unit": "GFLOP/s",
-            "cores": oracle.get_threads(), "kind": "port",
-            "sample": f"oracle dsposv n={n} nrhs={nrhs} kappa={kappa:g} nb=256, one solve "
-                      f"({dt:.2f} s, iter {it}, info {info})",
+            "cores": threads, "kind": "reference",
+            "sample": f"reference PLASMA plasma_dsposv (oracle/_ref, OpenBLAS 0.3.15 "
+                      f"single-threaded, {threads} OpenMP threads on {cpu_model()}), one solve "
+                      f"of the same n={n} nrhs={nrhs} system, nb={nb}: {dt:.2f} s, "
+                      f"iter {it}, info {info}",
             "seconds": dt}
 
 
@@ -227,29 +261,49 @@ def max_over_ranks(ms, world, device):
 
 
 def run_reference(args):
+    """The reference arm: the reference PLASMA's own plasma_dsposv (built
+    from its sources into oracle/_ref) on the same n = 32768 system, all
+    host cores, OpenBLAS single-threaded; one step = one solve.  The system
+    is generated on the GPU (the same generator as the GPU arm) and copied
+    to host memory before the timed steps."""
     rank, world, _ = dist_info()
     if rank != 0:
         return 0
-    import oracle
-    n = args.cpu_n
-    res = []
+    import torch
+    n, nrhs, nb = args.n, args.nrhs, (args.nb or 256)
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    A, B, xt = make_system(n, nrhs, args.kappa, dev)
+    a, b = host_system(A, B)
+    xt = xt.cpu().numpy().T
+    del A, B
+    if dev == "cuda":
+        torch.cuda.empty_cache()
+    threads = os.cpu_count() or 1
+    secs, infos, iters = [], [], []
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline(n, args.nrhs, args.kappa)
+        dt, info, it = reference_dsposv(a, b, nb, threads)
         if i >= args.warmup:
-            res.append(r)
-    value = float(np.median([r["value"] for r in res]))
-    secs = float(np.mean([r["seconds"] for r in res]))
+            secs.append(dt)
+            infos.append(info)
+            iters.append(it)
+    ms = float(np.mean(secs)) * 1e3
+    value = flops_of(n, nrhs) / (ms / 1e3) / 1e9
     line = {
         "impl": "reference",
-        "metric": "dsposv FP64-equivalent throughput to FP64 backward error",
+        "metric": METRIC,
         "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": secs * 1e3, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic",
-        "config": {"workload": f"dsposv n={n} (bounded CPU sample of n={args.n}) nrhs={args.nrhs} "
-                               f"A=Q diag(lambda) Q^T kappa={args.kappa:g}"},
-        "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": oracle.get_threads(),
-                         "kind": "port", "sample": res[-1]["sample"]},
+        "config": workload_config(args, nb),
+        "step_ms": [t * 1e3 for t in secs],
+        "iter": iters[-1], "info": infos[-1],
+        "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": threads,
+                         "kind": "reference",
+                         "sample": f"reference PLASMA plasma_dsposv (oracle/_ref, OpenBLAS "
+                                   f"0.3.15 single-threaded, {threads} OpenMP threads on "
+                                   f"{cpu_model()}), {args.steps} solves of the n={n} "
+                                   f"nrhs={nrhs} system, nb={nb}"},
         "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -719,8 +773,10 @@ def main():
 
     cpu = None
     if not args.no_cpu and rank == 0:
-        cpu = cpu_baseline(args.cpu_n, nrhs, args.kappa)
+        a_h, b_h = host_system(A, B)
+        cpu = cpu_baseline(a_h, b_h, args.nb or 256)
         cpu.pop("seconds", None)
+        del a_h, b_h
 
     if rank != 0:
         L.plasma_finalize()
@@ -750,18 +806,12 @@ def main():
         traffic = dram_per_tile * tiles / upd["launches"]
     value = world * flops_of(n, nrhs) / ms / 1e6
     line = {
-        "metric": "dsposv FP64-equivalent throughput to FP64 backward error "
-                  "(vs dposv) at n=32768 on 1 B200",
+        "metric": METRIC,
         "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic",
-        "config": {"workload": f"dsposv n={n} nrhs={nrhs} A=Q diag(lambda) Q^T "
-                               f"kappa={args.kappa:g} seed 11, uplo=L",
-                   "factor": args.mode, "refinement": args.refine,
-                   "nb": args.nb or L.plasma_tuning_get_potrf_nb(pb.PlasmaRealFloat, n),
-                   "l2": "inputs larger than L2 (A is 8.6 GB)",
-                   "parallelism": f"replicas x{world}"},
+        "config": dict(workload_config(args, nbv), parallelism=f"replicas x{world}"),
         "step_ms": step_ms,
         "iter": iters, "backward_error": berr, "forward_error": ferr,
         "backward_error_target": 50 * n * 2.0 ** -53,

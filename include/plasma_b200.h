@@ -49,6 +49,10 @@ void *plasma_get_stream(void);
 /* Number of kernels this library has launched since plasma_init(). */
 long long plasma_kernel_launches(void);
 
+/* Number of device (cudaMalloc) and page-locked host (cudaMallocHost)
+ * allocations this library has made since the process started. */
+long long plasma_device_allocations(void);
+
 /* Tile size the PlasmaTuning table holds for the size bucket of n
  * (dtyp = PlasmaRealDouble or PlasmaRealFloat), and its update by a measured
  * autotuner. */
@@ -98,10 +102,11 @@ int plasma_profile_query(int kclass, long long *launches, double *ms,
  * fails the request with PlasmaErrorIllegalValue, other shapes with
  * PlasmaErrorNotSupported.  The first call on a device looks the array's
  * address up (cudaGetSymbolAddress); make that first call before any stream
- * capture.  All calls share the one array: calls that overlap (other
- * streams, other host threads) race, and the array keeps the last call's
- * contents (each sweep clears its own ticket and abort words; the flags are
- * matched against a per-call epoch, not against zero).
+ * capture.  All calls share the one array and a per-device epoch counter
+ * (host memory): calls that overlap (other streams, other host threads)
+ * race on both, and the array keeps the last call's contents (each sweep
+ * clears its own ticket and abort words; the flags are matched against the
+ * call's epoch, not against zero).
  */
 #define PLASMA_NOALLOC_MAX_N 8192
 void plasma_omp_dpotrs_noalloc(plasma_enum_t uplo, plasma_desc_t A,

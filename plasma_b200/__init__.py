@@ -220,6 +220,7 @@ _SIGNATURES = [
     ("plasma_set_stream", c_int, [c_void_p]),
     ("plasma_get_stream", c_void_p, []),
     ("plasma_kernel_launches", c_longlong, []),
+    ("plasma_device_allocations", c_longlong, []),
     ("plasma_strerror", c_char_p, [c_int]),
     ("plasma_profile_enable", None, [c_int]),
     ("plasma_profile_query", c_int, [c_int, POINTER(c_longlong), POINTER(c_double),

@@ -12,15 +12,24 @@
  *                       up to itermax = 30 refinement steps; otherwise
  *                       iter = -31 and the FP64 potrf + two trsm.
  *
+ * Failures, as the reference: in its own configuration (FP32 factor,
+ * classical IR -- the defaults) a failed FP32 factorisation fails the call
+ * with that factorisation's info (the first non-positive leading minor of
+ * the FP32 matrix), and an FP32 overflow in a conversion (of A, B or a
+ * residual) fails it with info = 1; iter is then -31 and X is not written.
+ * The reference gets there by cancelling every later task of the sequence
+ * (each core task tests sequence->status first), so that its FP64 fallback
+ * never runs; its iter in that case is read from buffers no task filled,
+ * and -31 is what it returns in practice.  The reference's tester checks
+ * only info (test/test_zcposv.c:181-192).  The extended configurations
+ * (TF32 / BF16 / Auto factors, GMRES-IR or the automatic scheme) retry a
+ * failed factorisation scaled and shifted and then fall back to FP64, as
+ * LAPACK's dsposv does on an FP32 failure.
+ *
  * Deliberate differences (also listed in the design notes):
- *  - When the low-precision factorisation or a conversion fails, the reference
- *    marks the whole sequence as failed and returns that info with iter = -31
- *    without solving (an SPD matrix that is not SPD in FP32 is reported as
- *    not positive definite).  Here the solver falls back to the FP64
- *    factorisation, as LAPACK's dsposv -- the reference tester's oracle -- does,
- *    and returns the FP64 info (iter = -31).
  *  - Only the uplo triangle of A is converted (the reference converts the full
- *    general matrix, with a "TODO: need zlat2c" note at zcposv.c:447), and
+ *    general matrix, with a "TODO: need zlat2c" note at zcposv.c:447, so an
+ *    FP32 overflow in the triangle it never reads also gives info = 1), and
  *    into the LOWER triangle of As whatever uplo is (transposed tiles for
  *    uplo = Upper), so that the FP32 factor is always the lower one.
  *  - Extended factor precisions and GMRES-IR are available through
@@ -203,7 +212,7 @@ static int gmres_correction(refine_t *R)
  * reference stopping rule holds.  Returns the number of refinement steps, or
  * -1 when it did not converge within ITERMAX. */
 static int refine_column(refine_t *R, int scheme, double cte, double *xn_out,
-                         double *rn_out, int *used_gmres)
+                         double *rn_out, int *used_gmres, int *status)
 {
     precond(R, R->b, R->x);
     double prev = INFINITY;
@@ -213,7 +222,7 @@ static int refine_column(refine_t *R, int scheme, double cte, double *xn_out,
         residual_vec(R, &xn, &rn);
         *xn_out = xn;
         *rn_out = rn;
-        if (take_status(R->plasma) != 0)
+        if ((*status = take_status(R->plasma)) != 0)
             return -1;                     /* FP32 overflow in a conversion */
         /* stopping rule of the reference's conv(), zcposv.c:275-287 */
         if (rn <= xn * cte)
@@ -397,16 +406,20 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
         plan[nplan++] = (attempt_t){PlasmaFactorFP32, 0};
     } else if (cfg == PlasmaFactorFP32) {
         plan[nplan++] = (attempt_t){PlasmaFactorFP32, 0};
+        if (plasma->refinement != PlasmaRefineIR)
+            plan[nplan++] = (attempt_t){PlasmaFactorFP32, 1};
     } else {
         plan[nplan++] = (attempt_t){cfg, 0};
         plan[nplan++] = (attempt_t){cfg, 1};
     }
     const int scheme = plasma->refinement;
+    /* the reference's configuration keeps the reference's failure semantics */
+    const int ref_failure = cfg == PlasmaFactorFP32 && scheme == PlasmaRefineIR;
     const size_t n = (size_t)A.m, npad = (size_t)As.m;
     const int mres = GMRES_RESTART;
     double cte = 0.0;
     int converged = 0, used_gmres = 0, gm_iters = 0, attempts = 0;
-    int factor_failed = 0;
+    int factor_failed = 0, fstatus = 0;
 
     plasma_cuda_lag2s(S, st, call, B, Xs, PlasmaGeneral);
     size_t need = sizeof(double) * (size_t)n * (6 + mres + 1) +
@@ -455,9 +468,12 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
         if (a == 0 && up != NULL && !up->on_device) {
             upload_and_factor(plasma, up, A, As, d_anorm, sw, call, mode, sequence, request);
             cudaMemcpyAsync(&Anorm, d_anorm, sizeof(double), cudaMemcpyDeviceToHost, S);
-            factor_failed = take_status(plasma) != 0;
+            fstatus = take_status(plasma);
+            factor_failed = fstatus != 0;
             if (rep)
                 cudaEventRecord(e1, S);
+            if (factor_failed && ref_failure)
+                goto failed;
             if (factor_failed)
                 continue;
             goto factored;
@@ -479,9 +495,12 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
             RF.dscale = dvec;
         }
         plasma_pXpotrf_mode(plasma, uplo_s, As, sequence, request, call, mode);
-        factor_failed = take_status(plasma) != 0;
+        fstatus = take_status(plasma);
+        factor_failed = fstatus != 0;
         if (rep)
             cudaEventRecord(e1, S);
+        if (factor_failed && ref_failure)
+            goto failed;
         if (factor_failed)
             continue;
     factored:
@@ -496,9 +515,14 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
         for (int j = 0; j < nrhs; j++) {
             plasma_cuda_column(S, B, j, RF.b, 1);
             double xn = 0, rn = 0;
-            int it = refine_column(&RF, scheme, cte, &xn, &rn, &used_gmres);
+            int cstat = 0;
+            int it = refine_column(&RF, scheme, cte, &xn, &rn, &used_gmres, &cstat);
             Xnorm[j] = xn;
             Rnorm[j] = rn;
+            if (cstat != 0 && ref_failure) {
+                fstatus = cstat;
+                goto failed;
+            }
             if (it < 0) {
                 converged = 0;
                 break;
@@ -546,6 +570,19 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
     plasma_pXpotrs(plasma, uplo, A, X, sequence, request);
     if (rep) {
         rep->fallback_fp64 = 1;
+        cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
+    }
+    return;
+
+failed:
+    /* the reference's cancelled sequence: its info, iter = -31, no solve */
+    *iter = -ITERMAX - 1;
+    plasma_request_fail(sequence, request, fstatus);
+    if (rep) {
+        rep->attempts = attempts;
+        rep->anorm = Anorm;
+        cudaEventRecord(e2, S);
+        cudaEventSynchronize(e2);
         cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
     }
 }

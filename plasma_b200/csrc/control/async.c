@@ -57,6 +57,14 @@ int plasma_sequence_wait(plasma_sequence_t *sequence)
                                 PlasmaErrorInternal);
         return PlasmaErrorInternal;
     }
+    int cerr = plasma_take_cuda_error();
+    if (cerr != 0) {
+        /* a launch that never ran: its request is not known, so the error
+         * goes to the sequence waited on */
+        plasma_error(cudaGetErrorString((cudaError_t)cerr));
+        if (sequence && sequence->status == PlasmaSuccess)
+            plasma_request_fail(sequence, sequence->request, PlasmaErrorInternal);
+    }
     cudaMemcpy(plasma->hstat, plasma->dstat, sizeof(plasma_devstat_t),
                cudaMemcpyDeviceToHost);
     int status = plasma->hstat->status;

@@ -23,6 +23,24 @@ static int plasma_initialized_g = 0;
 static plasma_context_t plasma_context_g;
 static int plasma_device_request_g = 0;   /* PlasmaDevice set before init */
 long long plasma_launch_count_g = 0;
+long long plasma_alloc_count_g = 0;
+static int plasma_cuda_error_g = 0;        /* first unreported CUDA error */
+
+void plasma_note_cuda_error(void)
+{
+    cudaError_t e = cudaGetLastError();
+    /* an allocation that failed is reported by the caller's return code */
+    if (e != cudaSuccess && e != cudaErrorMemoryAllocation && plasma_cuda_error_g == 0)
+        plasma_cuda_error_g = (int)e;
+}
+
+int plasma_take_cuda_error(void)
+{
+    plasma_note_cuda_error();
+    int e = plasma_cuda_error_g;
+    plasma_cuda_error_g = 0;
+    return e;
+}
 
 plasma_context_t *plasma_context_self(void)
 {
@@ -278,6 +296,11 @@ long long plasma_kernel_launches(void)
     return plasma_launch_count_g;
 }
 
+long long plasma_device_allocations(void)
+{
+    return plasma_alloc_count_g;
+}
+
 int plasma_call_begin(plasma_context_t *c, plasma_sequence_t *sequence,
                       plasma_request_t *request)
 {
@@ -303,8 +326,10 @@ void *plasma_scratch(plasma_context_t *c, int slot, size_t bytes)
         c->scratch_bytes[slot] = 0;
     }
     size_t want = bytes + bytes / 8 + (1u << 20);
+    plasma_note_cuda_error();
+    plasma_alloc_count_g++;
     if (cudaMalloc(&c->scratch[slot], want) != cudaSuccess) {
-        cudaGetLastError();
+        plasma_note_cuda_error();
         c->scratch[slot] = NULL;
         return NULL;
     }
@@ -322,8 +347,10 @@ void *plasma_pinned(plasma_context_t *c, size_t bytes)
         c->pinned = NULL;
         c->pinned_bytes = 0;
     }
+    plasma_note_cuda_error();
+    plasma_alloc_count_g++;
     if (cudaMallocHost(&c->pinned, bytes) != cudaSuccess) {
-        cudaGetLastError();
+        plasma_note_cuda_error();
         c->pinned = NULL;
         return NULL;
     }
@@ -378,8 +405,10 @@ int plasma_sweep_reserve(plasma_context_t *c, plasma_desc_t A)
         }
         c->sweep_sync = NULL;
         c->sweep_sync_bytes = 0;
+        plasma_note_cuda_error();
+        plasma_alloc_count_g++;
         if (cudaMalloc(&c->sweep_sync, need) != cudaSuccess) {
-            cudaGetLastError();
+            plasma_note_cuda_error();
             return 0;
         }
         cudaMemsetAsync(c->sweep_sync, 0, need, c->stream);

@@ -40,8 +40,10 @@ static int desc_alloc(plasma_desc_t *A)
     A->matrix = NULL;
     if (bytes == 0)
         bytes = 16;
+    plasma_note_cuda_error();
+    plasma_alloc_count_g++;
     if (cudaMalloc(&A->matrix, bytes) != cudaSuccess) {
-        cudaGetLastError();
+        plasma_note_cuda_error();
         A->matrix = NULL;
         plasma_error("cudaMalloc() failed");
         return PlasmaErrorOutOfMemory;

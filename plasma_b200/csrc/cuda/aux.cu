@@ -165,12 +165,11 @@ extern "C" void plasma_cuda_residual(cudaStream_t s, plasma_devstat_t *st,
     cudaMemsetAsync(rnorm, 0, sizeof(double) * (size_t)B.n, s);
     if (B.mt == 0 || B.nt == 0) return;
     PLASMA_COUNT_LAUNCH();
-    static bool attr_set = false;
-    if (!attr_set) {
+    static unsigned long long attr_set = 0;
+    if (plasma_first_on_device(&attr_set)) {
         cudaFuncSetAttribute(k_residual,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                              200 * 1024);
-        attr_set = true;
     }
     size_t smem = (size_t)X.mb * (kCols + 1) * sizeof(double);
     dim3 grid(B.mt, B.nt, ceil_div(B.nb, kCols));

@@ -450,11 +450,10 @@ k_batched(BatchArgs a)
 template <typename T, int SPLIT>
 void launch_batched(cudaStream_t s, const BatchArgs &a, int grid)
 {
-    static bool attr = false;
-    if (!attr) {
+    static unsigned long long attr = 0;
+    if (plasma_first_on_device(&attr)) {
         cudaFuncSetAttribute(k_batched<T, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              batched_smem<T>());
-        attr = true;
     }
     k_batched<T, SPLIT><<<grid, BT, batched_smem<T>(), s>>>(a);
 }

@@ -15,7 +15,20 @@
 
 extern "C" long long plasma_launch_count_g;
 
-#define PLASMA_COUNT_LAUNCH() (++plasma_launch_count_g)
+#define PLASMA_COUNT_LAUNCH() (plasma_note_cuda_error(), ++plasma_launch_count_g)
+
+// True the first time it is called with this flag word for the current
+// device (bit d for device d).  Kernel attributes such as the dynamic shared
+// memory limit belong to one device's context, so each is set once per device.
+inline bool plasma_first_on_device(unsigned long long *mask)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (*mask & bit) return false;
+    *mask |= bit;
+    return true;
+}
 
 // A logical lower-storage view of one tile: element (i,j) of the logical tile
 // is p[j*ld + i], or p[i*ld + j] when the stored tile is its transpose.

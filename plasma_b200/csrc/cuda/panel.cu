@@ -433,11 +433,10 @@ template <typename T, int SPLIT>
 void launch_diag(cudaStream_t s, plasma_devstat_t *st, int call,
                  const plasma_desc_t &A, int k, int iinfo)
 {
-    static bool attr = false;
-    if (!attr) {
+    static unsigned long long attr = 0;
+    if (plasma_first_on_device(&attr)) {
         cudaFuncSetAttribute(k_potrf_diag_mma<T, SPLIT>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, diag_smem<T>());
-        attr = true;
     }
     k_potrf_diag_mma<T, SPLIT><<<1, THR, diag_smem<T>(), s>>>(A, k, iinfo, st, call);
 }
@@ -446,11 +445,10 @@ template <typename T, int SPLIT>
 void launch_trsm(cudaStream_t s, plasma_devstat_t *st, const plasma_desc_t &A,
                  int k, int mlo, int mhi)
 {
-    static bool attr = false;
-    if (!attr) {
+    static unsigned long long attr = 0;
+    if (plasma_first_on_device(&attr)) {
         cudaFuncSetAttribute(k_trsm_panel_mma<T, SPLIT>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, trsm_smem<T>());
-        attr = true;
     }
     dim3 grid((unsigned)(mhi - mlo), (unsigned)ceil_div(A.mb, TR));
     k_trsm_panel_mma<T, SPLIT><<<grid, THR, trsm_smem<T>(), s>>>(A, k, mlo, st);

@@ -184,12 +184,11 @@ template <int SPLIT>
 void launch(cudaStream_t s, plasma_devstat_t *st, int call, const plasma_desc_t &A, int k,
             int iinfo, int bytes)
 {
-    static bool attr = false;
-    if (!attr) {
+    static unsigned long long attr = 0;
+    if (plasma_first_on_device(&attr)) {
         cudaFuncSetAttribute(k_potrf_diag_smem<SPLIT>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                              smem_floats(SM_NBMAX) * 4);
-        attr = true;
     }
     k_potrf_diag_smem<SPLIT><<<1, SM_THREADS, bytes, s>>>(A, k, iinfo, st, call);
 }

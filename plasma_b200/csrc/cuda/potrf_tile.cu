@@ -233,12 +233,11 @@ void launch_potrf_tile(cudaStream_t s, plasma_devstat_t *st, int call,
 {
     int n = plasma_tile_mview(A, k);
     size_t smem = (size_t)n * (kIB + 1) * sizeof(T);
-    static bool attr_set = false;
-    if (!attr_set) {
+    static unsigned long long attr_set = 0;
+    if (plasma_first_on_device(&attr_set)) {
         cudaFuncSetAttribute(k_potrf_tile<T>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                              200 * 1024);
-        attr_set = true;
     }
     k_potrf_tile<T><<<1, kPotrfThreads, smem, s>>>(A, uplo, k, iinfo, st, call);
 }
@@ -249,12 +248,11 @@ void launch_trsm_panel(cudaStream_t s, plasma_devstat_t *st, int uplo,
 {
     int n = plasma_tile_mview(A, k);
     size_t smem = (size_t)kTrsmRows * (n + 1) * sizeof(T);
-    static bool attr_set = false;
-    if (!attr_set) {
+    static unsigned long long attr_set = 0;
+    if (plasma_first_on_device(&attr_set)) {
         cudaFuncSetAttribute(k_trsm_panel<T>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                              200 * 1024);
-        attr_set = true;
     }
     dim3 grid((unsigned)(mhi - mlo), (unsigned)ceil_div(A.mb, kTrsmRows));
     k_trsm_panel<T><<<grid, kTrsmThreads, smem, s>>>(A, uplo, k, mlo, st);
@@ -265,12 +263,11 @@ void launch_trtri(cudaStream_t s, plasma_devstat_t *st, int uplo,
                   const plasma_desc_t &A, T *W)
 {
     size_t smem = (size_t)A.mb * (kInvCols + 1) * sizeof(T);
-    static bool attr_set = false;
-    if (!attr_set) {
+    static unsigned long long attr_set = 0;
+    if (plasma_first_on_device(&attr_set)) {
         cudaFuncSetAttribute(k_trtri_tiles<T>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                              200 * 1024);
-        attr_set = true;
     }
     k_trtri_tiles<T><<<A.mt, kInvThreads, smem, s>>>(A, uplo, W, st);
 }

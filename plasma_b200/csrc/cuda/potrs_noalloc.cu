@@ -22,7 +22,9 @@
 // The ticket and abort words are cleared on the stream at the start of each
 // sweep; the ready flags are never cleared, each sweep waits for its own
 // epoch (a per-device counter, never 0, and the array starts zeroed), and the
-// block inverses are rewritten in full by every call.
+// block inverses are rewritten in full by every call.  The epoch counter is
+// host state shared by every call on the device too: calls from several host
+// threads race on it as they race on the array.
 #include "common.cuh"
 
 namespace {
@@ -37,13 +39,16 @@ __device__ __align__(256) double
     g_potrs_scratch[NA_W_DOUBLES + NA_SYNC_BYTES / sizeof(double)];
 
 double *g_scratch_addr[NA_MAX_DEVICES];
-int g_epoch[NA_MAX_DEVICES];
+unsigned g_epoch[NA_MAX_DEVICES];
 
+// The sweeps compare ready flags with the epoch for equality only, so the
+// counter's bit pattern is passed as it is; it skips 0 (the value of flags
+// no sweep has written) when it wraps after 2^32 sweeps.
 int next_epoch(int dev)
 {
-    if (++g_epoch[dev] <= 0)
-        g_epoch[dev] = 1;
-    return g_epoch[dev];
+    if (++g_epoch[dev] == 0u)
+        g_epoch[dev] = 1u;
+    return (int)g_epoch[dev];
 }
 
 }  // namespace
@@ -141,9 +146,14 @@ extern "C" void plasma_omp_dpotrs_noalloc(plasma_enum_t uplo, plasma_desc_t A,
     void *sync = W + NA_W_DOUBLES;
 
     plasma_call_begin(plasma, sequence, request);
+    // (the checks above make A eligible for 64-row FP64 block sweeps, so
+    // both sweeps launch; a sweep that does not launch fails the request)
     plasma_cuda_trtri_blocks(plasma->stream, plasma->dstat, uplo, A, W);
-    plasma_cuda_trsv(plasma->stream, plasma->dstat, uplo, 0, A, W, B.matrix,
-                     sync, next_epoch(dev), plasma->num_sms);
-    plasma_cuda_trsv(plasma->stream, plasma->dstat, uplo, 1, A, W, B.matrix,
-                     sync, next_epoch(dev), plasma->num_sms);
+    if (!plasma_cuda_trsv(plasma->stream, plasma->dstat, uplo, 0, A, W, B.matrix,
+                          sync, next_epoch(dev), plasma->num_sms) ||
+        !plasma_cuda_trsv(plasma->stream, plasma->dstat, uplo, 1, A, W, B.matrix,
+                          sync, next_epoch(dev), plasma->num_sms)) {
+        plasma_error("plasma_omp_dpotrs_noalloc: the block sweep did not launch");
+        plasma_request_fail(sequence, request, PlasmaErrorInternal);
+    }
 }

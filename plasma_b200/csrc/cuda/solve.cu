@@ -164,15 +164,14 @@ void sweep(cudaStream_t s, plasma_devstat_t *st, int uplo, int trans,
     const int nbw = A.mb;
     const int chunks = ceil_div(B.nb, kCols);
     const size_t smem = (size_t)B.mb * (kCols + 1) * sizeof(T);
-    static bool attr_set = false;
-    if (!attr_set) {
+    static unsigned long long attr_set = 0;
+    if (plasma_first_on_device(&attr_set)) {
         cudaFuncSetAttribute(k_diag_apply<T>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                              200 * 1024);
         cudaFuncSetAttribute(k_solve_update<T>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                              200 * 1024);
-        attr_set = true;
     }
     // many right-hand sides: the update of a step is one tensor-core GEMM on
     // views of the factor and of B (cuda/adjoint.cu, k_gemm_view)

@@ -764,12 +764,11 @@ template <typename T, int SB>
 void launch_trtri(cudaStream_t s, plasma_devstat_t *st, int uplo,
                   const plasma_desc_t &A, void *W, int nblk)
 {
-    static bool attr = false;
-    if (!attr) {
+    static unsigned long long attr = 0;
+    if (plasma_first_on_device(&attr)) {
         cudaFuncSetAttribute(k_trtri_blocks<T, SB>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                              trtri_smem<T, SB>());
-        attr = true;
     }
     k_trtri_blocks<T, SB><<<nblk, 256, trtri_smem<T, SB>(), s>>>(A, uplo, (T *)W, st);
 }
@@ -779,12 +778,11 @@ void launch_trsv(cudaStream_t s, plasma_devstat_t *st, int uplo, int backward,
                  const plasma_desc_t &A, const void *W, void *vec, SweepSync *sy,
                  int epoch, int grid)
 {
-    static bool attr = false;
-    if (!attr) {
+    static unsigned long long attr = 0;
+    if (plasma_first_on_device(&attr)) {
         cudaFuncSetAttribute(k_trsv<T, SB>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                              trsv_smem<T, SB>());
-        attr = true;
     }
     k_trsv<T, SB><<<grid, TS_THREADS, trsv_smem<T, SB>(), s>>>(
         A, uplo, backward, (const T *)W, (T *)vec, sy, epoch, st);
@@ -793,11 +791,10 @@ void launch_trsv(cudaStream_t s, plasma_devstat_t *st, int uplo, int backward,
 void launch_couple(cudaStream_t s, plasma_devstat_t *st, int uplo, const plasma_desc_t &A,
                    void *W, int nblk)
 {
-    static bool attr = false;
-    if (!attr) {
+    static unsigned long long attr = 0;
+    if (plasma_first_on_device(&attr)) {
         cudaFuncSetAttribute(k_trsv_couple, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              couple_smem());
-        attr = true;
     }
     k_trsv_couple<<<dim3(nblk, 3), 256, couple_smem(), s>>>(A, uplo, (float *)W, st);
 }
@@ -807,11 +804,10 @@ void launch_ll(cudaStream_t s, plasma_devstat_t *st, int uplo, int backward,
                const plasma_desc_t &A, const Couple &C, float *vec, unsigned long long *ll,
                SweepSync *sy, int epoch, int grid)
 {
-    static bool attr = false;
-    if (!attr) {
+    static unsigned long long attr = 0;
+    if (plasma_first_on_device(&attr)) {
         cudaFuncSetAttribute(k_trsv_ll<SHAPE_T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              ll_smem());
-        attr = true;
     }
     k_trsv_ll<SHAPE_T><<<grid, LL_THREADS, ll_smem(), s>>>(A, uplo, backward, C, vec, ll, sy,
                                                            epoch, st);

@@ -579,12 +579,11 @@ extern "C" void plasma_cuda_update(cudaStream_t s, plasma_devstat_t *st,
     }
     int prof = plasma_prof_begin(s);
     if (dmma) {
-        static bool attr_set = false;
-        if (!attr_set) {
+        static unsigned long long attr_set = 0;
+        if (plasma_first_on_device(&attr_set)) {
             cudaFuncSetAttribute(k_update_dmma,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  DSMEM);
-            attr_set = true;
         }
         // one CTA per work item: SMs free up often, so the high-priority
         // critical-path kernels of the next step are scheduled in between
@@ -634,20 +633,18 @@ extern "C" int plasma_cuda_sweep_update_mma(cudaStream_t s, plasma_devstat_t *st
     const long long nitems = (long long)(mhi - mlo) * g.sbm * g.ncb;
     PLASMA_COUNT_LAUNCH();
     if (L.precision == PlasmaRealDouble) {
-        static bool attr = false;
-        if (!attr) {
+        static unsigned long long attr = 0;
+        if (plasma_first_on_device(&attr)) {
             cudaFuncSetAttribute(k_sweep_mma<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  SweepGeo<double>::SMEM);
-            attr = true;
         }
         k_sweep_mma<double><<<(unsigned)nitems, THREADS, SweepGeo<double>::SMEM, s>>>(
             g, (int)nitems, st);
     } else {
-        static bool attr = false;
-        if (!attr) {
+        static unsigned long long attr = 0;
+        if (plasma_first_on_device(&attr)) {
             cudaFuncSetAttribute(k_sweep_mma<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  SweepGeo<float>::SMEM);
-            attr = true;
         }
         k_sweep_mma<float><<<(unsigned)nitems, THREADS, SweepGeo<float>::SMEM, s>>>(
             g, (int)nitems, st);

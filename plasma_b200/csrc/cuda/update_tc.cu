@@ -871,11 +871,10 @@ template <int MODE>
 void launch_update(cudaStream_t s, const CUtensorMap &map, const CUtensorMap &cmap,
                    const TcArgs &g, unsigned grid, plasma_devstat_t *st)
 {
-    static bool attr = false;
-    if (!attr) {
+    static unsigned long long attr = 0;
+    if (plasma_first_on_device(&attr)) {
         cudaFuncSetAttribute(k_update_tc<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              Geo<MODE>::SMEM);
-        attr = true;
     }
     k_update_tc<MODE><<<grid, TC_THREADS, Geo<MODE>::SMEM, s>>>(map, cmap, g, st);
 }
@@ -884,11 +883,10 @@ template <int MODE>
 void launch_pair(cudaStream_t s, const CUtensorMap &map, const CUtensorMap &cmap,
                  const TcArgs &g, unsigned grid, plasma_devstat_t *st)
 {
-    static bool attr = false;
-    if (!attr) {
+    static unsigned long long attr = 0;
+    if (plasma_first_on_device(&attr)) {
         cudaFuncSetAttribute(k_update_pair<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              PairGeo<MODE>::SMEM);
-        attr = true;
     }
     k_update_pair<MODE><<<grid, TC_THREADS, PairGeo<MODE>::SMEM, s>>>(map, cmap, g, st);
 }

@@ -103,6 +103,19 @@ int plasma_prof_begin(cudaStream_t s);
 void plasma_prof_end(int slot, cudaStream_t s, int kclass, double flops,
                      double bytes);
 
+/* CUDA errors that no return code reports (a kernel launch with a bad
+ * configuration, e.g. more dynamic shared memory than its limit, only
+ * reaches the host through cudaGetLastError): plasma_note_cuda_error()
+ * keeps the first one (allocation failures excepted: their callers
+ * report them), plasma_take_cuda_error() returns and clears it.  Called
+ * before every launch (PLASMA_COUNT_LAUNCH), before and after every
+ * allocation, and by plasma_sequence_wait, which fails the sequence with
+ * PlasmaErrorInternal. */
+void plasma_note_cuda_error(void);
+int plasma_take_cuda_error(void);
+/* device and pinned allocations made by the library (plasma_device_allocations) */
+extern long long plasma_alloc_count_g;
+
 /* Registers a plasma_omp_* call; returns the id its kernels report. */
 int plasma_call_begin(plasma_context_t *plasma, plasma_sequence_t *sequence,
                       plasma_request_t *request);

@@ -244,15 +244,30 @@ def test_dsposv_spectrum(L, golden, kappa):
     assert np.abs(x - xl).max() / np.abs(xl).max() < kappa * 1e-13
 
 
-def test_dsposv_fallback(L):
+def test_dsposv_fp32_failure(L):
+    """kappa = 1e12: the FP32 factorisation breaks down.  In the reference's
+    configuration (FP32 factor, IR) the call fails with the factorisation's
+    info, iter = -31 and X untouched, as the reference's cancelled sequence
+    does; the automatic mode escalates and solves through FP64."""
     set_nb(L, 32)
     n = 128
     a = gen.spectrum(n, 1e12, seed=11)
     b = np.asfortranarray(np.random.default_rng(1).standard_normal((n, 1)))
-    x = np.zeros_like(b, order="F")
+    x = np.full_like(b, 3.0, order="F")
     it = ctypes.c_int()
-    assert L.plasma_dsposv(LO, n, 1, a.ctypes.data, n, b.ctypes.data, n,
-                           x.ctypes.data, n, ctypes.byref(it)) == 0
+    info = L.plasma_dsposv(LO, n, 1, a.ctypes.data, n, b.ctypes.data, n,
+                           x.ctypes.data, n, ctypes.byref(it))
+    assert info > 0
+    assert it.value == -31
+    assert np.all(x == 3.0)
+    xo = np.full_like(b, 3.0, order="F")
+    assert oracle.dsposv(oracle.LOWER, a, b, xo, 32)[0] > 0
+    L.plasma_set(pb.PlasmaMixedPrecisionMode, pb.PlasmaFactorAuto)
+    try:
+        assert L.plasma_dsposv(LO, n, 1, a.ctypes.data, n, b.ctypes.data, n,
+                               x.ctypes.data, n, ctypes.byref(it)) == 0
+    finally:
+        L.plasma_set(pb.PlasmaMixedPrecisionMode, pb.PlasmaFactorFP32)
     assert it.value == -31
     assert solve_residual(a, x, b) < TOL * EPS
 
@@ -274,17 +289,19 @@ def test_dsposv_sweep_block_sizes(L, n, nb):
 
 
 def test_dsposv_nonspd(L):
-    """Not positive definite: the FP64 path reports LAPACK's info."""
+    """Not positive definite (--zerocol): the FP32 factorisation reports the
+    reference's info, iter = -31 and X is not written."""
     set_nb(L, 64)
     n = 200
     a, b = gen.diag_dominant(n, 1, seed=6)
     a = gen.zerocol(a, 150)
-    x = np.zeros_like(b, order="F")
+    x = np.full_like(b, 3.0, order="F")
     it = ctypes.c_int()
     info = L.plasma_dsposv(LO, n, 1, a.ctypes.data, n, b.ctypes.data, n,
                            x.ctypes.data, n, ctypes.byref(it))
     assert info == 151
     assert it.value == -31
+    assert np.all(x == 3.0)
 
 
 # ------------------------------------------------------------------ async API
@@ -571,17 +588,27 @@ def test_dsposv_overlapped_upload(L, n, nb, kappa):
 
 def test_dsposv_overlapped_upload_fallback(L):
     """kappa = 1e12: the FP32 factorization fails while later column groups
-    are still on their way; the FP64 tiles of A are completed regardless
-    and the FP64 fallback solves the system (iter = -31)."""
+    are still on their way.  The reference's configuration fails the call
+    (info > 0, iter = -31, X untouched) once the copies are done; in the
+    automatic mode the FP64 tiles of A are completed regardless and the
+    FP64 fallback solves the system (iter = -31)."""
     set_nb(L, 128)
     n = 2048
     a = gen.spectrum(n, 1e12, seed=11)
     b = np.random.default_rng(1).standard_normal((n, 1))
     A, B = _pinned_colmajor(a), _pinned_colmajor(b)
-    X = torch.zeros((1, n), dtype=torch.float64, pin_memory=True)
+    X = torch.full((1, n), 3.0, dtype=torch.float64, pin_memory=True)
     it = ctypes.c_int()
     assert L.plasma_dsposv(LO, n, 1, A.data_ptr(), n, B.data_ptr(), n, X.data_ptr(), n,
-                           ctypes.byref(it)) == 0
+                           ctypes.byref(it)) > 0
+    assert it.value == -31
+    assert bool((X == 3.0).all())
+    L.plasma_set(pb.PlasmaMixedPrecisionMode, pb.PlasmaFactorAuto)
+    try:
+        assert L.plasma_dsposv(LO, n, 1, A.data_ptr(), n, B.data_ptr(), n, X.data_ptr(), n,
+                               ctypes.byref(it)) == 0
+    finally:
+        L.plasma_set(pb.PlasmaMixedPrecisionMode, pb.PlasmaFactorFP32)
     assert it.value == -31
     assert solve_residual(a, X.numpy().T.copy(), b) < TOL * EPS
 
@@ -688,16 +715,51 @@ def test_dsposv_device_pointer(L, n, nb):
 
 def test_dsposv_device_pointer_fp32_overflow(L):
     """Entries beyond the FP32 range: the one-pass conversion reports the
-    overflow, the FP32 attempt is abandoned and the FP64 fallback solves the
-    system from the FP64 tiles the same pass wrote (iter = -31)."""
+    overflow.  The reference's configuration fails the call with info = 1
+    (core_zlag2c.c:60-75), iter = -31 and X untouched; the automatic mode
+    goes on to the FP64 fallback, which solves the system from the FP64
+    tiles the same pass wrote."""
     set_nb(L, 128)
     n = 600
     a, b = gen.diag_dominant(n, 1, seed=4500)
     a = a * 1e39
     A, B = _device_colmajor(a, n), _device_colmajor(b, n)
-    X = torch.zeros((1, n), dtype=torch.float64, device="cuda")
+    X = torch.full((1, n), 3.0, dtype=torch.float64, device="cuda")
     it = ctypes.c_int()
     assert L.plasma_dsposv(LO, n, 1, A.data_ptr(), n, B.data_ptr(), n, X.data_ptr(), n,
-                           ctypes.byref(it)) == 0
+                           ctypes.byref(it)) == 1
+    assert it.value == -31
+    assert bool((X == 3.0).all())
+    L.plasma_set(pb.PlasmaMixedPrecisionMode, pb.PlasmaFactorAuto)
+    try:
+        assert L.plasma_dsposv(LO, n, 1, A.data_ptr(), n, B.data_ptr(), n, X.data_ptr(), n,
+                               ctypes.byref(it)) == 0
+    finally:
+        L.plasma_set(pb.PlasmaMixedPrecisionMode, pb.PlasmaFactorFP32)
     assert it.value == -31
     assert solve_residual(a, X.cpu().numpy().T.copy(), b) < TOL * EPS
+
+
+
+
+# ------------------------------------------------------------------ lifecycle
+def test_reinit_and_solve_twice(L):
+    """plasma_finalize, plasma_set(PlasmaDevice), plasma_init and a solve, twice:
+    the kernels' shared-memory limits are set per device, launch errors are
+    checked at every synchronisation, and the answers stay right."""
+    n = 1500
+    a, b = gen.diag_dominant(n, 2, seed=77)
+    for _ in range(2):
+        assert L.plasma_finalize() == 0
+        assert L.plasma_set(pb.PlasmaDevice, 0) == 0
+        assert L.plasma_init() == 0
+        set_nb(L, 256)
+        x = np.asfortranarray(b.copy())
+        assert L.plasma_dposv(LO, n, 2, np.asfortranarray(a.copy()).ctypes.data, n,
+                              x.ctypes.data, n) == 0
+        assert solve_residual(a, x, b) < TOL * EPS
+        xs = np.zeros_like(b, order="F")
+        it = ctypes.c_int()
+        assert L.plasma_dsposv(LO, n, 2, a.ctypes.data, n, b.ctypes.data, n, xs.ctypes.data, n,
+                               ctypes.byref(it)) == 0
+        assert solve_residual(a, xs, b) < TOL * EPS

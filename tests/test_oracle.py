@@ -93,15 +93,32 @@ def test_dsposv_converges_like_reference(n):
     assert solve_residual(a, x, b) < TOL * EPS
 
 
-def test_dsposv_fallback_on_fp32_failure():
-    """kappa far beyond 1/eps_fp32: the FP32 factor fails or IR stalls; the
-    FP64 path answers with iter = -31 (zcposv.c:524)."""
+def test_dsposv_fp32_failure_cancels():
+    """kappa far beyond 1/eps_fp32: the FP32 factor breaks down, and as in
+    the reference's cancelled task sequence the call returns that info with
+    iter = -31, no FP64 solve and X untouched (zcposv.c:440-538 with the
+    sequence->status test of every core task)."""
     n = 128
     a = gen.spectrum(n, 1e12, seed=11)
     rng = np.random.default_rng(1)
     b = np.asfortranarray(rng.standard_normal((n, 1)))
-    x = np.zeros_like(b, order="F")
+    x = np.full_like(b, 3.0, order="F")
     info, it = oracle.dsposv(LO, a, b, x, 32)
+    assert info > 0
+    assert it == -31
+    assert np.all(x == 3.0)
+
+
+def test_dsposv_refinement_exhausted_goes_fp64():
+    """The FP32 factor succeeds but 30 refinement steps do not meet the
+    stopping rule: the FP64 factorisation answers with iter = -31
+    (zcposv.c:522-538).  kappa = 1e8 at n = 256 in upper storage is such a
+    case for the oracle's (and the reference's) FP32 rounding."""
+    n = 256
+    a = gen.spectrum(n, 1e8, seed=11)
+    b = np.asfortranarray(a @ np.random.default_rng(12).standard_normal((n, 2)))
+    x = np.zeros_like(b, order="F")
+    info, it = oracle.dsposv(UP, a, b, x, 256)
     assert info == 0
     assert it == -31
     assert solve_residual(a, x, b) < TOL * EPS

@@ -1,0 +1,213 @@
+"""The CPU oracle pinned to the reference PLASMA's own outputs (CPU only).
+
+reference_fixtures.npz holds what the reference itself (built from its
+sources by oracle/build_ref.sh, run by tests/golden/make_ref_golden.py)
+returns on seeded inputs: factor checksums, solutions, dsposv's iter and
+info, and its failure semantics.  The oracle must agree before it is trusted
+as the checker of the GPU library.  Where the reference library is present
+(oracle/_ref), a few cases are also run live against it, and the library's
+argument codes are compared with the reference's.
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+import gen
+import oracle
+from conftest import EPS, TOL, solve_residual
+from oracle import ref
+
+LO, UP = oracle.LOWER, oracle.UPPER
+
+
+@pytest.fixture(scope="session")
+def rg():
+    return np.load(os.path.join(os.path.dirname(__file__), "golden",
+                                "reference_fixtures.npz"))
+
+
+def have_ref():
+    return os.path.exists(ref.LIB_PATH) or ref.available()
+
+
+def F(a):
+    return np.asfortranarray(np.array(a, dtype=np.float64))
+
+
+def close(x, xr, tol=1e-13):
+    """Normwise agreement max|x - xr| / max|xr| < tol."""
+    assert np.abs(x - xr).max() / np.abs(xr).max() < tol
+
+
+@pytest.mark.parametrize("key,n,nb,seed", [("cfg1", 2048, 256, 42), ("rag", 1000, 128, 3000)])
+def test_oracle_factor_matches_reference(rg, key, n, nb, seed):
+    """Config 1 (and a ragged size): the oracle's factor against the
+    reference's, through diag(L) and L v, to within the potrf tester's
+    50 eps (test/test_zpotrf.c:124-141)."""
+    a, _ = gen.diag_dominant(n, 1, seed=seed)
+    v = gen.probe_vector(n)
+    an = np.linalg.norm(a)
+    for uplo, d, p in ((LO, "diagL", "Lv"), (UP, "diagU", "UTv")):
+        f = F(a)
+        assert oracle.potrf(uplo, f, nb) == 0
+        t = np.tril(f) if uplo == LO else np.triu(f).T
+        assert np.abs(np.diag(t) - rg[f"{key}_{d}"]).max() / np.abs(np.diag(t)).max() < TOL * EPS
+        assert np.linalg.norm(t @ v - rg[f"{key}_{p}"]) / (an * np.linalg.norm(v)) < TOL * EPS
+
+
+def test_oracle_solves_match_reference(rg):
+    a, b = gen.diag_dominant(2048, 1, seed=42)
+    x = F(b)
+    assert oracle.posv(LO, F(a), x, 256) == 0
+    close(x, rg["cfg1_dposv_X"])
+    a, b = gen.diag_dominant(1000, 3, seed=3000)
+    for uplo, key in ((LO, "rag_dposv_X"), (UP, "rag_dposv_up_X")):
+        x = F(b)
+        assert oracle.posv(uplo, F(a), x, 128) == 0
+        close(x, rg[key])
+    a, b = gen.diag_dominant(300, 4, seed=3001)
+    f = F(a)
+    assert oracle.potrf(LO, f, 64) == 0
+    x = F(b)
+    assert oracle.potrs(LO, f, x, 64) == 0
+    close(x, rg["potrs_X"])
+
+
+def test_oracle_dsposv_cfg1_matches_reference(rg):
+    a, b = gen.diag_dominant(2048, 1, seed=42)
+    x = F(np.zeros_like(b))
+    info, it = oracle.dsposv(LO, a, b, x, 256)
+    assert info == int(rg["cfg1_dsposv_info"]) == 0
+    assert it == int(rg["cfg1_dsposv_iter"])
+    close(x, rg["cfg1_dsposv_X"])
+
+
+@pytest.mark.parametrize("n,nb", [(256, 64), (1000, 128)])
+@pytest.mark.parametrize("kexp", [2, 5])
+@pytest.mark.parametrize("tag", ["L", "U"])
+def test_oracle_dsposv_iter_matches_reference(rg, n, nb, kexp, tag):
+    """dsposv's refinement count (zcposv.c:474-518) and solution, against the
+    reference's on the same bytes."""
+    a = gen.spectrum(n, 10.0 ** kexp, seed=11)
+    b = F(a @ np.random.default_rng(12).standard_normal((n, 2)))
+    x = F(np.zeros_like(b))
+    info, it = oracle.dsposv(LO if tag == "L" else UP, a, b, x, nb)
+    key = f"spec_n{n}_k{kexp}_{tag}"
+    assert info == int(rg[f"{key}_info"]) == 0
+    assert it == int(rg[f"{key}_iter"])
+    xr = rg[f"{key}_X"]
+    assert np.abs(x - xr).max() / np.abs(xr).max() < 10.0 ** kexp * 1e-13
+    assert solve_residual(a, x, b) < TOL * EPS
+
+
+@pytest.mark.parametrize("col", [0, 299, 999])
+def test_oracle_zerocol_info_matches_reference(rg, col):
+    """--zerocol (test/test_zcposv.c:104-110, :181-192; test_zpotrf.c:97-99,
+    :143-151): the same info, iter = -31 and X left as it was."""
+    a, b = gen.diag_dominant(1000, 2, seed=6)
+    x = F(np.full(b.shape, 7.0))
+    info, it = oracle.dsposv(LO, gen.zerocol(a, col), b, x, 128)
+    assert info == int(rg[f"fail_zerocol{col}_info"]) == col + 1
+    assert it == int(rg[f"fail_zerocol{col}_iter"]) == -31
+    assert np.all(x == 7.0) and np.all(rg[f"fail_zerocol{col}_X"] == 7.0)
+    f = F(a)
+    f[:, col] = 0.0
+    assert oracle.potrf(LO, f, 128) == int(rg[f"fail_potrf_zerocol{col}_info"])
+
+
+@pytest.mark.parametrize("tag", ["L", "U"])
+def test_oracle_fp32_failure_matches_reference(rg, tag):
+    """kappa = 1e12: the FP32 factorisation breaks down; the reference
+    cancels the sequence (info > 0, no FP64 solve).  The failing column
+    depends on FP32 rounding, so only its sign is compared."""
+    a = gen.spectrum(256, 1e12, seed=11)
+    b = F(np.random.default_rng(1).standard_normal((256, 1)))
+    x = F(np.full(b.shape, 7.0))
+    info, it = oracle.dsposv(LO if tag == "L" else UP, a, b, x, 64)
+    assert info > 0 and int(rg[f"fail_k12_{tag}_info"]) > 0
+    assert it == int(rg[f"fail_k12_{tag}_iter"]) == -31
+    assert np.all(x == 7.0)
+
+
+def test_oracle_overflow_matches_reference(rg):
+    a, b = gen.diag_dominant(1000, 2, seed=6)
+    ao = a.copy()
+    ao[5, 3] = ao[3, 5] = 1e39
+    bo = b.copy()
+    bo[4, 1] = -1e39
+    for key, aa, bb in (("fail_ovfA", ao, b), ("fail_ovfB", a, bo)):
+        x = F(np.full(b.shape, 7.0))
+        info, it = oracle.dsposv(LO, F(aa), F(bb), x, 128)
+        assert info == int(rg[f"{key}_info"]) == 1
+        assert it == int(rg[f"{key}_iter"]) == -31
+        assert np.all(x == 7.0)
+
+
+# ------------------------------------------------------- live reference runs
+needs_ref = pytest.mark.skipif(not have_ref(), reason="reference library not built here")
+
+
+@needs_ref
+@pytest.mark.parametrize("n,nb,seed", [(513, 96, 1), (1200, 256, 2)])
+def test_oracle_against_live_reference(n, nb, seed):
+    """Fresh seeds, run on the reference library and the oracle."""
+    a, b = gen.diag_dominant(n, 2, seed=seed)
+    xr, xo = F(b), F(b)
+    assert ref.dposv(LO, F(a), xr, nb) == 0
+    assert oracle.posv(LO, F(a), xo, nb) == 0
+    close(xo, xr)
+    s = gen.spectrum(n, 1e4, seed=seed)
+    bs = F(s @ np.ones((n, 1)))
+    xr, xo = F(np.zeros((n, 1))), F(np.zeros((n, 1)))
+    ir = ref.dsposv(UP, F(s), bs, xr, nb)
+    io = oracle.dsposv(UP, F(s), bs, xo, nb)
+    assert ir == io
+    assert np.abs(xo - xr).max() / np.abs(xr).max() < 1e-8
+
+
+@needs_ref
+def test_library_argument_codes_match_reference(monkeypatch):
+    """The library's LAPACK-layout entry points return the reference's codes
+    for each illegal argument and quick return (host-only context)."""
+    import plasma_b200 as pb
+    monkeypatch.setenv("PLASMA_ALLOW_NO_DEVICE", "1")
+    L = pb.lib()
+    R = ref.lib()
+    if L.plasma_init() != 0:
+        pytest.skip("library context unavailable")
+    try:
+        buf = np.zeros(64 * 4)
+        p = buf.ctypes.data
+        it1, it2 = ctypes.c_int(5), ctypes.c_int(5)
+        cases = [(999, 8, 2, 8, 8, 8), (LO, -1, 2, 8, 8, 8), (LO, 8, -1, 8, 8, 8),
+                 (LO, 8, 2, 7, 8, 8), (LO, 8, 2, 8, 7, 8), (LO, 8, 2, 8, 8, 7),
+                 (LO, 0, 2, 1, 1, 1), (LO, 8, 0, 8, 8, 8)]
+        for uplo, n, nrhs, lda, ldb, ldx in cases:
+            got = L.plasma_dsposv(uplo, n, nrhs, p, lda, p, ldb, p, ldx, ctypes.byref(it1))
+            want = R.plasma_dsposv(uplo, n, nrhs, ctypes.c_void_p(p), lda, ctypes.c_void_p(p),
+                                   ldb, ctypes.c_void_p(p), ldx, ctypes.byref(it2))
+            assert got == want, (uplo, n, nrhs, lda, ldb, ldx, got, want)
+            if want == 0:
+                assert it1.value == it2.value == 0
+            # posv / potrs on legal arguments would compute (this context has
+            # no device): compared only up to their quick returns
+            legal = (uplo in (LO, UP) and n >= 0 and nrhs >= 0 and lda >= max(1, n)
+                     and ldb >= max(1, n))
+            if not (legal and min(n, nrhs) > 0):
+                got = L.plasma_dposv(uplo, n, nrhs, p, lda, p, ldb)
+                want = R.plasma_dposv(uplo, n, nrhs, ctypes.c_void_p(p), lda,
+                                      ctypes.c_void_p(p), ldb)
+                assert got == want
+            if not (legal and max(n, nrhs) > 0):
+                got = L.plasma_dpotrs(uplo, n, nrhs, p, lda, p, ldb)
+                want = R.plasma_dpotrs(uplo, n, nrhs, ctypes.c_void_p(p), lda,
+                                       ctypes.c_void_p(p), ldb)
+                assert got == want
+        for uplo, n, lda in ((999, 8, 8), (LO, -1, 8), (LO, 8, 7), (LO, 0, 1)):
+            got = L.plasma_dpotrf(uplo, n, p, lda)
+            want = R.plasma_dpotrf(uplo, n, ctypes.c_void_p(p), lda)
+            assert got == want, (uplo, n, lda, got, want)
+    finally:
+        L.plasma_finalize()

@@ -58,3 +58,22 @@ def test_reference_arm_other_ranks_exit_quietly():
                        env=env, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip() == ""
+
+
+def test_reference_arm_prints_the_benchmark_metric():
+    """Rank 0 of the reference arm runs the reference PLASMA (oracle/_ref) and
+    prints the same metric string as the GPU arm, on the same workload."""
+    import bench
+    from oracle import ref
+    if not (os.path.exists(ref.LIB_PATH) or ref.available()):
+        pytest.skip("reference library not built here")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl",
+                        "reference", "--n", "512", "--steps", "1", "--warmup", "0"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference"
+    assert line["metric"] == bench.METRIC
+    assert line["cpu_baseline"]["kind"] == "reference"
+    assert line["info"] == 0 and line["iter"] >= 0
+    assert line["value"] > 0

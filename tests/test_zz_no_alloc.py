@@ -102,3 +102,37 @@ def test_noalloc_rejects_shapes(L):
     assert seq.status == pb.PlasmaErrorNotSupported
     L.plasma_desc_destroy(ctypes.byref(A))
     L.plasma_desc_destroy(ctypes.byref(B))
+
+
+def test_noalloc_allocates_nothing(L):
+    """The point of the entry point: the library's allocation counter does not
+    move across its calls, the first one at a size no call here has used
+    included (plasma_omp_dpotrs grows its workspace there)."""
+    n, nb = 2496, 192
+    assert L.plasma_set(pb.PlasmaNb, nb) == 0
+    a, b = gen.diag_dominant(n, 1, seed=4100)
+    f = np.asfortranarray(a.copy())
+    assert L.plasma_dpotrf(LO, n, f.ctypes.data, n) == 0
+    A, B = general_desc(L, n, n, nb), general_desc(L, n, 1, nb)
+    x = np.asfortranarray(b.copy())
+    seq, req = pb.new_sequence()
+    L.plasma_omp_dge2desc(f.ctypes.data, n, A, ctypes.byref(seq), ctypes.byref(req))
+    assert L.plasma_sequence_wait(ctypes.byref(seq)) == 0
+    try:
+        for _ in range(2):
+            seq, req = pb.new_sequence()
+            L.plasma_omp_dge2desc(x.ctypes.data, n, B, ctypes.byref(seq), ctypes.byref(req))
+            assert L.plasma_sequence_wait(ctypes.byref(seq)) == 0
+            before = L.plasma_device_allocations()
+            seq, req = pb.new_sequence()
+            L.plasma_omp_dpotrs_noalloc(LO, A, B, ctypes.byref(seq), ctypes.byref(req))
+            assert L.plasma_sequence_wait(ctypes.byref(seq)) == 0
+            assert L.plasma_device_allocations() == before
+            y = np.asfortranarray(np.zeros_like(b))
+            seq, req = pb.new_sequence()
+            L.plasma_omp_ddesc2ge(B, y.ctypes.data, n, ctypes.byref(seq), ctypes.byref(req))
+            assert L.plasma_sequence_wait(ctypes.byref(seq)) == 0
+            assert solve_residual(a, y, b) < TOL * EPS
+    finally:
+        L.plasma_desc_destroy(ctypes.byref(A))
+        L.plasma_desc_destroy(ctypes.byref(B))
