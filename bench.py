@@ -58,8 +58,13 @@ def parse():
                    help="band workload: comma-separated bandwidths")
     p.add_argument("--batch-count", type=int, default=4096,
                    help="matrices of the batched workload")
-    p.add_argument("--workload", default="dsposv", choices=["dsposv", "adjoint", "batched", "inverse",
-                                                     "band", "lu"],
+    p.add_argument("--kappas", default="1e2,1e5,1e8",
+                   help="mixed workload: condition numbers")
+    p.add_argument("--ns", default="8192,16384,32768", help="dposv workload: sizes")
+    p.add_argument("--nbs", default="128,256,384,512", help="dposv workload: tile sizes")
+    p.add_argument("--workload", default="dsposv",
+                   choices=["dsposv", "mixed", "dposv", "adjoint", "batched", "inverse",
+                            "band", "lu"],
                    help="dsposv: the headline; adjoint / batched: the differentiation "
                         "and batched-solve configurations, one JSON line each")
     return p.parse_args()
@@ -279,10 +284,14 @@ def run_reference(args):
     if dev == "cuda":
         torch.cuda.empty_cache()
     threads = os.cpu_count() or 1
+    # one untimed solve warms the host (each reference solve allocates and
+    # first-touches its own tile copies, so more warm-up changes nothing);
+    # a 20-second solve per step keeps the arm within minutes
+    warm = min(args.warmup, 1)
     secs, infos, iters = [], [], []
-    for i in range(args.warmup + args.steps):
+    for i in range(warm + args.steps):
         dt, info, it = reference_dsposv(a, b, nb, threads)
-        if i >= args.warmup:
+        if i >= warm:
             secs.append(dt)
             infos.append(info)
             iters.append(it)
@@ -292,7 +301,8 @@ def run_reference(args):
         "impl": "reference",
         "metric": METRIC,
         "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "warmup": warm, "warmup_requested": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic",
         "config": workload_config(args, nb),
@@ -622,8 +632,211 @@ def run_batched(args):
     return 0
 
 
+def _dsposv_cell(L, pb, A, B, X, xt, n, nrhs, mode, refine, steps, warmup):
+    """One (factor precision, refinement) cell on a device-resident system:
+    time of plasma_dsposv_ex (min over the timed solves, CUDA events), its
+    report, the backward error ||b - A x||_inf / (||A||_inf ||x||_inf) and
+    the forward error ||x - x_true||_inf / ||x_true||_inf."""
+    import torch
+    L.plasma_set(pb.PlasmaMixedPrecisionMode, MODES[mode])
+    L.plasma_set(pb.PlasmaRefinement, REFINE[refine])
+    it = ctypes.c_int()
+    info = pb.plasma_dsposv_info_t()
+    times, rc = [], 0
+    for rep in range(warmup + steps):
+        X.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        rc = L.plasma_dsposv_ex(pb.PlasmaLower, n, nrhs, A.data_ptr(), n, B.data_ptr(), n,
+                                X.data_ptr(), n, ctypes.byref(it), ctypes.byref(info))
+        e1.record()
+        torch.cuda.synchronize()
+        if rep >= warmup:
+            times.append(e0.elapsed_time(e1))
+    row = {"factor": mode, "refinement": refine, "info": rc, "iter": it.value,
+           "ms": min(times), "report": info.as_dict()}
+    if rc == 0:
+        Xc = X.T
+        R = B.T - A @ Xc
+        anorm = A.abs().sum(1).max().item()
+        row["backward_error"] = (R.abs().max(0).values /
+                                 (anorm * Xc.abs().max(0).values)).max().item()
+        row["forward_error"] = ((Xc - xt.T).abs().max(0).values /
+                                xt.T.abs().max(0).values).max().item()
+    return row
+
+
+def run_mixed(args):
+    """The mixed-precision configuration in full: kappa in {1e2, 1e5, 1e8} x
+    factor precision in {FP32 (three TF32 products), TF32, BF16}, each refined
+    by IR for kappa <= 1e5 and by GMRES-IR for kappa = 1e8, at n = --n
+    (32768), nrhs = 1, on device-resident operands.  Per cell: info, iter,
+    the report of plasma_dsposv_ex (factor precision used, attempts, GMRES
+    iterations, FP64 fallback), the time, the backward error and the forward
+    error against x_true; per kappa the plain FP64 dposv time on the same
+    matrix and its errors.  FP32 + IR is the reference's own configuration,
+    with its failure semantics: where its FP32 factorisation breaks down the
+    cell reports that info, as the reference does."""
+    import torch
+    import plasma_b200 as pb
+    L = pb.lib()
+    assert L.plasma_init() == 0
+    if args.nb > 0:
+        L.plasma_set(pb.PlasmaTuning, pb.PlasmaDisabled)
+        L.plasma_set(pb.PlasmaNb, args.nb)
+    n, nrhs = args.n, args.nrhs
+    out = {"workload": "mixed", "metric": "dsposv time and accuracy per kappa and "
+           "factor precision (vs plain FP64 dposv)", "n": n, "nrhs": nrhs, "unit": "ms",
+           "steps": args.steps, "warmup": args.warmup,
+           "backward_error_target": 50 * n * 2.0 ** -53, "results": []}
+    kappas = [float(k) for k in args.kappas.split(",")]
+    for kappa in kappas:
+        A, B, xt = make_system(n, nrhs, kappa, "cuda")
+        X = torch.zeros_like(B)
+        # plain FP64 dposv on a copy
+        Aw, Bw = A.clone(), B.clone()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        rc = L.plasma_dposv(pb.PlasmaLower, n, nrhs, Aw.data_ptr(), n, Bw.data_ptr(), n)
+        e1.record()
+        torch.cuda.synchronize()
+        Xd = Bw.T
+        anorm = A.abs().sum(1).max().item()
+        dposv = {"info": rc, "ms": e0.elapsed_time(e1),
+                 "backward_error": ((B.T - A @ Xd).abs().max(0).values /
+                                    (anorm * Xd.abs().max(0).values)).max().item(),
+                 "forward_error": ((Xd - xt.T).abs().max(0).values /
+                                   xt.T.abs().max(0).values).max().item()}
+        del Aw, Bw
+        refine = "gmres" if kappa >= 1e8 else "ir"
+        cells = []
+        for mode in ("fp32", "tf32", "bf16"):
+            cell = _dsposv_cell(L, pb, A, B, X, xt, n, nrhs, mode, refine, args.steps,
+                                args.warmup)
+            if cell["info"] == 0:
+                cell["speedup_vs_dposv"] = dposv["ms"] / cell["ms"]
+            cells.append(cell)
+        if kappa >= 1e8:
+            # the reference's own configuration on the same matrix
+            cells.append(_dsposv_cell(L, pb, A, B, X, xt, n, nrhs, "fp32", "ir", 1, 0))
+        out["results"].append({"kappa": kappa, "dposv": dposv, "cells": cells})
+        del A, B, X, xt
+        torch.cuda.empty_cache()
+    L.plasma_set(pb.PlasmaMixedPrecisionMode, MODES["fp32"])
+    L.plasma_set(pb.PlasmaRefinement, REFINE["ir"])
+    print(json.dumps(out), flush=True)
+    L.plasma_finalize()
+    return 0
+
+
+def make_diag_dominant(n, nrhs, seed, device):
+    """A = sym(U[-0.5, 0.5]) + n I, B = U[-1, 1] (n x nrhs column-major, held
+    as nrhs x n row-major), generated on the device."""
+    import torch
+    g = torch.Generator(device=device).manual_seed(seed)
+    A = torch.rand(n, n, generator=g, device=device, dtype=torch.float64) - 0.5
+    A = torch.tril(A) + torch.tril(A, -1).T
+    A.diagonal().add_(n)
+    B = torch.rand(nrhs, n, generator=g, device=device, dtype=torch.float64) * 2 - 1
+    return A.contiguous(), B.contiguous()
+
+
+def run_dposv(args):
+    """Plain FP64 plasma_dposv (the FP64 tensor-core path), n in --ns
+    (8192, 16384, 32768), nrhs = 16, A = sym(U[-0.5, 0.5]) + n I (seed 7),
+    device-resident, lower storage; nb over {128, 256, 384, 512} and the
+    library's tuned choice.  GFLOP/s = (n^3/3) / t (and the reference
+    tester's flops, potrf + potrs), as a fraction of the FP64 tensor peak
+    (cuBLAS DGEMM measured live).  --impl reference times the reference
+    PLASMA's plasma_dposv (oracle/_ref) on the host cores instead."""
+    import torch
+    ns = [int(v) for v in args.ns.split(",")]
+    nrhs = 16
+    out = {"workload": "dposv", "metric": "plain FP64 dposv GFLOP/s (n^3/3 / t), "
+           "fraction of FP64 tensor peak", "unit": "GFLOP/s", "nrhs": nrhs,
+           "steps": args.steps, "warmup": args.warmup, "results": []}
+    if args.impl == "reference":
+        threads = os.cpu_count() or 1
+        from oracle import ref
+        ref.set_threads(threads)
+        for n in ns:
+            A, B = make_diag_dominant(n, nrhs, 7, "cuda" if torch.cuda.is_available() else "cpu")
+            a, b = host_system(A, B)
+            del A, B
+            t = []
+            for rep in range(max(1, args.steps)):
+                x = b.copy(order="F")
+                af = a.copy(order="F")
+                t0 = time.perf_counter()
+                info = ref.dposv(ref.LOWER, af, x, 256)
+                t.append(time.perf_counter() - t0)
+                assert info == 0, info
+            ms = min(t) * 1e3
+            out["results"].append({"n": n, "nb": 256, "ms": ms,
+                                   "gflops": n ** 3 / 3 / ms / 1e6,
+                                   "cores": threads, "cpu": cpu_model()})
+        out["impl"] = "reference"
+        print(json.dumps(out), flush=True)
+        return 0
+    import plasma_b200 as pb
+    L = pb.lib()
+    assert L.plasma_init() == 0
+    peaks = measured_peaks(torch)
+    out["fp64_peak_tflops"] = peaks["fp64"]
+    for n in ns:
+        A, B = make_diag_dominant(n, nrhs, 7, "cuda")
+        Aw, Bw = torch.empty_like(A), torch.empty_like(B)
+        rows = []
+        for nb in [0] + [int(v) for v in args.nbs.split(",")]:
+            if nb == 0:
+                L.plasma_set(pb.PlasmaTuning, pb.PlasmaEnabled)
+            else:
+                L.plasma_set(pb.PlasmaTuning, pb.PlasmaDisabled)
+                L.plasma_set(pb.PlasmaNb, nb)
+            times = []
+            for rep in range(args.warmup + args.steps):
+                Aw.copy_(A)
+                Bw.copy_(B)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record()
+                rc = L.plasma_dposv(pb.PlasmaLower, n, nrhs, Aw.data_ptr(), n, Bw.data_ptr(), n)
+                e1.record()
+                torch.cuda.synchronize()
+                assert rc == 0, rc
+                if rep >= args.warmup:
+                    times.append(e0.elapsed_time(e1))
+            nbv = nb or L.plasma_tuning_get_potrf_nb(pb.PlasmaRealDouble, n)
+            Xd = Bw.T
+            R = B.T - A @ Xd
+            anorm = A.abs().sum(1).max().item()
+            res = (R.abs().max(0).values / (n * anorm * Xd.abs().max(0).values)).max().item()
+            ms = min(times)
+            rows.append({"nb": nbv, "tuned": nb == 0, "ms": ms,
+                         "gflops": n ** 3 / 3 / ms / 1e6,
+                         "tester_gflops": (n ** 3 / 3 + 2 * n * n * nrhs) / ms / 1e6,
+                         "frac_fp64_peak": n ** 3 / 3 / ms / 1e9 / peaks["fp64"],
+                         "tester_residual": res})
+        best = min(rows, key=lambda r: r["ms"])
+        out["results"].append({"n": n, "best": best, "all": rows})
+        del A, B, Aw, Bw
+        torch.cuda.empty_cache()
+    print(json.dumps(out), flush=True)
+    L.plasma_finalize()
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "mixed":
+        return run_mixed(args)
+    if args.workload == "dposv":
+        return run_dposv(args)
     if args.workload == "adjoint":
         return run_adjoint(args)
     if args.workload == "inverse":
@@ -770,6 +983,25 @@ def main():
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(n * nrhs * 8),
                "ms_per_step": ems, "host_memory": "page-locked"}
         del ah, bh, xh
+        # the same call on pageable host buffers (what a C caller passing
+        # malloc'd arrays gets)
+        ap = A.cpu()
+        bp = B.cpu()
+        xp = torch.zeros_like(bp)
+        pts = []
+        for _ in range(2):
+            g0 = torch.cuda.Event(enable_timing=True)
+            g1 = torch.cuda.Event(enable_timing=True)
+            g0.record()
+            rc = L.plasma_dsposv_ex(pb.PlasmaLower, n, nrhs, ap.data_ptr(), n, bp.data_ptr(),
+                                    n, xp.data_ptr(), n, ctypes.byref(it), None)
+            g1.record()
+            torch.cuda.synchronize()
+            assert rc == 0
+            pts.append(g0.elapsed_time(g1))
+        e2e["pageable"] = {"value": flops_of(n, nrhs) / min(pts) / 1e6,
+                           "ms_per_step": min(pts), "host_memory": "pageable"}
+        del ap, bp, xp
 
     cpu = None
     if not args.no_cpu and rank == 0:

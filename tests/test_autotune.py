@@ -40,7 +40,6 @@ def test_autotune_potrf_sets_table(L, tmp_path):
     # the LAPACK-layout solve uses the tuned nb and stays correct
     n = 2048
     a, b = gen.diag_dominant(n, 3, seed=77)
-    x = np.asfortranarray(b.copy())
-    assert L.plasma_dposv(pb.PlasmaLower, n, 3, np.asfortranarray(a.copy()).ctypes.data, n,
-                          x.ctypes.data, n) == 0
+    x, af = np.asfortranarray(b.copy()), np.asfortranarray(a.copy())
+    assert L.plasma_dposv(pb.PlasmaLower, n, 3, af.ctypes.data, n, x.ctypes.data, n) == 0
     assert solve_residual(a, x, b) < TOL * EPS

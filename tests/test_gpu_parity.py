@@ -201,9 +201,8 @@ def test_spotrf_sposv(L, n, nb):
         t = np.tril if uplo == LO else np.triu
         err = np.linalg.norm(t(f).astype(np.float64) - t(fo)) / np.linalg.norm(a)
         assert err < TOL * SEPS
-        x = b32.copy(order="F")
-        assert L.plasma_sposv(uplo, n, 3, a32.copy(order="F").ctypes.data, n,
-                              x.ctypes.data, n) == 0
+        x, af = b32.copy(order="F"), a32.copy(order="F")
+        assert L.plasma_sposv(uplo, n, 3, af.ctypes.data, n, x.ctypes.data, n) == 0
         assert solve_residual(a, x.astype(np.float64), b) < TOL * SEPS
 
 
@@ -281,8 +280,8 @@ def test_dsposv_sweep_block_sizes(L, n, nb):
     b = np.asfortranarray(np.random.default_rng(n).standard_normal((n, 1)))
     x = np.zeros((n, 1), order="F")
     it = ctypes.c_int(0)
-    assert L.plasma_dsposv(LO, n, 1, np.asfortranarray(a.copy()).ctypes.data, n,
-                           np.asfortranarray(b.copy()).ctypes.data, n,
+    af, bf = np.asfortranarray(a.copy()), np.asfortranarray(b.copy())
+    assert L.plasma_dsposv(LO, n, 1, af.ctypes.data, n, bf.ctypes.data, n,
                            x.ctypes.data, n, ctypes.byref(it)) == 0
     assert it.value >= 0
     assert solve_residual(a, x, b) < TOL * EPS
@@ -504,9 +503,8 @@ def test_single_rhs_sweeps(L, uplo, n, nb):
     (nb = 96); compare with the oracle."""
     set_nb(L, nb)
     a, b = gen.diag_dominant(n, 1, seed=1100 + n)
-    x = np.asfortranarray(b.copy())
-    assert L.plasma_dposv(uplo, n, 1, np.asfortranarray(a.copy()).ctypes.data, n,
-                          x.ctypes.data, n) == 0
+    x, af = np.asfortranarray(b.copy()), np.asfortranarray(a.copy())
+    assert L.plasma_dposv(uplo, n, 1, af.ctypes.data, n, x.ctypes.data, n) == 0
     xo = np.asfortranarray(b.copy())
     assert oracle.posv(uplo, np.asfortranarray(a.copy()), xo, nb) == 0
     np.testing.assert_allclose(x, xo, rtol=1e-12, atol=1e-15)
@@ -527,9 +525,9 @@ def test_dsposv_anorm_tile_pass(L, uplo, n, nb):
     x = np.zeros_like(b, order="F")
     it = ctypes.c_int()
     info = pb.plasma_dsposv_info_t()
-    assert L.plasma_dsposv_ex(uplo, n, 1, np.asfortranarray(a).ctypes.data, n,
-                              np.asfortranarray(b).ctypes.data, n, x.ctypes.data, n,
-                              ctypes.byref(it), ctypes.byref(info)) == 0
+    af, bf = np.asfortranarray(a), np.asfortranarray(b)
+    assert L.plasma_dsposv_ex(uplo, n, 1, af.ctypes.data, n, bf.ctypes.data, n,
+                              x.ctypes.data, n, ctypes.byref(it), ctypes.byref(info)) == 0
     ref = np.abs(a).sum(axis=1).max()
     assert abs(info.anorm - ref) <= 1e-13 * ref
     assert solve_residual(a, x, b) < TOL * EPS
@@ -542,9 +540,8 @@ def test_dposv_many_rhs(L, uplo):
     set_nb(L, 128)
     n, nrhs = 700, 100
     a, b = gen.diag_dominant(n, nrhs, seed=1700)
-    x = np.asfortranarray(b.copy())
-    assert L.plasma_dposv(uplo, n, nrhs, np.asfortranarray(a.copy()).ctypes.data, n,
-                          x.ctypes.data, n) == 0
+    x, af = np.asfortranarray(b.copy()), np.asfortranarray(a.copy())
+    assert L.plasma_dposv(uplo, n, nrhs, af.ctypes.data, n, x.ctypes.data, n) == 0
     assert solve_residual(a, x, b) < TOL * EPS
     xo = np.asfortranarray(b.copy())
     assert oracle.posv(uplo, np.asfortranarray(a.copy()), xo, 128) == 0
@@ -754,9 +751,8 @@ def test_reinit_and_solve_twice(L):
         assert L.plasma_set(pb.PlasmaDevice, 0) == 0
         assert L.plasma_init() == 0
         set_nb(L, 256)
-        x = np.asfortranarray(b.copy())
-        assert L.plasma_dposv(LO, n, 2, np.asfortranarray(a.copy()).ctypes.data, n,
-                              x.ctypes.data, n) == 0
+        x, af = np.asfortranarray(b.copy()), np.asfortranarray(a.copy())
+        assert L.plasma_dposv(LO, n, 2, af.ctypes.data, n, x.ctypes.data, n) == 0
         assert solve_residual(a, x, b) < TOL * EPS
         xs = np.zeros_like(b, order="F")
         it = ctypes.c_int()

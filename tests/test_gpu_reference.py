@@ -59,8 +59,9 @@ def close(x, xr, tol):
 def dsposv(L, uplo, a, b, fill=7.0):
     n, nrhs = b.shape
     x = F(np.full(b.shape, fill))
+    af, bf = F(a), F(b)                  # held until the call returns
     it = ctypes.c_int(-99)
-    info = L.plasma_dsposv(uplo, n, nrhs, F(a).ctypes.data, n, F(b).ctypes.data, n,
+    info = L.plasma_dsposv(uplo, n, nrhs, af.ctypes.data, n, bf.ctypes.data, n,
                            x.ctypes.data, n, ctypes.byref(it))
     return info, it.value, x
 
@@ -82,14 +83,14 @@ def test_factor_matches_reference(L, rg, key, n, nb, seed):
 def test_solves_match_reference(L, rg):
     set_nb(L, 256)
     a, b = gen.diag_dominant(2048, 1, seed=42)
-    x = F(b)
-    assert L.plasma_dposv(LO, 2048, 1, F(a).ctypes.data, 2048, x.ctypes.data, 2048) == 0
+    x, af = F(b), F(a)
+    assert L.plasma_dposv(LO, 2048, 1, af.ctypes.data, 2048, x.ctypes.data, 2048) == 0
     close(x, rg["cfg1_dposv_X"], 1e-13)
     set_nb(L, 128)
     a, b = gen.diag_dominant(1000, 3, seed=3000)
     for uplo, key in ((LO, "rag_dposv_X"), (UP, "rag_dposv_up_X")):
-        x = F(b)
-        assert L.plasma_dposv(uplo, 1000, 3, F(a).ctypes.data, 1000, x.ctypes.data, 1000) == 0
+        x, af = F(b), F(a)
+        assert L.plasma_dposv(uplo, 1000, 3, af.ctypes.data, 1000, x.ctypes.data, 1000) == 0
         close(x, rg[key], 1e-13)
     set_nb(L, 64)
     a, b = gen.diag_dominant(300, 4, seed=3001)
