@@ -149,6 +149,7 @@ static int gmres_correction(refine_t *R)
     double H[GMRES_RESTART + 1][GMRES_RESTART];
     double cs[GMRES_RESTART], sn[GMRES_RESTART], g[GMRES_RESTART + 1];
     double hcol[GMRES_RESTART + 1], hcol2[GMRES_RESTART + 1], y[GMRES_RESTART];
+    double gtrace[GMRES_RESTART];      /* |g_{j+1}|, the residual after step j */
 
     precond(R, R->r, R->z);
     double beta = sqrt(dot_host(R, R->z, R->z));
@@ -196,6 +197,11 @@ static int gmres_correction(refine_t *R)
         R->gmres_iters++;
         if (fabs(g[j + 1]) <= GMRES_TOL * beta || !(hn > 0.0))
             break;
+        /* a stagnating Krylov residual (less than 2x over the last 10
+         * steps): the preconditioner is too weak, end this solve early */
+        if (j >= 10 && fabs(g[j + 1]) > 0.5 * gtrace[j - 10])
+            break;
+        gtrace[j] = fabs(g[j + 1]);
     }
     /* back substitution H(0:k,0:k) y = g(0:k) */
     for (int i = k - 1; i >= 0; i--) {
@@ -211,12 +217,13 @@ static int gmres_correction(refine_t *R)
 /* Solves for the current b: initial x = M^{-1} b, then refinement until the
  * reference stopping rule holds.  Returns the number of refinement steps, or
  * -1 when it did not converge within ITERMAX. */
-static int refine_column(refine_t *R, int scheme, double cte, double *xn_out,
-                         double *rn_out, int *used_gmres, int *status)
+static int refine_column(refine_t *R, int scheme, double cte, int give_up,
+                         double *xn_out, double *rn_out, int *used_gmres, int *status)
 {
     precond(R, R->b, R->x);
     double prev = INFINITY;
     int gm = scheme == PlasmaRefineGMRES;
+    int stalls = 0;
     for (int it = 0; it <= ITERMAX; it++) {
         double xn, rn;
         residual_vec(R, &xn, &rn);
@@ -229,9 +236,23 @@ static int refine_column(refine_t *R, int scheme, double cte, double *xn_out,
             return it;
         if (it == ITERMAX)
             break;
-        /* automatic scheme: switch to GMRES-IR when IR stops contracting */
-        if (scheme == PlasmaRefineAuto && !gm && it > 0 && rn > 0.5 * prev)
+        /* give_up (the extended configurations): a factor that no longer
+         * contracts the residual -- IR: less than 2x per step, GMRES-IR: less
+         * than 10x per restarted solve, twice in a row, or a growing
+         * residual -- is abandoned for the next attempt instead of running
+         * out the 30 steps.  The reference's configuration always runs
+         * them (zcposv.c:485-518). */
+        /* automatic scheme: switch to GMRES-IR when IR stops contracting
+         * (before any giving up: GMRES gets its chance first) */
+        if (scheme == PlasmaRefineAuto && !gm && it > 0 && rn > 0.5 * prev) {
             gm = 1;
+            stalls = 0;
+        } else if (give_up && it > 0) {
+            const double need = gm ? 0.1 : 0.5;
+            stalls = (rn > need * prev) ? stalls + 1 : 0;
+            if (!(rn < prev) || stalls >= 2)
+                return -1;
+        }
         prev = rn;
         if (gm) {
             *used_gmres = 1;
@@ -409,8 +430,11 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
         if (plasma->refinement != PlasmaRefineIR)
             plan[nplan++] = (attempt_t){PlasmaFactorFP32, 1};
     } else {
+        /* TF32 / BF16 first, then FP32: a factor too coarse for the
+         * matrix's condition escalates to FP32 before the FP64 fallback */
         plan[nplan++] = (attempt_t){cfg, 0};
         plan[nplan++] = (attempt_t){cfg, 1};
+        plan[nplan++] = (attempt_t){PlasmaFactorFP32, 0};
     }
     const int scheme = plasma->refinement;
     /* the reference's configuration keeps the reference's failure semantics */
@@ -458,6 +482,11 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
 
     for (int a = 0; a < nplan && !converged; a++) {
         const int mode = plan[a].mode;
+        /* a scaled and shifted retry of the same precision answers a
+         * factorisation that broke down; after a factor that was computed
+         * but did not refine, the next precision is tried instead */
+        if (a > 0 && plan[a].scaled && plan[a - 1].mode == mode && !factor_failed)
+            continue;
         attempts++;
         if (rep) rep->factor_mode = mode;
         if (a > 0 && rep) cudaEventRecord(e0, S);
@@ -516,7 +545,8 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
             plasma_cuda_column(S, B, j, RF.b, 1);
             double xn = 0, rn = 0;
             int cstat = 0;
-            int it = refine_column(&RF, scheme, cte, &xn, &rn, &used_gmres, &cstat);
+            int it = refine_column(&RF, scheme, cte, !ref_failure, &xn, &rn, &used_gmres,
+                                   &cstat);
             Xnorm[j] = xn;
             Rnorm[j] = rn;
             if (cstat != 0 && ref_failure) {

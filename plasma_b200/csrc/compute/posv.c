@@ -38,12 +38,24 @@ void plasma_pXpotrs(plasma_context_t *plasma, plasma_enum_t uplo,
         return;
     }
     /* one right-hand side: B is a contiguous vector, solved by the
-     * one-launch sweeps; otherwise step-by-step tile sweeps */
+     * one-launch sweeps; up to 32: the multi-column one-launch sweeps, 16
+     * columns at a time; otherwise step-by-step tile sweeps */
     if (B.n == 1 && B.nt == 1 && B.i == 0 && B.j == 0 && B.gn == 1 &&
         plasma_sweep_reserve(plasma, A)) {
         plasma_cuda_trtri_blocks(plasma->stream, plasma->dstat, uplo, A, W);
         plasma_sweep(plasma, uplo, 0, A, W, B.matrix);
         plasma_sweep(plasma, uplo, 1, A, W, B.matrix);
+        return;
+    }
+    if (B.n >= 2 && B.n <= 32 && B.i == 0 && B.j == 0 && B.m == A.m &&
+        B.precision == A.precision && plasma_cuda_trsv_block(A) > 0 &&
+        plasma_sweep_reserve(plasma, A)) {
+        plasma_cuda_trtri_blocks(plasma->stream, plasma->dstat, uplo, A, W);
+        for (int c0 = 0; c0 < B.n; c0 += 16) {
+            const int nc = imin(16, B.n - c0);
+            plasma_sweep_rows(plasma, uplo, 0, A, W, B, c0, nc);
+            plasma_sweep_rows(plasma, uplo, 1, A, W, B, c0, nc);
+        }
         return;
     }
     plasma_cuda_trsm_sweep(plasma->stream, plasma->dstat, uplo, PlasmaNoTrans,
@@ -201,9 +213,15 @@ static int Xposv(plasma_enum_t prec, plasma_enum_t uplo, int n, int nrhs,
         plasma_tune_potrf(plasma, prec, n);
     int nb = plasma->nb;
 
+    /* an upper-stored matrix goes through lower tiles, as in Xpotrf; its
+     * host staging buffer keeps the untouched strictly lower part of the
+     * diagonal blocks for the way back, so B is converted before it and
+     * after it */
+    const int via_lower = uplo == PlasmaUpper;
     plasma_desc_t A, B;
     /* the tile copy of A lives in a slot the context keeps between calls */
-    int retval = plasma_desc_kept(plasma, PLASMA_SLOT_DESC_A, prec, uplo, nb, n, n, &A);
+    int retval = plasma_desc_kept(plasma, PLASMA_SLOT_DESC_A, prec,
+                                  via_lower ? PlasmaLower : uplo, nb, n, n, &A);
     if (retval != PlasmaSuccess)
         return retval;
     retval = plasma_desc_general_create(prec, nb, nb, n, nrhs, 0, 0, n, nrhs, &B);
@@ -214,11 +232,19 @@ static int Xposv(plasma_enum_t prec, plasma_enum_t uplo, int n, int nrhs,
     plasma_sequence_init(&sequence);
     plasma_request_init(&request);
 
-    plasma_omp_Xlapack2desc(pA, lda, A, uplo, &sequence, &request);
-    plasma_omp_Xlapack2desc(pB, ldb, B, PlasmaGeneral, &sequence, &request);
-    plasma_omp_Xposv(uplo, A, B, &sequence, &request);
+    if (via_lower) {
+        plasma_omp_Xlapack2desc(pB, ldb, B, PlasmaGeneral, &sequence, &request);
+        plasma_omp_Xlapack2desc_t(pA, lda, A, &sequence, &request);
+    } else {
+        plasma_omp_Xlapack2desc(pA, lda, A, uplo, &sequence, &request);
+        plasma_omp_Xlapack2desc(pB, ldb, B, PlasmaGeneral, &sequence, &request);
+    }
+    plasma_omp_Xposv(via_lower ? PlasmaLower : uplo, A, B, &sequence, &request);
     plasma_sequence_wait(&sequence);
-    plasma_omp_Xdesc2lapack(A, pA, lda, uplo, &sequence, &request);
+    if (via_lower)
+        plasma_omp_Xdesc2lapack_t(A, pA, lda, &sequence, &request);
+    else
+        plasma_omp_Xdesc2lapack(A, pA, lda, uplo, &sequence, &request);
     plasma_omp_Xdesc2lapack(B, pB, ldb, PlasmaGeneral, &sequence, &request);
     plasma_sequence_wait(&sequence);
 

@@ -90,9 +90,16 @@ static int Xpotrf(plasma_enum_t prec, plasma_enum_t uplo, int n, void *pA,
         plasma_tune_potrf(plasma, prec, n);
     int nb = plasma->nb;
 
+    /* An upper-stored matrix is factored through lower tiles: its tile
+     * copy holds U^T (the transpose of the stored triangle), the lower
+     * factor L of that copy is the transpose of the upper factor U, and it
+     * goes back transposed.  The trailing updates then run on the tensor
+     * cores, which take lower tiles. */
+    const int via_lower = uplo == PlasmaUpper;
     plasma_desc_t A;
     /* the tile copy lives in a slot the context keeps between calls */
-    int retval = plasma_desc_kept(plasma, PLASMA_SLOT_DESC_A, prec, uplo, nb, n, n, &A);
+    int retval = plasma_desc_kept(plasma, PLASMA_SLOT_DESC_A, prec,
+                                  via_lower ? PlasmaLower : uplo, nb, n, n, &A);
     if (retval != PlasmaSuccess) {
         plasma_error("tile copy of A failed");
         return retval;
@@ -102,12 +109,18 @@ static int Xpotrf(plasma_enum_t prec, plasma_enum_t uplo, int n, void *pA,
     plasma_sequence_init(&sequence);
     plasma_request_init(&request);
 
-    plasma_omp_Xlapack2desc(pA, lda, A, uplo, &sequence, &request);
-    plasma_omp_Xpotrf(uplo, A, &sequence, &request);
+    if (via_lower)
+        plasma_omp_Xlapack2desc_t(pA, lda, A, &sequence, &request);
+    else
+        plasma_omp_Xlapack2desc(pA, lda, A, uplo, &sequence, &request);
+    plasma_omp_Xpotrf(via_lower ? PlasmaLower : uplo, A, &sequence, &request);
     /* After a failure the reference's desc2tr tasks see the failed sequence
      * and skip, leaving pA as it was; waiting here makes that exact. */
     plasma_sequence_wait(&sequence);
-    plasma_omp_Xdesc2lapack(A, pA, lda, uplo, &sequence, &request);
+    if (via_lower)
+        plasma_omp_Xdesc2lapack_t(A, pA, lda, &sequence, &request);
+    else
+        plasma_omp_Xdesc2lapack(A, pA, lda, uplo, &sequence, &request);
     plasma_sequence_wait(&sequence);
     return sequence.status;
 }

@@ -135,6 +135,61 @@ void plasma_omp_Xdesc2lapack(plasma_desc_t A, void *pA, int lda,
     cudaStreamSynchronize(plasma->stream);
 }
 
+/* The upper triangle of the column-major pA into the lower descriptor A,
+ * transposed (A = U^T), and back: the LAPACK-layout drivers factor an
+ * upper-stored matrix through lower tiles.  Host arrays are staged through
+ * the device buffer (upper triangle only). */
+void plasma_omp_Xlapack2desc_t(const void *pA, int lda, plasma_desc_t A,
+                               plasma_sequence_t *sequence, plasma_request_t *request)
+{
+    plasma_context_t *plasma = plasma_context_self();
+    if (!check_xfer(plasma, pA, lda, A, sequence, request))
+        return;
+    if (A.m == 0 || A.n == 0)
+        return;
+    size_t elem = plasma_element_size(A.precision);
+    const void *src = pA;
+    int ld = lda;
+    if (!plasma_is_device_pointer(pA)) {
+        ld = A.m;
+        void *buf = plasma_scratch(plasma, PLASMA_SLOT_STAGING,
+                                   (size_t)ld * (size_t)A.n * elem);
+        if (buf == NULL) {
+            plasma_request_fail(sequence, request, PlasmaErrorOutOfMemory);
+            return;
+        }
+        copy_region(plasma, buf, (size_t)ld, pA, (size_t)lda, A.m, A.n, A.nb,
+                    PlasmaUpper, elem, cudaMemcpyHostToDevice);
+        src = buf;
+    }
+    plasma_cuda_lapack_to_tile_t(plasma->stream, plasma->dstat, A, src, ld);
+}
+
+void plasma_omp_Xdesc2lapack_t(plasma_desc_t A, void *pA, int lda,
+                               plasma_sequence_t *sequence, plasma_request_t *request)
+{
+    plasma_context_t *plasma = plasma_context_self();
+    if (!check_xfer(plasma, pA, lda, A, sequence, request))
+        return;
+    if (A.m == 0 || A.n == 0)
+        return;
+    if (plasma_is_device_pointer(pA)) {
+        plasma_cuda_tile_to_lapack_t(plasma->stream, plasma->dstat, A, pA, lda);
+        return;
+    }
+    size_t elem = plasma_element_size(A.precision);
+    int ld = A.m;
+    void *buf = plasma_scratch(plasma, PLASMA_SLOT_STAGING, (size_t)ld * (size_t)A.n * elem);
+    if (buf == NULL) {
+        plasma_request_fail(sequence, request, PlasmaErrorOutOfMemory);
+        return;
+    }
+    plasma_cuda_tile_to_lapack_t(plasma->stream, plasma->dstat, A, buf, ld);
+    copy_region(plasma, pA, (size_t)lda, buf, (size_t)ld, A.m, A.n, A.nb, PlasmaUpper, elem,
+                cudaMemcpyDeviceToHost);
+    cudaStreamSynchronize(plasma->stream);
+}
+
 void plasma_omp_dge2desc(double *pA, int lda, plasma_desc_t A,
                          plasma_sequence_t *sequence, plasma_request_t *request)
 {

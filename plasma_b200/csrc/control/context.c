@@ -429,6 +429,19 @@ int plasma_sweep(plasma_context_t *c, plasma_enum_t uplo, int backward,
                             c->sweep_sync, c->sweep_epoch, c->num_sms);
 }
 
+/* The multi-column one-launch sweep (up to 16 columns of the tile matrix B)
+ * with the context's ready flags and a fresh epoch; 0 when not launched. */
+int plasma_sweep_rows(plasma_context_t *c, plasma_enum_t uplo, int backward,
+                      plasma_desc_t A, const void *W, plasma_desc_t B, int c0, int ncols)
+{
+    if (!plasma_sweep_reserve(c, A))
+        return 0;
+    if (++c->sweep_epoch <= 0)
+        c->sweep_epoch = 1;
+    return plasma_cuda_trsm_rows(c->stream, c->dstat, uplo, backward, A, W, B, c0, ncols,
+                                 c->sweep_sync, c->sweep_epoch, c->num_sms);
+}
+
 /* A descriptor over a scratch slot that the context keeps between calls
  * (the LAPACK-layout drivers' tile copies): no allocation once the slot is
  * large enough, storage zeroed on the context stream.  type = PlasmaGeneral

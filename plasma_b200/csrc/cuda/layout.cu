@@ -210,6 +210,63 @@ k_tile_copy_t(plasma_desc_t A, plasma_desc_t B, plasma_devstat_t *st, int call)
         plasma_fail(st, 1, call);
 }
 
+// The lower tiles of B (m >= n) <-> the upper triangle of the column-major
+// array pA, transposed: tile (m,n) element (i,j) is pA(r, c) with
+// r = n*nb + j <= c = m*nb + i, i.e. B holds U^T = L when pA holds the
+// upper triangle U of a symmetric matrix.  Used for upper storage, whose
+// factor is the transpose of the lower one, so that the tensor-core tile
+// kernels (written for lower tiles) factor it.  32 x 32 blocks go through
+// shared memory so that both sides are read and written along their
+// columns.  The strictly upper part of a diagonal tile (the strictly lower
+// part of pA) is zero on the way in and not written on the way out.
+template <typename T, bool TO_TILE>
+__global__ void __launch_bounds__(kThreads)
+k_lapack_tile_t(plasma_desc_t B, T *pA, int lda, const plasma_devstat_t *st)
+{
+    __shared__ T blk[32][33];
+    const int m = blockIdx.x, n = blockIdx.y;
+    if (m < n || __syncthreads_or(plasma_failed(st))) return;
+    T *tile = (T *)plasma_tile_addr(B, m, n);
+    const int ldt = plasma_tile_mmain(B, m);
+    const int rows = plasma_tile_mview(B, m), cols = plasma_tile_nview(B, n);
+    // pA(n*nb + j, m*nb + i) = f[j + i*lda]
+    T *f = pA + (size_t)B.mb * m * lda + (size_t)B.nb * n;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const bool diag = m == n;
+    for (int i0 = 0; i0 < rows; i0 += 32)
+        for (int j0 = 0; j0 < cols; j0 += 32) {
+            __syncthreads();
+            if (TO_TILE) {
+                // read along pA's columns: j = j0 + tx contiguous
+                for (int q = ty; q < 32; q += kThreads / 32) {
+                    const int j = j0 + tx, i = i0 + q;
+                    T v = T(0);
+                    if (j < cols && i < rows && (!diag || i >= j))
+                        v = f[(size_t)i * lda + j];
+                    blk[q][tx] = v;                    // blk[i - i0][j - j0]
+                }
+                __syncthreads();
+                for (int q = ty; q < 32; q += kThreads / 32) {
+                    const int i = i0 + tx, j = j0 + q;
+                    if (i < rows && j < cols)
+                        tile[(size_t)j * ldt + i] = blk[tx][q];
+                }
+            } else {
+                // read along the tile's columns: i = i0 + tx contiguous
+                for (int q = ty; q < 32; q += kThreads / 32) {
+                    const int i = i0 + tx, j = j0 + q;
+                    blk[q][tx] = (i < rows && j < cols) ? tile[(size_t)j * ldt + i] : T(0);
+                }
+                __syncthreads();                       // blk[j - j0][i - i0]
+                for (int q = ty; q < 32; q += kThreads / 32) {
+                    const int j = j0 + tx, i = i0 + q;
+                    if (j < cols && i < rows && (!diag || i >= j))
+                        f[(size_t)i * lda + j] = blk[tx][q];
+                }
+            }
+        }
+}
+
 // X(m,n) += R(m,n)  (reference compute/pzgeadd.c:28-73 with alpha = beta = 1)
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
@@ -311,7 +368,36 @@ extern "C" void plasma_cuda_tile_to_lapack(cudaStream_t s, plasma_devstat_t *st,
             A, uplo, (float *)pA, lda, 0, st);
 }
 
-// Band descriptors of lower or upper storage (A.uplo); the caller checks
+// The upper triangle of the column-major pA <-> the lower tiles of B,
+// transposed (k_lapack_tile_t); B is a lower (packed or general) descriptor
+// of square tiles with B.i = B.j = 0.
+extern "C" void plasma_cuda_lapack_to_tile_t(cudaStream_t s, plasma_devstat_t *st,
+                                             plasma_desc_t B, const void *pA, int lda)
+{
+    if (B.mt == 0 || B.nt == 0) return;
+    PLASMA_COUNT_LAUNCH();
+    if (B.precision == PlasmaRealDouble)
+        k_lapack_tile_t<double, true><<<tile_grid(B), kThreads, 0, s>>>(
+            B, (double *)pA, lda, st);
+    else
+        k_lapack_tile_t<float, true><<<tile_grid(B), kThreads, 0, s>>>(
+            B, (float *)pA, lda, st);
+}
+
+extern "C" void plasma_cuda_tile_to_lapack_t(cudaStream_t s, plasma_devstat_t *st,
+                                             plasma_desc_t B, void *pA, int lda)
+{
+    if (B.mt == 0 || B.nt == 0) return;
+    PLASMA_COUNT_LAUNCH();
+    if (B.precision == PlasmaRealDouble)
+        k_lapack_tile_t<double, false><<<tile_grid(B), kThreads, 0, s>>>(
+            B, (double *)pA, lda, st);
+    else
+        k_lapack_tile_t<float, false><<<tile_grid(B), kThreads, 0, s>>>(
+            B, (float *)pA, lda, st);
+}
+
+// Band descriptors of lower or upper storage (A.uplo); the caller checks// Band descriptors of lower or upper storage (A.uplo); the caller checks
 // ldab >= kl+1 (lower) or ku+1 (upper).
 extern "C" void plasma_cuda_band_to_tile(cudaStream_t s, plasma_devstat_t *st,
                                          plasma_desc_t A, const void *pAB, int ldab)

@@ -66,6 +66,15 @@ __device__ __forceinline__ void cp_async_el_any(T *dst, const T *src)
     else cp_async_4(dst, src, true);
 }
 
+// as above; valid = false writes zero and reads nothing (src must still be
+// a global address)
+template <typename T>
+__device__ __forceinline__ void cp_async_el_any_z(T *dst, const T *src, bool valid)
+{
+    if (sizeof(T) == 8) cp_async_8(dst, src, valid);
+    else cp_async_4(dst, src, valid);
+}
+
 // Logical block (bi, bj) of L, SB x SB: element (i,j) at p[i*si + j*sj].
 template <typename T>
 struct LBlock {
@@ -328,6 +337,195 @@ k_trtri_blocks(plasma_desc_t A, int uplo, T *W, const plasma_devstat_t *st)
         }
         __syncthreads();
     }
+}
+
+// ---------------------------------------------------------------------------
+// One-launch sweeps for a few right-hand sides (potrs / posv with
+// 2 <= nrhs <= 32; the reference runs them as the tile tasks of pztrsm.c):
+// the ticketed row blocks of k_trsv, each applied to NR columns of B at
+// once, so the factor is read once per NR columns instead of once per
+// column, and B stays in its tile layout.
+//   forward : X_u = W_u   (B_u - sum_{k<u} L(u,k) X_k)
+//   backward: X_u = W_u^T (B_u - sum_{k>u} L(k,u)^T X_k)
+// Block u streams the operator blocks of the earlier tickets through a
+// two-deep cp.async ring in shared memory, stored as Ms[c*(SB+1) + i] =
+// M(i,c) whatever the storage order of L (the global reads are coalesced
+// along whichever index is contiguous).  Thread (i, h) owns row i and the
+// h-th share of the columns c of the operator and keeps its NR partial sums
+// in registers across all blocks k; the shares meet in shared memory once,
+// before the diagonal block.  Solution blocks of other CTAs are read
+// through L2 (ld.global.cg) after their ready flag.
+// ---------------------------------------------------------------------------
+constexpr int TR_THREADS = 256;
+
+template <typename T, int SB, int NR>
+constexpr int trsm_rows_smem()
+{
+    return (2 * SB * (SB + 1) + SB * NR + (TR_THREADS / SB) * SB * NR) * (int)sizeof(T);
+}
+
+template <typename T>
+__device__ __forceinline__ T *b_elem(const plasma_desc_t &B, int row, int col)
+{
+    const int m = row / B.mb, r = row - m * B.mb;
+    const int t = col / B.nb, c = col - t * B.nb;
+    return (T *)plasma_tile_addr(B, m, t) + (size_t)c * plasma_tile_mmain(B, m) + r;
+}
+
+// Ms[c*(SB+1) + i] <- q[i*mi + c*mc] for i < ri, c < rc, zero elsewhere
+template <typename T, int SB>
+__device__ __forceinline__ void stage_op(T *Ms, const T *q, int mi, int mc, int ri, int rc,
+                                         int tid)
+{
+    constexpr int LDM = SB + 1;
+    if (mi == 1) {
+        for (int e = tid; e < SB * SB; e += TR_THREADS) {
+            const int i = e % SB, c = e / SB;
+            const bool v = i < ri && c < rc;
+            cp_async_el_any_z(Ms + c * LDM + i, v ? q + (size_t)i + (size_t)c * mc : q, v);
+        }
+    } else {
+        for (int e = tid; e < SB * SB; e += TR_THREADS) {
+            const int c = e % SB, i = e / SB;
+            const bool v = i < ri && c < rc;
+            cp_async_el_any_z(Ms + c * LDM + i, v ? q + (size_t)i * mi + (size_t)c : q, v);
+        }
+    }
+}
+
+template <typename T, int SB, int NR>
+__global__ void __launch_bounds__(TR_THREADS, 1)
+k_trsm_rows(plasma_desc_t A, int uplo, int backward, const T *W, plasma_desc_t B,
+            int c0, int ncols, SweepSync *sy, int epoch, plasma_devstat_t *st)
+{
+    constexpr int LDM = SB + 1;
+    constexpr int SH = TR_THREADS / SB;      // column shares
+    constexpr int CS = SB / SH;              // columns of the operator per share
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *Ms[2] = {reinterpret_cast<T *>(smem_raw),
+                reinterpret_cast<T *>(smem_raw) + SB * LDM};
+    T *Xs = Ms[1] + SB * LDM;                // [SB][NR]
+    T *red = Xs + SB * NR;                   // [SH][SB][NR]
+    __shared__ int blk_s, ok_s;
+    if (plasma_failed(st)) return;
+    const int n = A.m;
+    const int nblk = (n + SB - 1) / SB;
+    const int tid = threadIdx.x;
+    const int i = tid % SB, h = tid / SB;
+    const bool lower = uplo == PlasmaLower;
+
+    for (;;) {
+        if (tid == 0) blk_s = atomicAdd(&sy->ticket, 1);
+        __syncthreads();
+        const int t = blk_s;
+        __syncthreads();
+        if (t >= nblk) break;
+        const int u = backward ? nblk - 1 - t : t;
+        const int rows = min(SB, n - u * SB);
+
+        // operator of ticket s: forward L(u,k), backward L(k,u)^T
+        auto stage = [&](int s, T *buf) {
+            const int k = backward ? nblk - 1 - s : s;
+            const int kr = min(SB, n - k * SB);
+            if (!backward) {
+                LBlock<T> b = lblock<T, SB>(A, lower, u, k);
+                stage_op<T, SB>(buf, b.p, b.si, b.sj, rows, kr, tid);
+            } else {
+                LBlock<T> b = lblock<T, SB>(A, lower, k, u);
+                stage_op<T, SB>(buf, b.p, b.sj, b.si, rows, kr, tid);
+            }
+        };
+        T acc[NR];
+#pragma unroll
+        for (int j = 0; j < NR; j++) acc[j] = T(0);
+        if (t > 0) stage(0, Ms[0]);
+        cp_async_commit();
+        for (int s = 0; s < t; s++) {
+            const int k = backward ? nblk - 1 - s : s;
+            const int kr = min(SB, n - k * SB);
+            if (s + 1 < t) stage(s + 1, Ms[(s + 1) & 1]);
+            cp_async_commit();
+            if (tid == 0) {
+                ok_s = wait_block(sy, k, epoch) ? 1 : 0;
+                if (!ok_s) plasma_fail(st, PlasmaErrorInternal, 0);
+            }
+            __syncthreads();
+            if (!ok_s) {
+                cp_async_wait<0>();
+                return;
+            }
+            for (int e = tid; e < SB * NR; e += TR_THREADS) {
+                const int r = e / NR, j = e - (e / NR) * NR;
+                Xs[e] = (r < kr && j < ncols) ? __ldcg(b_elem<T>(B, k * SB + r, c0 + j)) : T(0);
+            }
+            cp_async_wait<1>();
+            __syncthreads();
+            const T *Mb = Ms[s & 1];
+#pragma unroll 4
+            for (int c = h * CS; c < (h + 1) * CS; c++) {
+                const T m = Mb[c * LDM + i];
+#pragma unroll
+                for (int j = 0; j < NR; j++) acc[j] += m * Xs[c * NR + j];
+            }
+            __syncthreads();
+        }
+        cp_async_wait<0>();
+        // the diagonal block's operator: W_u (forward) or W_u^T (backward)
+        const T *wu = W + (size_t)u * SB * SB;
+        if (!backward) stage_op<T, SB>(Ms[0], wu, 1, SB, SB, SB, tid);
+        else stage_op<T, SB>(Ms[0], wu, SB, 1, SB, SB, tid);
+        cp_async_commit();
+#pragma unroll
+        for (int j = 0; j < NR; j++) red[(h * SB + i) * NR + j] = acc[j];
+        __syncthreads();
+        for (int e = tid; e < SB * NR; e += TR_THREADS) {
+            const int r = e / NR, j = e - (e / NR) * NR;
+            T v = (r < rows && j < ncols) ? *b_elem<T>(B, u * SB + r, c0 + j) : T(0);
+#pragma unroll
+            for (int q = 0; q < SH; q++) v -= red[(q * SB + r) * NR + j];
+            Xs[e] = v;
+        }
+        cp_async_wait<0>();
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < NR; j++) acc[j] = T(0);
+#pragma unroll 4
+        for (int c = h * CS; c < (h + 1) * CS; c++) {
+            const T m = Ms[0][c * LDM + i];
+#pragma unroll
+            for (int j = 0; j < NR; j++) acc[j] += m * Xs[c * NR + j];
+        }
+#pragma unroll
+        for (int j = 0; j < NR; j++) red[(h * SB + i) * NR + j] = acc[j];
+        __syncthreads();
+        for (int e = tid; e < SB * NR; e += TR_THREADS) {
+            const int r = e / NR, j = e - (e / NR) * NR;
+            if (r < rows && j < ncols) {
+                T v = T(0);
+#pragma unroll
+                for (int q = 0; q < SH; q++) v += red[(q * SB + r) * NR + j];
+                *b_elem<T>(B, u * SB + r, c0 + j) = v;
+            }
+        }
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) st_release(&sy->flags[u], epoch);
+    }
+}
+
+template <typename T, int SB, int NR>
+void launch_trsm_rows(cudaStream_t s, plasma_devstat_t *st, int uplo, int backward,
+                      const plasma_desc_t &A, const void *W, const plasma_desc_t &B, int c0,
+                      int ncols, SweepSync *sy, int epoch, int grid)
+{
+    static unsigned long long attr = 0;
+    if (plasma_first_on_device(&attr)) {
+        cudaFuncSetAttribute(k_trsm_rows<T, SB, NR>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             trsm_rows_smem<T, SB, NR>());
+    }
+    k_trsm_rows<T, SB, NR><<<grid, TR_THREADS, trsm_rows_smem<T, SB, NR>(), s>>>(
+        A, uplo, backward, (const T *)W, B, c0, ncols, sy, epoch, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -929,5 +1127,53 @@ extern "C" int plasma_cuda_trsv(cudaStream_t s, plasma_devstat_t *st,
         launch_trsv<float, 64>(s, st, uplo, backward, A, W, vec, sy, epoch, grid);
     double n = A.m, es = plasma_element_size(A.precision);
     plasma_prof_end(prof, s, PLASMA_KCLASS_SOLVE, n * n, es * n * n / 2.0);
+    return 1;
+}
+
+// In-place solve of op(L) X = B(:, c0 .. c0+ncols-1) for up to 16 columns of
+// a tile matrix B (B.i = B.j = 0), the one-launch multi-column sweep
+// (k_trsm_rows); W, sync and epoch as for plasma_cuda_trsv.  Returns 0
+// (nothing launched) when the factor's tiles admit no block sweep.
+extern "C" int plasma_cuda_trsm_rows(cudaStream_t s, plasma_devstat_t *st,
+                                     plasma_enum_t uplo, int backward, plasma_desc_t A,
+                                     const void *W, plasma_desc_t B, int c0, int ncols,
+                                     void *sync, int epoch, int num_sms)
+{
+    const int sb = plasma_cuda_trsv_block(A);
+    if (sb == 0 || B.i != 0 || B.j != 0 || B.precision != A.precision || B.m != A.m ||
+        ncols < 1 || ncols > 16 || c0 < 0 || c0 + ncols > B.n)
+        return 0;
+    const int nblk = (A.m + sb - 1) / sb;
+    if (nblk == 0) return 1;
+    SweepSync *sy = (SweepSync *)sync;
+    cudaMemsetAsync(&sy->ticket, 0, 2 * sizeof(int), s);
+    const int grid = nblk < num_sms ? nblk : num_sms;
+    PLASMA_COUNT_LAUNCH();
+    int prof = plasma_prof_begin(s);
+    if (A.precision == PlasmaRealDouble) {
+        if (ncols <= 4)
+            launch_trsm_rows<double, 64, 4>(s, st, uplo, backward, A, W, B, c0, ncols, sy,
+                                            epoch, grid);
+        else
+            launch_trsm_rows<double, 64, 16>(s, st, uplo, backward, A, W, B, c0, ncols, sy,
+                                             epoch, grid);
+    } else if (sb == 128) {
+        if (ncols <= 4)
+            launch_trsm_rows<float, 128, 4>(s, st, uplo, backward, A, W, B, c0, ncols, sy,
+                                            epoch, grid);
+        else
+            launch_trsm_rows<float, 128, 16>(s, st, uplo, backward, A, W, B, c0, ncols, sy,
+                                             epoch, grid);
+    } else {
+        if (ncols <= 4)
+            launch_trsm_rows<float, 64, 4>(s, st, uplo, backward, A, W, B, c0, ncols, sy,
+                                           epoch, grid);
+        else
+            launch_trsm_rows<float, 64, 16>(s, st, uplo, backward, A, W, B, c0, ncols, sy,
+                                            epoch, grid);
+    }
+    double n = A.m, es = plasma_element_size(A.precision);
+    plasma_prof_end(prof, s, PLASMA_KCLASS_SOLVE, n * n * ncols,
+                    es * (n * n / 2.0 + 2.0 * n * ncols));
     return 1;
 }

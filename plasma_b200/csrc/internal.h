@@ -146,6 +146,18 @@ void plasma_cuda_lapack_to_tile(cudaStream_t s, plasma_devstat_t *st,
 void plasma_cuda_tile_to_lapack(cudaStream_t s, plasma_devstat_t *st,
                                 plasma_desc_t A, plasma_enum_t uplo,
                                 void *pA, int lda);
+/* The upper triangle of the column-major pA <-> the lower tiles of B,
+ * transposed (an upper-stored matrix factored through lower tiles). */
+void plasma_cuda_lapack_to_tile_t(cudaStream_t s, plasma_devstat_t *st,
+                                  plasma_desc_t B, const void *pA, int lda);
+void plasma_cuda_tile_to_lapack_t(cudaStream_t s, plasma_devstat_t *st,
+                                  plasma_desc_t B, void *pA, int lda);
+/* LAPACK-layout <-> tile conversions of an upper-stored array through lower
+ * tiles (compute/transfer.c) */
+void plasma_omp_Xlapack2desc_t(const void *pA, int lda, plasma_desc_t A,
+                               plasma_sequence_t *sequence, plasma_request_t *request);
+void plasma_omp_Xdesc2lapack_t(plasma_desc_t A, void *pA, int lda,
+                               plasma_sequence_t *sequence, plasma_request_t *request);
 /* LAPACK band storage (ldab >= kd+1) <-> band tile descriptor of lower or
  * upper storage (reference compute/pzpb2desc.c, pzdesc2pb.c). */
 void plasma_cuda_band_to_tile(cudaStream_t s, plasma_devstat_t *st,
@@ -306,6 +318,9 @@ void plasma_cuda_trtri_blocks(cudaStream_t s, plasma_devstat_t *st,
 int plasma_cuda_trsv(cudaStream_t s, plasma_devstat_t *st, plasma_enum_t uplo,
                      int backward, plasma_desc_t A, const void *W, void *vec,
                      void *sync, int epoch, int num_sms);
+int plasma_cuda_trsm_rows(cudaStream_t s, plasma_devstat_t *st, plasma_enum_t uplo,
+                          int backward, plasma_desc_t A, const void *W, plasma_desc_t B,
+                          int c0, int ncols, void *sync, int epoch, int num_sms);
 size_t plasma_cuda_dots_work(int nv);
 void plasma_cuda_dots(cudaStream_t s, const double *V, size_t ldv, int nv,
                       const double *w, size_t n, double *out, double *work);
@@ -331,6 +346,8 @@ void plasma_cuda_column(cudaStream_t s, plasma_desc_t D, int j, void *v,
 /* One-launch sweep with the context's ready-flag buffer (W from
  * plasma_cuda_trtri_blocks); returns 0 when the factor is not eligible. */
 int plasma_sweep_reserve(plasma_context_t *plasma, plasma_desc_t A);
+int plasma_sweep_rows(plasma_context_t *plasma, plasma_enum_t uplo, int backward,
+                      plasma_desc_t A, const void *W, plasma_desc_t B, int c0, int ncols);
 int plasma_desc_kept(plasma_context_t *c, int slot, plasma_enum_t precision,
                      plasma_enum_t type, int nb, int m, int n, plasma_desc_t *A);
 int plasma_sweep(plasma_context_t *plasma, plasma_enum_t uplo, int backward,

@@ -494,6 +494,87 @@ def test_gmres_ir_ill_conditioned(L, mode, refine):
         L.plasma_set(pb.PlasmaRefinement, pb.PlasmaRefineIR)
 
 
+def _errors(a, x, xt):
+    """Normwise backward error ||b - A x||_inf / (||A||_inf ||x||_inf) with
+    b = A x_true, and forward error ||x - x_true||_inf / ||x_true||_inf."""
+    r = a @ xt - a @ x
+    be = np.abs(r).max() / (np.abs(a).sum(axis=1).max() * np.abs(x).max())
+    fe = np.abs(x - xt).max() / np.abs(xt).max()
+    return be, fe
+
+
+@pytest.mark.parametrize("mode", [pb.PlasmaFactorFP32, pb.PlasmaFactorTF32,
+                                  pb.PlasmaFactorBF16, pb.PlasmaFactorAuto])
+@pytest.mark.parametrize("refine", [pb.PlasmaRefineGMRES, pb.PlasmaRefineAuto])
+def test_gmres_ir_kappa_1e8(L, mode, refine):
+    """kappa = 1e8, the condition GMRES-IR is there for: the FP32 factor
+    preconditions GMRES to the FP64 stopping rule without the FP64 fallback;
+    a TF32 / BF16 factor that cannot get there escalates to FP32 (the report
+    says which precision answered).  Backward error <= 50 n eps, forward
+    error <= kappa * 1e-14."""
+    set_nb(L, 256)
+    L.plasma_set(pb.PlasmaMixedPrecisionMode, mode)
+    L.plasma_set(pb.PlasmaRefinement, refine)
+    try:
+        n, kappa = 2048, 1e8
+        a = gen.spectrum(n, kappa, seed=11)
+        xt = np.random.default_rng(12).standard_normal((n, 1))
+        b = np.asfortranarray(a @ xt)
+        rc, it, x, info = dsposv_ex(L, LO, a, b)
+        assert rc == 0
+        assert it >= 0 and info.fallback_fp64 == 0, (it, info.as_dict())
+        assert info.refinement == pb.PlasmaRefineGMRES and info.gmres_iterations > 0
+        if mode == pb.PlasmaFactorFP32:
+            assert info.factor_mode == pb.PlasmaFactorFP32 and info.attempts == 1
+        be, fe = _errors(a, x, xt)
+        assert be <= 50 * n * EPS, be
+        assert fe <= kappa * 1e-14, fe
+    finally:
+        L.plasma_set(pb.PlasmaMixedPrecisionMode, pb.PlasmaFactorFP32)
+        L.plasma_set(pb.PlasmaRefinement, pb.PlasmaRefineIR)
+
+
+def test_gmres_ir_kappa_1e8_fixture(L, golden):
+    """n = 256, kappa = 1e8 (the spec8 fixture): FP32 factor + GMRES-IR
+    against LAPACK's FP64 dposv answer and x_true."""
+    set_nb(L, 64)
+    L.plasma_set(pb.PlasmaRefinement, pb.PlasmaRefineGMRES)
+    try:
+        n, kappa = 256, 1e8
+        a = gen.spectrum(n, kappa, seed=11)
+        xt = golden["spec8_xtrue"]
+        b = np.asfortranarray(a @ xt)
+        rc, it, x, info = dsposv_ex(L, LO, a, b)
+        assert rc == 0 and it >= 0 and info.fallback_fp64 == 0
+        be, fe = _errors(a, x, xt)
+        assert be <= 50 * n * EPS
+        assert fe <= kappa * 1e-14
+        xl = golden["spec8_X"]
+        assert np.abs(x - xl).max() / np.abs(xl).max() <= kappa * 1e-14
+    finally:
+        L.plasma_set(pb.PlasmaRefinement, pb.PlasmaRefineIR)
+
+
+@pytest.mark.parametrize("mode", [pb.PlasmaFactorTF32, pb.PlasmaFactorBF16])
+def test_ir_stall_escalates_to_fp32(L, mode):
+    """kappa = 1e5 with classical IR: a TF32 / BF16 factor does not contract
+    the residual; instead of running out 30 steps and the FP64 fallback the
+    solver escalates to the FP32 factor, which refines (iter >= 0)."""
+    set_nb(L, 256)
+    L.plasma_set(pb.PlasmaMixedPrecisionMode, mode)
+    try:
+        n, kappa = 2048, 1e5
+        a = gen.spectrum(n, kappa, seed=11)
+        xt = np.random.default_rng(12).standard_normal((n, 1))
+        b = np.asfortranarray(a @ xt)
+        rc, it, x, info = dsposv_ex(L, LO, a, b)
+        assert rc == 0 and it >= 0 and info.fallback_fp64 == 0
+        assert info.factor_mode == pb.PlasmaFactorFP32 and info.attempts >= 2
+        assert solve_residual(a, x, b) < TOL * EPS
+    finally:
+        L.plasma_set(pb.PlasmaMixedPrecisionMode, pb.PlasmaFactorFP32)
+
+
 @pytest.mark.parametrize("uplo", [LO, UP])
 @pytest.mark.parametrize("n,nb", [(1000, 128), (777, 256), (64, 64), (1000, 192),
                                   (500, 96), (4100, 512)])
@@ -512,6 +593,68 @@ def test_single_rhs_sweeps(L, uplo, n, nb):
     a32 = np.asfortranarray(a.astype(np.float32))
     x32 = np.asfortranarray(b.astype(np.float32))
     assert L.plasma_sposv(uplo, n, 1, a32.ctypes.data, n, x32.ctypes.data, n) == 0
+    assert solve_residual(a, x32.astype(np.float64), b) < TOL * SEPS
+
+
+@pytest.mark.parametrize("n,nb,prec", [(8192, 256, "d"), (3000, 256, "s"), (1000, 128, "d"),
+                                       (777, 192, "d"), (1024, 128, "s")])
+def test_upper_storage_through_lower_tiles(L, n, nb, prec):
+    """uplo = Upper in the LAPACK-layout drivers: the upper triangle goes to
+    lower tiles transposed and is factored there (tensor-core updates), then
+    comes back transposed.  The factor matches the oracle's upper factor, the
+    solution the oracle's, and the strictly lower part of pA (NaN here) is
+    neither read nor written -- host and device arrays."""
+    set_nb(L, nb)
+    a, b = gen.diag_dominant(n, 4, seed=1300 + n)
+    dt, eps = (np.float64, EPS) if prec == "d" else (np.float32, SEPS)
+    au = np.triu(a) + np.tril(np.full_like(a, np.nan), -1)
+    fo = np.asfortranarray(a.copy())
+    assert oracle.potrf(oracle.UPPER, fo, nb) == 0
+    uo = np.triu(fo)
+    # potrf, host array
+    f = np.asfortranarray(au.astype(dt))
+    assert getattr(L, f"plasma_{prec}potrf")(UP, n, f.ctypes.data, n) == 0
+    assert np.isnan(np.tril(f, -1)[np.tril_indices(n, -1)]).all()
+    err = np.linalg.norm(np.triu(f).astype(np.float64) - uo) / np.linalg.norm(a)
+    assert err < TOL * eps, err
+    # posv, device arrays
+    A = torch.from_numpy(np.ascontiguousarray(au.astype(dt).T)).cuda()
+    B = torch.from_numpy(np.ascontiguousarray(b.astype(dt).T)).cuda()
+    assert getattr(L, f"plasma_{prec}posv")(UP, n, 4, A.data_ptr(), n, B.data_ptr(), n) == 0
+    fd = A.cpu().numpy().T
+    assert np.isnan(fd[np.tril_indices(n, -1)]).all()
+    assert np.linalg.norm(np.triu(fd).astype(np.float64) - uo) / np.linalg.norm(a) < TOL * eps
+    x = B.cpu().numpy().T.astype(np.float64)
+    assert solve_residual(a, x, b) < TOL * eps
+    if prec == "d":
+        xo = np.asfortranarray(b.copy())
+        assert oracle.posv(oracle.UPPER, np.asfortranarray(a.copy()), xo, nb) == 0
+        assert np.abs(x - xo).max() / np.abs(xo).max() < 1e-13
+
+
+@pytest.mark.parametrize("uplo", [LO, UP])
+@pytest.mark.parametrize("n,nb,nrhs", [(1000, 256, 16), (777, 128, 3), (2048, 256, 17),
+                                       (1000, 192, 32), (300, 64, 2), (4100, 512, 5)])
+def test_multi_rhs_sweeps(L, uplo, n, nb, nrhs):
+    """2 <= nrhs <= 32 uses the one-launch multi-column block sweeps (16
+    columns per launch; FP64 64-row and FP32 128-row blocks); compare with
+    the oracle and the tester's residual, FP64 and FP32, posv and potrs."""
+    set_nb(L, nb)
+    a, b = gen.diag_dominant(n, nrhs, seed=1200 + n + nrhs)
+    x, af = np.asfortranarray(b.copy()), np.asfortranarray(a.copy())
+    assert L.plasma_dposv(uplo, n, nrhs, af.ctypes.data, n, x.ctypes.data, n) == 0
+    assert solve_residual(a, x, b) < TOL * EPS
+    xo = np.asfortranarray(b.copy())
+    assert oracle.posv(uplo, np.asfortranarray(a.copy()), xo, nb) == 0
+    assert np.abs(x - xo).max() / np.abs(xo).max() < 1e-13
+    # potrs with the factor just computed, on new right-hand sides
+    b2 = np.asfortranarray(np.random.default_rng(n).standard_normal((n, nrhs)))
+    x2 = np.asfortranarray(b2.copy())
+    assert L.plasma_dpotrs(uplo, n, nrhs, af.ctypes.data, n, x2.ctypes.data, n) == 0
+    assert solve_residual(a, x2, b2) < TOL * EPS
+    a32 = np.asfortranarray(a.astype(np.float32))
+    x32 = np.asfortranarray(b.astype(np.float32))
+    assert L.plasma_sposv(uplo, n, nrhs, a32.ctypes.data, n, x32.ctypes.data, n) == 0
     assert solve_residual(a, x32.astype(np.float64), b) < TOL * SEPS
 
 
