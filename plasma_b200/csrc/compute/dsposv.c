@@ -197,9 +197,9 @@ static int gmres_correction(refine_t *R)
         R->gmres_iters++;
         if (fabs(g[j + 1]) <= GMRES_TOL * beta || !(hn > 0.0))
             break;
-        /* a stagnating Krylov residual (less than 2x over the last 10
+        /* a stagnating Krylov residual (less than 2x over the last 20
          * steps): the preconditioner is too weak, end this solve early */
-        if (j >= 10 && fabs(g[j + 1]) > 0.5 * gtrace[j - 10])
+        if (j >= 20 && fabs(g[j + 1]) > 0.5 * gtrace[j - 20])
             break;
         gtrace[j] = fabs(g[j + 1]);
     }
@@ -416,25 +416,35 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
      * shifted when the factorisation breaks down; Auto escalates
      * BF16 -> TF32 -> FP32.  Whatever fails ends in the FP64 path below.
      * ---------------------------------------------------------------- */
-    typedef struct { int mode; int scaled; } attempt_t;
-    attempt_t plan[4];
+    /* scaled: 0 = as is; c > 0 = unit diagonal and a shift of c*u */
+    typedef struct { int mode; double scaled; } attempt_t;
+    attempt_t plan[10];
     int nplan = 0;
     const int cfg = plasma->mixed_mode;
     if (cfg == PlasmaFactorAuto) {
         plan[nplan++] = (attempt_t){PlasmaFactorBF16, 0};
-        plan[nplan++] = (attempt_t){PlasmaFactorBF16, 1};
-        plan[nplan++] = (attempt_t){PlasmaFactorTF32, 1};
+        plan[nplan++] = (attempt_t){PlasmaFactorBF16, 4};
+        plan[nplan++] = (attempt_t){PlasmaFactorTF32, 4};
         plan[nplan++] = (attempt_t){PlasmaFactorFP32, 0};
+        for (double c = 4; c <= 16384; c *= 16)
+            plan[nplan++] = (attempt_t){PlasmaFactorFP32, c};
     } else if (cfg == PlasmaFactorFP32) {
         plan[nplan++] = (attempt_t){PlasmaFactorFP32, 0};
+        /* a breakdown is retried with shifts of 4u, 64u, 1024u, 16384u:
+         * the factorization's rounding error grows with the order and the
+         * norm of the scaled matrix, and GMRES-IR tolerates a shifted
+         * preconditioner */
         if (plasma->refinement != PlasmaRefineIR)
-            plan[nplan++] = (attempt_t){PlasmaFactorFP32, 1};
+            for (double c = 4; c <= 16384; c *= 16)
+                plan[nplan++] = (attempt_t){PlasmaFactorFP32, c};
     } else {
         /* TF32 / BF16 first, then FP32: a factor too coarse for the
          * matrix's condition escalates to FP32 before the FP64 fallback */
         plan[nplan++] = (attempt_t){cfg, 0};
-        plan[nplan++] = (attempt_t){cfg, 1};
+        plan[nplan++] = (attempt_t){cfg, 4};
         plan[nplan++] = (attempt_t){PlasmaFactorFP32, 0};
+        for (double c = 4; c <= 16384; c *= 16)
+            plan[nplan++] = (attempt_t){PlasmaFactorFP32, c};
     }
     const int scheme = plasma->refinement;
     /* the reference's configuration keeps the reference's failure semantics */
@@ -443,7 +453,7 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
     const int mres = GMRES_RESTART;
     double cte = 0.0;
     int converged = 0, used_gmres = 0, gm_iters = 0, attempts = 0;
-    int factor_failed = 0, fstatus = 0;
+    int factor_failed = 0, fstatus = 0, last = 0;
 
     plasma_cuda_lag2s(S, st, call, B, Xs, PlasmaGeneral);
     size_t need = sizeof(double) * (size_t)n * (6 + mres + 1) +
@@ -482,11 +492,15 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
 
     for (int a = 0; a < nplan && !converged; a++) {
         const int mode = plan[a].mode;
-        /* a scaled and shifted retry of the same precision answers a
-         * factorisation that broke down; after a factor that was computed
-         * but did not refine, the next precision is tried instead */
-        if (a > 0 && plan[a].scaled && plan[a - 1].mode == mode && !factor_failed)
+        /* a scaled (and shifted) factor of the same precision follows one
+         * that broke down, and, under GMRES-IR or the automatic scheme, an
+         * unscaled one that did not refine (equilibration can make the
+         * factor a good preconditioner, not a contraction for plain IR);
+         * larger shifts only follow a scaled factorization that broke down */
+        if (a > 0 && plan[a].scaled > 0 && plan[last].mode == mode && !factor_failed &&
+            (plan[last].scaled > 0 || scheme == PlasmaRefineIR))
             continue;
+        last = a;
         attempts++;
         if (rep) rep->factor_mode = mode;
         if (a > 0 && rep) cudaEventRecord(e0, S);
@@ -514,13 +528,13 @@ static void Xdsposv(plasma_context_t *plasma, plasma_enum_t uplo,
             else
                 plasma_cuda_lag2s_upper_to_lower(S, st, call, A, As);
         }
-        if (plan[a].scaled) {
+        if (plan[a].scaled > 0) {
             /* unit diagonal, then + c u I with u the unit roundoff of the
-             * products and c = 4 */
+             * products and c from the plan */
             double u = mode == PlasmaFactorBF16 ? 0x1p-8 :
                        mode == PlasmaFactorTF32 ? 0x1p-11 : 0x1p-24;
             plasma_cuda_diag_rsqrt(S, A, dvec, n, npad);
-            plasma_cuda_scale_shift(S, As, uplo_s, dvec, (float)(4.0 * u));
+            plasma_cuda_scale_shift(S, As, uplo_s, dvec, (float)(plan[a].scaled * u));
             RF.dscale = dvec;
         }
         plasma_pXpotrf_mode(plasma, uplo_s, As, sequence, request, call, mode);

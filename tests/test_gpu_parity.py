@@ -545,7 +545,7 @@ def test_gmres_ir_kappa_1e8_fixture(L, golden):
         xt = golden["spec8_xtrue"]
         b = np.asfortranarray(a @ xt)
         rc, it, x, info = dsposv_ex(L, LO, a, b)
-        assert rc == 0 and it >= 0 and info.fallback_fp64 == 0
+        assert rc == 0 and it >= 0 and info.fallback_fp64 == 0, (rc, it, info.as_dict())
         be, fe = _errors(a, x, xt)
         assert be <= 50 * n * EPS
         assert fe <= kappa * 1e-14
