@@ -272,6 +272,7 @@ typedef struct {
     const double *pA;
     int lda;
     int on_device;
+    int pageable;        /* host memory that is not page-locked */
 } upload_t;
 
 /* Tile-column groups that each hold about the same share of the lower
@@ -300,8 +301,9 @@ static int column_groups(int nt, int *gstart)
  * converted to the FP64 tiles of A and the FP32 tiles of As as soon as it
  * is in, and the factorization of As runs on the groups already in place
  * (plasma_pXpotrf_arrivals).  ||A||_inf follows the last group on the copy
- * stream.  With page-locked host memory the copies overlap the kernels;
- * pageable memory gives the same result without the overlap. */
+ * stream.  Page-locked host memory is copied directly; pageable memory goes
+ * through the staging slots (plasma_stage_copy), and both overlap the
+ * kernels. */
 static void upload_and_factor(plasma_context_t *plasma, const upload_t *up,
                               plasma_desc_t A, plasma_desc_t As, double *d_anorm,
                               double *symv_work, int call, int mode,
@@ -326,16 +328,25 @@ static void upload_and_factor(plasma_context_t *plasma, const upload_t *up,
      * storage, the right-hand side) */
     cudaEventRecord(plasma->ev[4], S);
     cudaStreamWaitEvent(cp, plasma->ev[4], 0);
+    if (up->pageable)
+        plasma_stage_begin(plasma, S);
     for (int g = 0; g < ng; g++) {
         for (int j = gstart[g]; j < gstart[g + 1]; j++) {
             const int c0 = j * nb;
             const int w = n - c0 < nb ? n - c0 : nb;
-            cudaMemcpy2DAsync(stage + (size_t)c0 * n + c0, (size_t)n * sizeof(double),
-                              up->pA + (size_t)c0 * up->lda + c0,
-                              (size_t)up->lda * sizeof(double),
-                              (size_t)(n - c0) * sizeof(double), (size_t)w,
-                              cudaMemcpyHostToDevice, cp);
+            double *dst = stage + (size_t)c0 * n + c0;
+            const double *src = up->pA + (size_t)c0 * up->lda + c0;
+            const size_t ldd = (size_t)n * sizeof(double), lds = (size_t)up->lda * sizeof(double);
+            const size_t bytes = (size_t)(n - c0) * sizeof(double);
+            if (up->pageable)
+                plasma_stage_copy(plasma, dst, ldd, src, lds, bytes, (size_t)w,
+                                  cudaMemcpyHostToDevice);
+            else
+                cudaMemcpy2DAsync(dst, ldd, src, lds, bytes, (size_t)w, cudaMemcpyHostToDevice,
+                                  cp);
         }
+        if (up->pageable)
+            plasma_stage_join(plasma, cp);       /* the group's columns are in */
         plasma_cuda_upload_cols(cp, st, call, A, As, stage, n, gstart[g], gstart[g + 1]);
         cudaEventRecord(plasma->ev_group[g], cp);
     }
@@ -793,7 +804,7 @@ int plasma_dsposv_ex(plasma_enum_t uplo, int n, int nrhs,
         pipeline_env = e == NULL || atoi(e) != 0;
     }
     const int on_device = plasma_is_device_pointer(pA);
-    upload_t up = {pA, lda, on_device};
+    upload_t up = {pA, lda, on_device, !on_device && plasma_is_pageable(pA)};
     const int pipelined = pipeline_env && uplo == PlasmaLower && plasma->lookahead != 0 &&
                           !on_device;
     /* a lower-stored device matrix goes to both tile copies in one pass

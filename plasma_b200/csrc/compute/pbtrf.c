@@ -306,9 +306,9 @@ void plasma_omp_Xpb2desc(const void *pAB, int ldab, plasma_desc_t A,
             plasma_request_fail(sequence, request, PlasmaErrorOutOfMemory);
             return;
         }
-        cudaMemcpy2DAsync(buf, (size_t)ld * elem, pAB, (size_t)ldab * elem,
-                          (size_t)ld * elem, (size_t)A.n, cudaMemcpyHostToDevice,
-                          plasma->stream);
+        plasma_copy_2d(plasma, plasma->stream, buf, (size_t)ld * elem, pAB,
+                       (size_t)ldab * elem, (size_t)ld * elem, (size_t)A.n,
+                       cudaMemcpyHostToDevice, plasma_is_pageable(pAB));
         src = buf;
     }
     plasma_cuda_band_to_tile(plasma->stream, plasma->dstat, A, src, ld);
@@ -337,14 +337,14 @@ void plasma_omp_Xdesc2pb(plasma_desc_t A, void *pAB, int ldab,
      * returns them unchanged. */
     const int nc = imin(A.n, ld - 1);
     const int c0 = A.uplo == PlasmaLower ? A.n - nc : 0;
+    const int pageable = plasma_is_pageable(pAB);
     if (nc > 0)
-        cudaMemcpy2DAsync(buf + (size_t)c0 * ld * elem, (size_t)ld * elem,
-                          (const char *)pAB + (size_t)c0 * ldab * elem, (size_t)ldab * elem,
-                          (size_t)ld * elem, (size_t)nc, cudaMemcpyHostToDevice,
-                          plasma->stream);
+        plasma_copy_2d(plasma, plasma->stream, buf + (size_t)c0 * ld * elem, (size_t)ld * elem,
+                       (const char *)pAB + (size_t)c0 * ldab * elem, (size_t)ldab * elem,
+                       (size_t)ld * elem, (size_t)nc, cudaMemcpyHostToDevice, pageable);
     plasma_cuda_tile_to_band(plasma->stream, plasma->dstat, A, buf, ld);
-    cudaMemcpy2DAsync(pAB, (size_t)ldab * elem, buf, (size_t)ld * elem, (size_t)ld * elem,
-                      (size_t)A.n, cudaMemcpyDeviceToHost, plasma->stream);
+    plasma_copy_2d(plasma, plasma->stream, pAB, (size_t)ldab * elem, buf, (size_t)ld * elem,
+                   (size_t)ld * elem, (size_t)A.n, cudaMemcpyDeviceToHost, pageable);
     cudaStreamSynchronize(plasma->stream);
 }
 

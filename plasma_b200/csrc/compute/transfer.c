@@ -5,8 +5,9 @@
  * plasma_omp_{d,s}{ge2desc,desc2ge,tr2desc,desc2tr} follow the reference's
  * compute/zge2desc.c:27-68 (argument checks, then one lacpy per tile,
  * compute/pzge2desc.c:22-56, pztr2desc.c:22-51).  The user array may live on
- * the host (it is staged through a device column-major buffer with one
- * cudaMemcpy2DAsync) or on the device (packed directly by the kernel).
+ * the host (it is staged through a device column-major buffer; pageable
+ * host memory also goes through the page-locked slots of
+ * control/staging.c) or on the device (packed directly by the kernel).
  */
 #include "../internal.h"
 
@@ -23,6 +24,27 @@ static void copy_region(plasma_context_t *plasma, void *dst, size_t ldd,
 {
     if (rows <= 0 || cols <= 0)
         return;
+    const void *host = kind == cudaMemcpyHostToDevice ? src : dst;
+    if (plasma_is_pageable(host)) {
+        plasma_stage_begin(plasma, plasma->stream);
+        if (uplo != PlasmaLower && uplo != PlasmaUpper) {
+            plasma_stage_copy(plasma, dst, ldd * elem, src, lds * elem, (size_t)rows * elem,
+                              (size_t)cols, kind);
+        } else {
+            for (int c0 = 0; c0 < cols; c0 += nb) {
+                int w = cols - c0 < nb ? cols - c0 : nb;
+                int r0 = uplo == PlasmaLower ? (c0 < rows ? c0 : rows) : 0;
+                int r1 = uplo == PlasmaLower ? rows : (c0 + nb < rows ? c0 + nb : rows);
+                if (r1 > r0)
+                    plasma_stage_copy(plasma, (char *)dst + ((size_t)c0 * ldd + r0) * elem,
+                                      ldd * elem,
+                                      (const char *)src + ((size_t)c0 * lds + r0) * elem,
+                                      lds * elem, (size_t)(r1 - r0) * elem, (size_t)w, kind);
+            }
+        }
+        plasma_stage_join(plasma, plasma->stream);
+        return;
+    }
     if (uplo != PlasmaLower && uplo != PlasmaUpper) {
         cudaMemcpy2DAsync(dst, ldd * elem, src, lds * elem,
                           (size_t)rows * elem, (size_t)cols, kind,

@@ -119,6 +119,11 @@ int plasma_init(void)
     for (int i = 0; i < PLASMA_NUM_STREAMS; i++)
         cudaStreamCreateWithPriority(&c->aux[i], cudaStreamNonBlocking,
                                      i == 0 || i == PLASMA_STREAM_COPY ? prio_hi : prio_lo);
+    for (int i = 0; i < PLASMA_STAGE_STREAMS; i++) {
+        cudaStreamCreateWithFlags(&c->stage[i], cudaStreamNonBlocking);
+        cudaEventCreateWithFlags(&c->ev_stage[i], cudaEventDisableTiming);
+    }
+    cudaEventCreateWithFlags(&c->ev_stage_in, cudaEventDisableTiming);
     for (int i = 0; i < 8; i++)
         cudaEventCreateWithFlags(&c->ev[i], cudaEventDisableTiming);
     for (int i = 0; i < PLASMA_MAX_GROUPS; i++)
@@ -161,6 +166,11 @@ int plasma_finalize(void)
     if (c->hstat) cudaFreeHost(c->hstat);
     for (int i = 0; i < PLASMA_NUM_STREAMS; i++)
         if (c->aux[i]) cudaStreamDestroy(c->aux[i]);
+    for (int i = 0; i < PLASMA_STAGE_STREAMS; i++) {
+        if (c->stage[i]) cudaStreamDestroy(c->stage[i]);
+        if (c->ev_stage[i]) cudaEventDestroy(c->ev_stage[i]);
+    }
+    if (c->ev_stage_in) cudaEventDestroy(c->ev_stage_in);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     memset(c, 0, sizeof(*c));
     plasma_initialized_g = 0;
@@ -343,6 +353,8 @@ void *plasma_pinned(plasma_context_t *c, size_t bytes)
         return c->pinned;
     if (c->pinned) {
         cudaStreamSynchronize(c->stream);
+        for (int i = 0; i < PLASMA_STAGE_STREAMS; i++)
+            cudaStreamSynchronize(c->stage[i]);
         cudaFreeHost(c->pinned);
         c->pinned = NULL;
         c->pinned_bytes = 0;
@@ -350,12 +362,24 @@ void *plasma_pinned(plasma_context_t *c, size_t bytes)
     plasma_note_cuda_error();
     plasma_alloc_count_g++;
     if (cudaMallocHost(&c->pinned, bytes) != cudaSuccess) {
-        plasma_note_cuda_error();
+        cudaGetLastError();            /* the callers fall back; not an error */
         c->pinned = NULL;
         return NULL;
     }
     c->pinned_bytes = bytes;
     return c->pinned;
+}
+
+int plasma_is_pageable(const void *p)
+{
+    struct cudaPointerAttributes attr;
+    if (p == NULL)
+        return 0;
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    return attr.type == cudaMemoryTypeUnregistered;
 }
 
 int plasma_is_device_pointer(const void *p)

@@ -40,6 +40,7 @@ typedef struct {
 #define PLASMA_STREAM_COPY 2
 #define PLASMA_GROUP_STREAMS (PLASMA_NUM_STREAMS - 3)
 #define PLASMA_MAX_GROUPS 32     /* column groups of an arriving matrix */
+#define PLASMA_STAGE_STREAMS 4   /* copies of pageable host blocks       */
 #define PLASMA_SCRATCH_SLOTS 9
 
 /* scratch slots */
@@ -73,6 +74,10 @@ typedef struct {
     cudaStream_t stream;                     /* the sequence stream         */
     cudaStream_t own_stream;                 /* created by plasma_init()    */
     cudaStream_t aux[PLASMA_NUM_STREAMS];    /* look-ahead / update streams */
+    cudaStream_t stage[PLASMA_STAGE_STREAMS];/* pageable-host staging       */
+    cudaEvent_t ev_stage[PLASMA_STAGE_STREAMS];
+    cudaEvent_t ev_stage_in;
+    unsigned stage_next;                     /* round robin over stage[]    */
     plasma_devstat_t *dstat;                 /* device status word          */
     plasma_devstat_t *dquiet;                /* a status word no kernel sets
                                                 (work that must complete)  */
@@ -128,6 +133,19 @@ void *plasma_pinned(plasma_context_t *plasma, size_t bytes);
 
 /* Queries whether p is device memory of the context's device. */
 int plasma_is_device_pointer(const void *p);
+/* Host memory that is neither page-locked nor registered with CUDA. */
+int plasma_is_pageable(const void *p);
+
+/* Host <-> device copies of column-major blocks (cudaMemcpy2DAsync
+ * arguments; width in bytes, height in columns) through page-locked
+ * staging slots when the host side is pageable (control/staging.c). */
+void plasma_stage_begin(plasma_context_t *plasma, cudaStream_t s);
+void plasma_stage_copy(plasma_context_t *plasma, void *dst, size_t dpitch, const void *src,
+                       size_t spitch, size_t width, size_t height, enum cudaMemcpyKind kind);
+void plasma_stage_join(plasma_context_t *plasma, cudaStream_t s);
+void plasma_copy_2d(plasma_context_t *plasma, cudaStream_t s, void *dst, size_t dpitch,
+                    const void *src, size_t spitch, size_t width, size_t height,
+                    enum cudaMemcpyKind kind, int pageable);
 
 static inline int imin(int a, int b) { return a < b ? a : b; }
 static inline int imax(int a, int b) { return a > b ? a : b; }

@@ -726,6 +726,50 @@ def test_dsposv_overlapped_upload(L, n, nb, kappa):
     assert np.abs(x - xo).max() / np.abs(xo).max() < kappa * 1e-14
 
 
+@pytest.mark.parametrize("n,nb,lda", [(3000, 256, 3000), (2500, 64, 2519)])
+def test_dsposv_pageable_upload_matches_pinned(L, n, nb, lda):
+    """A pageable host matrix goes up through the page-locked staging slots
+    (host copies on the staging streams, chunks going round them): the same
+    bytes reach the device as from page-locked memory, so the iteration
+    count and the solution are identical, with lda > n too."""
+    set_nb(L, nb)
+    a = gen.spectrum(n, 1e4, seed=2300 + n)
+    b = a @ np.random.default_rng(n).standard_normal((n, 1))
+    ap = np.zeros((lda, n), order="F")
+    ap[:n] = a
+    A, B = _pinned_colmajor(ap), _pinned_colmajor(b)
+    X = torch.zeros((1, n), dtype=torch.float64, pin_memory=True)
+    it = ctypes.c_int(-99)
+    assert L.plasma_dsposv(LO, n, 1, A.data_ptr(), lda, B.data_ptr(), n, X.data_ptr(), n,
+                           ctypes.byref(it)) == 0
+    bp = np.asfortranarray(b)
+    xp = np.zeros((n, 1), order="F")
+    itp = ctypes.c_int(-98)
+    assert L.plasma_dsposv(LO, n, 1, ap.ctypes.data, lda, bp.ctypes.data, n, xp.ctypes.data,
+                           n, ctypes.byref(itp)) == 0
+    assert itp.value == it.value >= 0
+    assert np.array_equal(xp, X.numpy().T)
+    assert solve_residual(a, xp, b) < TOL * EPS
+
+
+@pytest.mark.parametrize("uplo", [LO, UP])
+def test_dpotrf_pageable_matches_pinned(L, uplo):
+    """dpotrf on a pageable array (up and back down through the staging
+    slots, chunks of whole columns, a ragged last tile column) returns the
+    same factor, bit for bit, as on a page-locked copy of it."""
+    set_nb(L, 128)
+    n, lda = 1500, 1507
+    a, _ = gen.diag_dominant(n, 1, seed=77)
+    ap = np.zeros((lda, n), order="F")
+    ap[:n] = a
+    ap[n:] = 5.0                      # rows below the matrix stay as they are
+    A = _pinned_colmajor(ap)
+    assert L.plasma_dpotrf(uplo, n, A.data_ptr(), lda) == 0
+    assert L.plasma_dpotrf(uplo, n, ap.ctypes.data, lda) == 0
+    assert np.array_equal(ap, A.numpy().T)
+    assert np.all(ap[n:] == 5.0)
+
+
 def test_dsposv_overlapped_upload_fallback(L):
     """kappa = 1e12: the FP32 factorization fails while later column groups
     are still on their way.  The reference's configuration fails the call
