@@ -39,7 +39,9 @@ typedef struct {
     int mode;          /* PLASMA_TC_* product precision of the tensor-core
                           update, or 0 for the DMMA/SIMT update            */
     int full;          /* panel copies: every panel (1) or two buffers (0) */
-    char *panel[2];    /* rounded copies of panel k (buffer k & 1, or all) */
+    char *panel[3];    /* rounded copies of panel k (buffer k % 3, or all) */
+    char *wimg;        /* operand image of the diagonal tile for the
+                          tensor-core panel solve (plasma_cuda_trsm_tc)    */
 } walk_t;
 
 /* FP32 factors: every mode runs its update on the tensor cores when the
@@ -59,11 +61,16 @@ static int tc_mode(plasma_desc_t A, int mode)
          : (A.mb == 256 && split_env) ? PLASMA_TC_BF16X6 : PLASMA_TC_TF32X3;
 }
 
-/* the panel copies: two buffers, or one holding every panel */
+/* the panel copies: three buffers, or one holding every panel; then the
+ * operand image of the panel solve.  Panel k's copy is written by the
+ * solve of step k (or by plasma_cuda_panel_round right after it); with
+ * three buffers the one it reuses was last read by the step k-3 update,
+ * which the critical stream has waited for (N(k-2)) before step k. */
 static size_t panel_scratch_bytes(plasma_desc_t A, int tc, int full)
 {
     const size_t one = (plasma_cuda_panel_bytes(tc, A, full) + 1023) & ~(size_t)1023;
-    return (full ? 1 : 2) * one + 1024;
+    const size_t wimg = (plasma_cuda_trsm_tc_bytes(A.nb) + 1023) & ~(size_t)1023;
+    return (full ? 1 : 3) * one + wimg + 1024;
 }
 
 void plasma_pXpotrf_reserve(plasma_context_t *plasma, plasma_enum_t uplo, plasma_desc_t A,
@@ -75,7 +82,7 @@ void plasma_pXpotrf_reserve(plasma_context_t *plasma, plasma_enum_t uplo, plasma
 
 static void *panel_buf(walk_t *w, int k)
 {
-    return w->full ? w->panel[0] : w->panel[k & 1];
+    return w->full ? w->panel[0] : w->panel[k % 3];
 }
 
 static void update(walk_t *w, cudaStream_t s, int k, int nlo, int nhi)
@@ -92,6 +99,22 @@ static void round_panel(walk_t *w, cudaStream_t s, int k)
 {
     if (w->mode)
         plasma_cuda_panel_round(s, w->st, w->mode, w->A, k, panel_buf(w, k), w->full);
+}
+
+/* The panel solve of step k: on the tensor cores next to a tensor-core
+ * update (which then also writes the rounded panel copies when the update
+ * takes TF32 operands), else the generic kernels.  Returns 1 when the
+ * panel copies are written. */
+static int trsm(walk_t *w, cudaStream_t s, int k)
+{
+    if (w->mode && w->wimg != NULL) {
+        const int r = plasma_cuda_trsm_tc(s, w->st, w->mode, w->A, k, k + 1, w->A.mt,
+                                          w->wimg, panel_buf(w, k), w->full);
+        if (r)
+            return r == 2;
+    }
+    plasma_cuda_trsm_panel(s, w->st, w->uplo, w->A, k, k + 1, w->A.mt, NULL);
+    return 0;
 }
 
 void plasma_pXpotrf(plasma_context_t *plasma, plasma_enum_t uplo,
@@ -150,14 +173,15 @@ static void walk_groups(plasma_context_t *plasma, walk_t *w, int call, int ngrou
     int gk = 0;                      /* group of column k + 1 */
     for (int k = 0; k < mt; k++) {
         plasma_cuda_potrf_tile(crit, st, call, uplo, A, k, A.nb * k, NULL);
-        plasma_cuda_trsm_panel(crit, st, uplo, A, k, k + 1, mt, NULL);
+        const int rounded = trsm(w, crit, k);
         if (k + 1 >= mt)
             break;
         while (gstart[gk + 1] <= k + 1) gk++;
         cudaStreamWaitEvent(crit, arrive[gk], 0);
         if (have_next)
             cudaStreamWaitEvent(crit, ev_next, 0);
-        round_panel(w, crit, k);
+        if (!rounded)
+            round_panel(w, crit, k);
         cudaEventRecord(ev_panel, crit);
         update(w, crit, k, k + 1, k + 2);
 
@@ -229,7 +253,8 @@ void plasma_pXpotrf_arrivals(plasma_context_t *plasma, plasma_enum_t uplo,
     w.sms = plasma->num_sms;
     w.mode = 0;
     w.full = grouped;
-    w.panel[0] = w.panel[1] = NULL;
+    w.panel[0] = w.panel[1] = w.panel[2] = NULL;
+    w.wimg = NULL;
     int tc = tc_mode(A, mode);
     if (plasma_cuda_update_tc_ok(A, uplo)) {
         char *buf = (char *)plasma_scratch(plasma, PLASMA_SLOT_MIXED,
@@ -240,6 +265,8 @@ void plasma_pXpotrf_arrivals(plasma_context_t *plasma, plasma_enum_t uplo,
             w.mode = tc;
             w.panel[0] = buf;
             w.panel[1] = buf + one;
+            w.panel[2] = buf + 2 * one;
+            w.wimg = buf + (w.full ? 1 : 3) * one;
         }
     }
     /* FP32 panels: TF32 products next to a TF32/BF16 update, else the
@@ -251,8 +278,7 @@ void plasma_pXpotrf_arrivals(plasma_context_t *plasma, plasma_enum_t uplo,
     if (plasma->lookahead == 0 || mt < 3) {
         for (int k = 0; k < mt; k++) {
             plasma_cuda_potrf_tile(S, st, call, uplo, A, k, A.nb * k, NULL);
-            plasma_cuda_trsm_panel(S, st, uplo, A, k, k + 1, mt, NULL);
-            if (w.mode)
+            if (!trsm(&w, S, k))
                 round_panel(&w, S, k);
             update(&w, S, k, k + 1, mt);
         }
@@ -279,15 +305,14 @@ void plasma_pXpotrf_arrivals(plasma_context_t *plasma, plasma_enum_t uplo,
     int have_next = 0;   /* N(k-1) was recorded */
     for (int k = 0; k < mt; k++) {
         plasma_cuda_potrf_tile(crit, st, call, uplo, A, k, A.nb * k, NULL);
-        plasma_cuda_trsm_panel(crit, st, uplo, A, k, k + 1, mt, NULL);
+        const int rounded = trsm(&w, crit, k);
         if (k + 1 >= mt)
             break;
-        /* the bulk stream is done with column k+1 (its step k-1 update) and,
-         * since N(k-1) follows the whole step k-2 update on that stream, with
-         * the panel buffer that the rounded copy of panel k is about to reuse */
+        /* the bulk stream is done with column k+1 (its step k-1 update) */
         if (have_next)
             cudaStreamWaitEvent(crit, ev_next, 0);
-        round_panel(&w, crit, k);
+        if (!rounded)
+            round_panel(&w, crit, k);
         cudaEventRecord(ev_panel, crit);
 
         /* critical: the next panel column */

@@ -44,10 +44,9 @@
 // bounded (about 2 s); on expiry the CTA records PlasmaErrorInternal, lets
 // what it issued drain and frees its tensor memory.
 #include "common.cuh"
+#include "tc.cuh"
 
-#include <cuda.h>
 #include <cuda_bf16.h>
-#include <cudaTypedefs.h>
 #include <stdlib.h>
 
 namespace {
@@ -83,103 +82,6 @@ struct Geo {
                                 TC_EPI_WARPS * EPI_BUFS * TC_EPI_BUF_BYTES + 1024;
 };
 
-__device__ __forceinline__ void mbar_init(uint64_t *bar, int count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-                 "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
-    return ok != 0;
-}
-
-// Bounded wait: false after ~2 s (or at once when the CTA already gave up).
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity,
-                                          volatile int *abort_flag)
-{
-    long long t0 = clock64();
-    while (!mbar_try(bar, parity)) {
-        if (*abort_flag) return false;
-        if (clock64() - t0 > 4000000000LL) {
-            *abort_flag = 1;
-            return false;
-        }
-    }
-    return true;
-}
-
-__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map,
-                                            uint64_t *bar, int c0, int c1, int c2,
-                                            int c3)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cta.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%3, %4, %5, %6}], [%2];"
-        :: "r"(smem_u32(dst)), "l"(map), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2),
-           "r"(c3)
-        : "memory");
-}
-
-// C(tile)[y .. y+31, x .. x+31] += staged 32 x 32 block (column-major)
-__device__ __forceinline__ void tma_reduce_add_3d(const CUtensorMap *map, const void *src,
-                                                  int c0, int c1, int c2)
-{
-    asm volatile(
-        "cp.reduce.async.bulk.tensor.3d.global.shared::cta.add.tile.bulk_group"
-        " [%0, {%2, %3, %4}], [%1];"
-        :: "l"(map), "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2) : "memory");
-}
-
-__device__ __forceinline__ void bulk_commit()
-{
-    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-}
-
-template <int N>
-__device__ __forceinline__ void bulk_wait_read()
-{
-    asm volatile("cp.async.bulk.wait_group.read %0;" :: "n"(N) : "memory");
-}
-
-__device__ __forceinline__ void bulk_wait_all()
-{
-    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
-}
-
-// Shared-memory matrix descriptor of an MN-major operand.  BF16 uses the
-// 128-byte swizzle (8 K-rows of 128 bytes per atom, layout type 2); MN-major
-// TF32 operands only exist with the 128-byte swizzle of 32-byte atomicity
-// (4 K-rows per atom, layout type 1).  lbo = stride between 128-byte MN
-// chunks, sbo = stride between K atoms.
-__device__ __forceinline__ uint64_t smem_desc(const void *p, uint32_t lbo, uint32_t sbo,
-                                              uint32_t layout)
-{
-    uint64_t d = 0;
-    d |= (uint64_t)((smem_u32(p) >> 4) & 0x3FFF);
-    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
-    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
-    d |= (uint64_t)1 << 46;                  // descriptor version (sm_100)
-    d |= (uint64_t)layout << 61;
-    return d;
-}
-
 __device__ __forceinline__ uint32_t instr_desc(int mode, int n)
 {
     uint32_t fmt = mode == MODE_BF16 ? 1u : 2u;   // BF16 : TF32
@@ -211,25 +113,6 @@ __device__ __forceinline__ void mma_commit(uint64_t *bar)
 {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                  :: "r"(smem_u32(bar)) : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
-{
-    uint32_t r[32];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
-          "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
-          "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]),
-          "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
-          "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
 
 struct TcArgs {
@@ -810,21 +693,6 @@ k_update_pair(const __grid_constant__ CUtensorMap opmap,
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
-{
-    // resolved through the runtime so that the library does not link the
-    // driver library directly (it must load on machines without a GPU)
-    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    if (encode == nullptr) {
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void **)&encode,
-                                    cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess)
-            encode = nullptr;
-    }
-    return encode;
-}
-
 // Operand map: 4-D over the column-major panel tiles
 //   dim 0: 128 bytes of a column (MN inner), dim 1: K (columns, stride nb),
 //   dim 2: 128-byte MN chunks (stride 128 bytes), dim 3: tiles
@@ -935,6 +803,12 @@ int mode_parts(int mode)
     return mode == PLASMA_TC_TF32X3 ? 2 : mode == PLASMA_TC_BF16X6 ? 3 : 1;
 }
 }  // namespace
+
+extern "C" void plasma_cuda_panel_layout(plasma_desc_t A, int k, int full, int *poff,
+                                         int *pstride)
+{
+    panel_layout(A, k, full, poff, pstride);
+}
 
 // Eligibility of the tensor-core update for an FP32 descriptor: general or
 // packed-lower storage, lower, square tiles of 128 or 256, no ragged tile.

@@ -211,6 +211,12 @@ void plasma_cuda_potrf_tile(cudaStream_t s, plasma_devstat_t *st, int call,
 /* Panel solve of step k: A(m,k) <- A(m,k) * L_kk^{-T} for m = k+1..mt-1
  * (upper: A(k,m) <- U_kk^{-T} A(k,m)), given W = inv(L_kk). mlo..mhi-1 is the
  * tile range processed. */
+/* Panel solve of step k on the tensor cores (FP32, lower, tiles of 128 or
+ * 256); writes the update's rounded panel copies when the mode's operands
+ * are TF32.  0: not eligible, 1: solved, 2: solved and copies written. */
+int plasma_cuda_trsm_tc(cudaStream_t s, plasma_devstat_t *st, int mode, plasma_desc_t A,
+                        int k, int mlo, int mhi, void *wimg, void *panel, int full);
+size_t plasma_cuda_trsm_tc_bytes(int nb);
 void plasma_cuda_trsm_panel(cudaStream_t s, plasma_devstat_t *st,
                             plasma_enum_t uplo, plasma_desc_t A, int k,
                             int mlo, int mhi, const void *winv);
