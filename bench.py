@@ -515,6 +515,9 @@ def run_lu(args):
     import plasma_b200 as pb
     L = pb.lib()
     assert L.plasma_init() == 0
+    if args.nb:
+        L.plasma_set(pb.PlasmaTuning, pb.PlasmaDisabled)
+        L.plasma_set(pb.PlasmaNb, args.nb)
     rows = []
     for n in (4096,):
         g = torch.Generator(device="cuda").manual_seed(9)

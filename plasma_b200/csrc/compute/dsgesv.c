@@ -78,13 +78,17 @@ typedef struct {
     void *tmp;             /* nb x max(n, nrhs) block row            */
     size_t tmp_cols;
     void *parts;           /* per-CTA pivot candidates of the panel  */
+    void *Wf, *Wb;         /* block inverses of the one-launch sweeps */
+    int sweeps;            /* Wf, Wb hold the current factor's        */
 } lu_work_t;
 
 static int lu_work(plasma_context_t *plasma, plasma_desc_t A, int ncols, lu_work_t *w)
 {
     const size_t es = plasma_element_size(A.precision);
     const size_t nbsq = (size_t)A.mb * A.mb;
-    char *buf = (char *)plasma_scratch(plasma, PLASMA_SLOT_WORK, 2 * A.mt * nbsq * es + 256);
+    const size_t wsw = (plasma_cuda_trsv_w_bytes(A) + 255) & ~(size_t)255;
+    char *buf = (char *)plasma_scratch(plasma, PLASMA_SLOT_WORK,
+                                       2 * A.mt * nbsq * es + 2 * wsw + 256);
     const size_t cols = (size_t)(ncols > A.n ? ncols : A.n);
     void *tmp = plasma_scratch(plasma, PLASMA_SLOT_ADJOINT, (size_t)A.mb * cols * es + 256);
     void *parts = plasma_scratch(plasma, PLASMA_SLOT_MIXED, plasma_cuda_getrf_parts_bytes(A));
@@ -93,6 +97,9 @@ static int lu_work(plasma_context_t *plasma, plasma_desc_t A, int ncols, lu_work
     w->parts = parts;
     w->WL = buf;
     w->WU = buf + A.mt * nbsq * es;
+    w->Wf = buf + 2 * A.mt * nbsq * es;
+    w->Wb = (char *)w->Wf + wsw;
+    w->sweeps = 0;
     plasma_desc_general_init(A.precision, w->WL, A.mb, A.mb, A.mb, A.mt * A.mb, 0, 0,
                              A.mb, A.mt * A.mb, &w->Wd);
     plasma_desc_general_init(A.precision, w->WU, A.mb, A.mb, A.mb, A.mt * A.mb, 0, 0,
@@ -141,6 +148,9 @@ static void plasma_pXgetrf(plasma_context_t *plasma, plasma_desc_t A, int *dpiv,
                                       view(A, r0, c1), 1.0, view(A, c1, c1), 0, 0);
         }
     }
+    /* the block inverses of the one-launch sweeps (one right-hand side) */
+    w->sweeps = plasma_sweep_reserve(plasma, A) &&
+                plasma_cuda_trtri_blocks_lu(S, st, A, w->Wf, w->Wb);
 }
 
 /* A X = B with the factor of plasma_pXgetrf (pivots dpiv, inverses in w):
@@ -152,6 +162,13 @@ static void plasma_pXgetrs(plasma_context_t *plasma, plasma_desc_t A, const int 
     plasma_devstat_t *st = plasma->dstat;
     const int mt = A.mt, N = B.n;
     plasma_cuda_laswp(S, st, B, dpiv, 0, A.m, 0, N);
+    /* one right-hand side (a contiguous vector): the one-launch sweeps,
+     * L y = P b (unit lower, forward), then U x = y (backward) */
+    if (w->sweeps && N == 1 && B.gn == 1 && B.nt == 1) {
+        plasma_sweep(plasma, PlasmaLower, 0, A, w->Wf, B.matrix);
+        plasma_sweep(plasma, PlasmaUpper, 1, A, w->Wb, B.matrix);
+        return;
+    }
     for (int k = 0; k < mt; k++) {
         const int kb = plasma_tile_mview(A, k), r0 = k * A.mb, r1 = r0 + kb;
         apply_inverse(plasma, w, w->Wd, B, k, kb, 0, N);
@@ -191,15 +208,19 @@ static int check_descs(plasma_desc_t A, plasma_desc_t B, plasma_desc_t X, plasma
     return A.mb == A.nb;
 }
 
-/* R = B - A X; xn, rn (device) <- columnwise max |X|, |R| */
+/* R = B - A X; xn, rn (device) <- columnwise max |X|, |R|.  part: scratch
+ * of the one-column product (plasma_cuda_gemv_part_bytes). */
 static void residual(plasma_context_t *plasma, plasma_desc_t A, plasma_desc_t B,
-                     plasma_desc_t X, plasma_desc_t R, double *xn, double *rn)
+                     plasma_desc_t X, plasma_desc_t R, double *xn, double *rn, double *part)
 {
     cudaStream_t S = plasma->stream;
     plasma_devstat_t *st = plasma->dstat;
     plasma_cuda_lacpy(S, st, B, R);
-    plasma_cuda_gemm_view(S, st, A.m, B.n, A.n, -1.0, view(A, 0, 0), view(X, 0, 0), 1.0,
-                          view(R, 0, 0), 0, 0);
+    if (B.n == 1 && X.gn == 1 && R.gn == 1)
+        plasma_cuda_gemv_sub(S, st, A, X.matrix, R.matrix, part);
+    else
+        plasma_cuda_gemm_view(S, st, A.m, B.n, A.n, -1.0, view(A, 0, 0), view(X, 0, 0), 1.0,
+                              view(R, 0, 0), 0, 0);
     plasma_cuda_colmax(S, st, X, xn);
     plasma_cuda_colmax(S, st, R, rn);
 }
@@ -255,9 +276,12 @@ void plasma_omp_dsgesv(plasma_desc_t A, int *ipiv, plasma_desc_t B, plasma_desc_
     double *dsmall = (double *)plasma_scratch(plasma, PLASMA_SLOT_SMALL,
                                               sizeof(double) * (2 * (size_t)nrhs + 8));
     int *dpiv = (int *)plasma_scratch(plasma, PLASMA_SLOT_SYMV, sizeof(int) * ((size_t)n + 8));
+    double *part = (double *)plasma_scratch(plasma, PLASMA_SLOT_REFINE,
+                                            plasma_cuda_gemv_part_bytes(A));
     double *hn = (double *)malloc(sizeof(double) * (2 * (size_t)nrhs + 1));
     lu_work_t w;
-    if (dsmall == NULL || dpiv == NULL || hn == NULL || !lu_work(plasma, A, nrhs, &w)) {
+    if (dsmall == NULL || dpiv == NULL || part == NULL || hn == NULL ||
+        !lu_work(plasma, A, nrhs, &w)) {
         free(hn);
         plasma_request_fail(sequence, request, PlasmaErrorOutOfMemory);
         return;
@@ -268,7 +292,7 @@ void plasma_omp_dsgesv(plasma_desc_t A, int *ipiv, plasma_desc_t B, plasma_desc_
 
     /* ||A||_inf, cte = ||A|| eps sqrt(n) (zcgesv.c:426-434) */
     double anorm = 0.0;
-    plasma_cuda_lange_inf(S, st, A, d_anorm);
+    plasma_cuda_lange_inf(S, st, A, d_anorm, part);
     cudaMemcpyAsync(&anorm, d_anorm, sizeof(double), cudaMemcpyDeviceToHost, S);
     int fallback = take_status(plasma) != 0;
     const double cte = anorm * eps * sqrt((double)n);
@@ -290,7 +314,7 @@ void plasma_omp_dsgesv(plasma_desc_t A, int *ipiv, plasma_desc_t B, plasma_desc_
     if (!fallback) {
         plasma_pXgetrs(plasma, As, dpiv, &ws, Xs);
         plasma_cuda_slag2d(S, st, Xs, X);
-        residual(plasma, A, B, X, R, d_xn, d_rn);
+        residual(plasma, A, B, X, R, d_xn, d_rn, part);
         cudaMemcpyAsync(hn, d_xn, sizeof(double) * 2 * nrhs, cudaMemcpyDeviceToHost, S);
         cudaStreamSynchronize(S);
         done = converged(h_rn, h_xn, nrhs, cte);
@@ -301,7 +325,7 @@ void plasma_omp_dsgesv(plasma_desc_t A, int *ipiv, plasma_desc_t B, plasma_desc_
             plasma_pXgetrs(plasma, As, dpiv, &ws, Xs);
             plasma_cuda_slag2d(S, st, Xs, R);
             plasma_cuda_geadd(S, st, R, X);
-            residual(plasma, A, B, X, R, d_xn, d_rn);
+            residual(plasma, A, B, X, R, d_xn, d_rn, part);
             cudaMemcpyAsync(hn, d_xn, sizeof(double) * 2 * nrhs, cudaMemcpyDeviceToHost, S);
             cudaStreamSynchronize(S);
             done = converged(h_rn, h_xn, nrhs, cte);
@@ -366,9 +390,18 @@ int plasma_dsgesv(int n, int nrhs, double *pA, int lda, int *ipiv, double *pB, i
         return PlasmaErrorIllegalValue;
     if (plasma->device < 0)
         return PlasmaErrorEnvironment;
-    if (plasma->tuning)
-        plasma_tune_potrf(plasma, PlasmaRealFloat, n);
-    const int nb = plasma->nb;
+    /* tuned: 64-wide tiles when the FP32 LU's panels fit the one-launch
+     * cluster panel (the panel's column chain is the LU's critical path;
+     * wider tiles only lengthen it), else the Cholesky table's size */
+    int nb = plasma->nb;
+    if (plasma->tuning) {
+        if (n <= plasma_cuda_getrf_cluster_rows(PlasmaRealFloat)) {
+            nb = 64;
+        } else {
+            plasma_tune_potrf(plasma, PlasmaRealFloat, n);
+            nb = plasma->nb;
+        }
+    }
 
     plasma_desc_t A, As, B, X, Xs, R;
     int rc = plasma_desc_kept(plasma, PLASMA_SLOT_DESC_A, PlasmaRealDouble, PlasmaGeneral, nb,

@@ -37,7 +37,7 @@
 //             only waits until these warps have read X_j).
 #include "common.cuh"
 #include "tc.cuh"
-#include "mma.cuh"
+#include "inv64.cuh"
 
 namespace {
 
@@ -394,20 +394,6 @@ __device__ __forceinline__ void put_w(float *__restrict__ whi, float *__restrict
     if (split == 3) wlo[e] = __uint_as_float(tf32_round(v - __uint_as_float(hi)));
 }
 
-// One warp: the 16 x 8 block C (+)= A (16 x K) B (K x 8) on DMMA, A and B
-// row-major in shared memory (fragment layout of dmma_16x8x8).
-__device__ __forceinline__ void warp_tile_f64(double (&c)[4], const double *A, int lda,
-                                              const double *B, int ldb, int K)
-{
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    for (int k0 = 0; k0 < K; k0 += 8) {
-        const double af[4] = {A[g * lda + k0 + t], A[(g + 8) * lda + k0 + t],
-                              A[g * lda + k0 + t + 4], A[(g + 8) * lda + k0 + t + 4]};
-        const double bf[2] = {B[(k0 + t) * ldb + g], B[(k0 + t + 4) * ldb + g]};
-        dmma_16x8x8(c, af, bf);
-    }
-}
-
 __global__ void __launch_bounds__(256)
 k_trsm_prep(plasma_desc_t A, int k, float *w, int split, const plasma_devstat_t *st)
 {
@@ -416,10 +402,7 @@ k_trsm_prep(plasma_desc_t A, int k, float *w, int split, const plasma_devstat_t 
     double (*Ls)[LD] = reinterpret_cast<double (*)[LD]>(prep_smem);
     double (*Iv)[LD] = Ls + TS_B;
     double (*Tm)[TLD] = reinterpret_cast<double (*)[TLD]>(Iv + TS_B);
-    double *rdiag = &Tm[48][0];                // 1 / L_ii (Tm rows 48 .. 63 are unused
-                                               // until then)
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int g = lane >> 2, t = lane & 3;
+    const int tid = threadIdx.x;
     const int nb = A.mb, nblk = nb / TS_B;
     const float *__restrict__ L = (const float *)plasma_tile_addr(A, k, k);
     const int ldl = plasma_tile_mmain(A, k);
@@ -463,71 +446,7 @@ k_trsm_prep(plasma_desc_t A, int k, float *w, int split, const plasma_devstat_t 
         }
     }
     __syncthreads();
-    if (tid < TS_B) rdiag[tid] = 1.0 / Ls[tid][tid];
-    __syncthreads();
-    // the eight 8 x 8 diagonal blocks: a thread per column, in registers
-    if (tid < TS_B) {
-        const int o = tid & ~7, cc = tid & 7;
-        double x[8];
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            double s = i == cc ? 1.0 : 0.0;
-#pragma unroll
-            for (int q = 0; q < i; q++) s -= Ls[o + i][o + q] * x[q];
-            x[i] = i >= cc ? s * rdiag[o + i] : 0.0;
-        }
-#pragma unroll
-        for (int i = 0; i < 8; i++) Iv[o + i][o + cc] = x[i];
-    }
-    __syncthreads();
-    // pairs [A 0; B C] of h x h blocks: the lower-left block of the inverse,
-    // -C^-1 (B A^-1).  Iv is zero above its diagonal, so the products may
-    // run over whole rows of the triangular factors.
-    {   // h = 8: four pairs, a thread per entry
-        const int p = tid / 64, i = (tid % 64) / 8, c = tid % 8, o = 16 * p;
-        double s = 0.0;
-#pragma unroll
-        for (int q = 0; q < 8; q++) s += Ls[o + 8 + i][o + q] * Iv[o + q][o + c];
-        Tm[o + i][c] = s;
-        __syncthreads();
-        s = 0.0;
-#pragma unroll
-        for (int q = 0; q < 8; q++) s += Iv[o + 8 + i][o + 8 + q] * Tm[o + q][c];
-        Iv[o + 8 + i][o + c] = -s;
-        __syncthreads();
-    }
-    {   // h = 16: two pairs, warps 0-3 each a 16 x 8 block of one pair
-        const int p = warp >> 1, nt = warp & 1, o = 32 * p;
-        if (warp < 4) {
-            double c[4] = {0.0, 0.0, 0.0, 0.0};
-            warp_tile_f64(c, &Ls[o + 16][o], LD, &Iv[o][o + 8 * nt], LD, 16);
-#pragma unroll
-            for (int e = 0; e < 4; e++) Tm[o + g + 8 * (e >> 1)][8 * nt + 2 * t + (e & 1)] = c[e];
-        }
-        __syncthreads();
-        if (warp < 4) {
-            double c[4] = {0.0, 0.0, 0.0, 0.0};
-            warp_tile_f64(c, &Iv[o + 16][o + 16], LD, &Tm[o][8 * nt], TLD, 16);
-#pragma unroll
-            for (int e = 0; e < 4; e++)
-                Iv[o + 16 + g + 8 * (e >> 1)][o + 8 * nt + 2 * t + (e & 1)] = -c[e];
-        }
-        __syncthreads();
-    }
-    {   // h = 32: one pair, warp w the 16 x 8 block (w / 4, w mod 4)
-        const int mt = warp >> 2, nt = warp & 3;
-        double c[4] = {0.0, 0.0, 0.0, 0.0};
-        warp_tile_f64(c, &Ls[32 + 16 * mt][0], LD, &Iv[0][8 * nt], LD, 32);
-#pragma unroll
-        for (int e = 0; e < 4; e++) Tm[16 * mt + g + 8 * (e >> 1)][8 * nt + 2 * t + (e & 1)] = c[e];
-        __syncthreads();
-        double d[4] = {0.0, 0.0, 0.0, 0.0};
-        warp_tile_f64(d, &Iv[32 + 16 * mt][32], LD, &Tm[0][8 * nt], TLD, 32);
-#pragma unroll
-        for (int e = 0; e < 4; e++)
-            Iv[32 + 16 * mt + g + 8 * (e >> 1)][8 * nt + 2 * t + (e & 1)] = -d[e];
-        __syncthreads();
-    }
+    inv_lower64(Ls, Iv, Tm, false);
 #pragma unroll
     for (int q = 0; q < PER; q++) {
         const int e = tid + 256 * q, i = e % TS_B, c = e / TS_B;

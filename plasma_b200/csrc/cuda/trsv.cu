@@ -295,9 +295,10 @@ k_trsv(plasma_desc_t A, int uplo, int backward, const T *W, T *vec,
 
 // W_u = inv(logical L diagonal block u, SB x SB), written densely
 // ([u][c*SB + i]); rows and columns beyond the matrix are the identity.
+// unit: the diagonal of L is taken as one (the unit-lower factor of an LU).
 template <typename T, int SB>
 __global__ void __launch_bounds__(256)
-k_trtri_blocks(plasma_desc_t A, int uplo, T *W, const plasma_devstat_t *st)
+k_trtri_blocks(plasma_desc_t A, int uplo, int unit, T *W, const plasma_devstat_t *st)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *Ls = reinterpret_cast<T *>(smem_raw);       // [SB][SB+1]
@@ -309,7 +310,7 @@ k_trtri_blocks(plasma_desc_t A, int uplo, T *W, const plasma_devstat_t *st)
     const int tid = threadIdx.x;
     for (int e = tid; e < SB * SB; e += 256) {
         int i = e % SB, c = e / SB;
-        Ls[c * (SB + 1) + i] = (i < rows && c < rows && i >= c)
+        Ls[c * (SB + 1) + i] = (i < rows && c < rows && i >= c && !(unit && i == c))
             ? b.p[(size_t)i * b.si + (size_t)c * b.sj] : (i == c ? T(1) : T(0));
     }
     __syncthreads();
@@ -960,7 +961,7 @@ template <typename T, int SB> constexpr int trtri_smem()
 
 template <typename T, int SB>
 void launch_trtri(cudaStream_t s, plasma_devstat_t *st, int uplo,
-                  const plasma_desc_t &A, void *W, int nblk)
+                  const plasma_desc_t &A, void *W, int nblk, int unit = 0)
 {
     static unsigned long long attr = 0;
     if (plasma_first_on_device(&attr)) {
@@ -968,7 +969,7 @@ void launch_trtri(cudaStream_t s, plasma_devstat_t *st, int uplo,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                              trtri_smem<T, SB>());
     }
-    k_trtri_blocks<T, SB><<<nblk, 256, trtri_smem<T, SB>(), s>>>(A, uplo, (T *)W, st);
+    k_trtri_blocks<T, SB><<<nblk, 256, trtri_smem<T, SB>(), s>>>(A, uplo, unit, (T *)W, st);
 }
 
 template <typename T, int SB>
@@ -1081,6 +1082,32 @@ extern "C" void plasma_cuda_trtri_blocks(cudaStream_t s, plasma_devstat_t *st,
         PLASMA_COUNT_LAUNCH();
         launch_couple(s, st, uplo, A, W, nblk);
     }
+}
+
+// The block inverses for the one-launch sweeps with an LU factor held in
+// the general tile matrix A (unit-lower L below the diagonal, U on and
+// above it): Wf for L y = b (the sweep with uplo = Lower, forward), Wb for
+// U x = y (uplo = Upper, backward: U is the transpose of the logical lower
+// factor of upper storage).  Returns 0 (nothing launched) unless the sweep
+// block is 64 rows (FP64 tiles, or FP32 tiles whose size is an odd multiple
+// of 64).
+extern "C" int plasma_cuda_trtri_blocks_lu(cudaStream_t s, plasma_devstat_t *st,
+                                           plasma_desc_t A, void *Wf, void *Wb)
+{
+    const int sb = plasma_cuda_trsv_block(A);
+    if (sb != 64) return 0;
+    const int nblk = (A.m + sb - 1) / sb;
+    if (nblk == 0) return 1;
+    PLASMA_COUNT_LAUNCH();
+    PLASMA_COUNT_LAUNCH();
+    if (A.precision == PlasmaRealDouble) {
+        launch_trtri<double, 64>(s, st, PlasmaLower, A, Wf, nblk, 1);
+        launch_trtri<double, 64>(s, st, PlasmaUpper, A, Wb, nblk, 0);
+    } else {
+        launch_trtri<float, 64>(s, st, PlasmaLower, A, Wf, nblk, 1);
+        launch_trtri<float, 64>(s, st, PlasmaUpper, A, Wb, nblk, 0);
+    }
+    return 1;
 }
 
 // In-place solve of op(L) x = vec for one right-hand side (vec contiguous):

@@ -217,6 +217,10 @@ void plasma_cuda_potrf_tile(cudaStream_t s, plasma_devstat_t *st, int call,
 int plasma_cuda_trsm_tc(cudaStream_t s, plasma_devstat_t *st, int mode, plasma_desc_t A,
                         int k, int mlo, int mhi, void *wimg, void *panel, int full);
 size_t plasma_cuda_trsm_tc_bytes(int nb);
+/* Block inverses for the one-launch sweeps with an LU factor (unit-lower L
+ * forward, U backward); 0 when the sweep block is not 64 rows. */
+int plasma_cuda_trtri_blocks_lu(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t A,
+                                void *Wf, void *Wb);
 void plasma_cuda_trsm_panel(cudaStream_t s, plasma_devstat_t *st,
                             plasma_enum_t uplo, plasma_desc_t A, int k,
                             int mlo, int mhi, const void *winv);
@@ -415,8 +419,15 @@ void plasma_cuda_laswp(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t D,
                        const int *ipiv, int j0, int j1, int c0, int c1);
 void plasma_cuda_trtri_lu(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t A,
                           int k0, int k1, void *WL, void *WU);
+/* ||A||_inf and y -= A x (one right-hand side) of a general tile matrix;
+ * part: scratch of plasma_cuda_gemv_part_bytes(A) bytes. */
+size_t plasma_cuda_gemv_part_bytes(plasma_desc_t A);
+/* Largest panel height that the one-launch LU panel takes (64-wide tiles). */
+int plasma_cuda_getrf_cluster_rows(int precision);
 void plasma_cuda_lange_inf(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t A,
-                           double *dnorm);
+                           double *dnorm, double *part);
+void plasma_cuda_gemv_sub(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t A,
+                          const void *x, void *y, double *part);
 void plasma_cuda_colmax(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t D,
                         double *out);
 
