@@ -80,6 +80,8 @@ typedef struct {
     void *parts;           /* per-CTA pivot candidates of the panel  */
     void *Wf, *Wb;         /* block inverses of the one-launch sweeps */
     int sweeps;            /* Wf, Wb hold the current factor's        */
+    int *perm;             /* the interchanges as one permutation     */
+    int permuted;          /* perm holds the current factor's         */
 } lu_work_t;
 
 static int lu_work(plasma_context_t *plasma, plasma_desc_t A, int ncols, lu_work_t *w)
@@ -88,7 +90,8 @@ static int lu_work(plasma_context_t *plasma, plasma_desc_t A, int ncols, lu_work
     const size_t nbsq = (size_t)A.mb * A.mb;
     const size_t wsw = (plasma_cuda_trsv_w_bytes(A) + 255) & ~(size_t)255;
     char *buf = (char *)plasma_scratch(plasma, PLASMA_SLOT_WORK,
-                                       2 * A.mt * nbsq * es + 2 * wsw + 256);
+                                       2 * A.mt * nbsq * es + 2 * wsw +
+                                           sizeof(int) * ((size_t)A.m + 8) + 256);
     const size_t cols = (size_t)(ncols > A.n ? ncols : A.n);
     void *tmp = plasma_scratch(plasma, PLASMA_SLOT_ADJOINT, (size_t)A.mb * cols * es + 256);
     void *parts = plasma_scratch(plasma, PLASMA_SLOT_MIXED, plasma_cuda_getrf_parts_bytes(A));
@@ -100,6 +103,8 @@ static int lu_work(plasma_context_t *plasma, plasma_desc_t A, int ncols, lu_work
     w->Wf = buf + 2 * A.mt * nbsq * es;
     w->Wb = (char *)w->Wf + wsw;
     w->sweeps = 0;
+    w->permuted = 0;
+    w->perm = (int *)((char *)w->Wb + wsw);
     plasma_desc_general_init(A.precision, w->WL, A.mb, A.mb, A.mb, A.mt * A.mb, 0, 0,
                              A.mb, A.mt * A.mb, &w->Wd);
     plasma_desc_general_init(A.precision, w->WU, A.mb, A.mb, A.mb, A.mt * A.mb, 0, 0,
@@ -138,12 +143,12 @@ static void plasma_pXgetrf(plasma_context_t *plasma, plasma_desc_t A, int *dpiv,
         const int kb = plasma_tile_nview(A, k);
         const int r0 = k * A.mb, c1 = r0 + kb;
         plasma_cuda_getrf_panel(S, st, call, A, k, dpiv, w->parts);
-        plasma_cuda_laswp(S, st, A, dpiv, r0, r0 + kb, 0, r0);
-        plasma_cuda_laswp(S, st, A, dpiv, r0, r0 + kb, c1, A.n);
+        plasma_cuda_laswp_skip(S, st, A, dpiv, r0, r0 + kb, 0, A.n, r0, c1);
         plasma_cuda_trtri_lu(S, st, A, k, k + 1, w->WL, w->WU);
         if (c1 < A.n) {
-            apply_inverse(plasma, w, w->Wd, A, k, kb, c1, A.n - c1);
-            if (c1 < A.m)
+            if (!plasma_cuda_lu_rowsolve(S, st, A, k, w->WL))
+                apply_inverse(plasma, w, w->Wd, A, k, kb, c1, A.n - c1);
+            if (c1 < A.m && !plasma_cuda_lu_update(S, st, A, k))
                 plasma_cuda_gemm_view(S, st, A.m - c1, A.n - c1, kb, -1.0, view(A, c1, r0),
                                       view(A, r0, c1), 1.0, view(A, c1, c1), 0, 0);
         }
@@ -151,6 +156,7 @@ static void plasma_pXgetrf(plasma_context_t *plasma, plasma_desc_t A, int *dpiv,
     /* the block inverses of the one-launch sweeps (one right-hand side) */
     w->sweeps = plasma_sweep_reserve(plasma, A) &&
                 plasma_cuda_trtri_blocks_lu(S, st, A, w->Wf, w->Wb);
+    w->permuted = plasma_cuda_lu_perm(S, st, dpiv, A.m, w->perm);
 }
 
 /* A X = B with the factor of plasma_pXgetrf (pivots dpiv, inverses in w):
@@ -161,7 +167,8 @@ static void plasma_pXgetrs(plasma_context_t *plasma, plasma_desc_t A, const int 
     cudaStream_t S = plasma->stream;
     plasma_devstat_t *st = plasma->dstat;
     const int mt = A.mt, N = B.n;
-    plasma_cuda_laswp(S, st, B, dpiv, 0, A.m, 0, N);
+    if (!(N == 1 && w->permuted && plasma_cuda_permute_vec(S, st, B, 0, w->perm, A.m)))
+        plasma_cuda_laswp(S, st, B, dpiv, 0, A.m, 0, N);
     /* one right-hand side (a contiguous vector): the one-launch sweeps,
      * L y = P b (unit lower, forward), then U x = y (backward) */
     if (w->sweeps && N == 1 && B.gn == 1 && B.nt == 1) {

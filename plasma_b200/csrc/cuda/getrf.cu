@@ -31,6 +31,7 @@
 // for FP64, the three-product TF32 split for FP32).
 #include "common.cuh"
 #include "inv64.cuh"
+#include "mma.cuh"
 
 #include <float.h>
 #include <limits.h>
@@ -198,10 +199,10 @@ constexpr int LW_COLS = LW_WARPS * LW_COLS_PER_WARP;
 
 template <typename T>
 __global__ void __launch_bounds__(32 * LW_WARPS)
-k_laswp_rows(plasma_desc_t D, const int *ipiv, int j0, int nj, int c0, int c1,
-             const plasma_devstat_t *st)
+k_laswp_rows(plasma_desc_t D, const int *ipiv, int j0, int nj, int c0, int c1, int skip0,
+             int skip1, const plasma_devstat_t *st)
 {
-    __shared__ int tgt[64], slot[64], src[128], row[128];
+    __shared__ int tgt[64], slot[64], src[128], row[128], pos_of_slot[64];
     __shared__ int npos;
     if (plasma_failed(st)) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -223,7 +224,6 @@ k_laswp_rows(plasma_desc_t D, const int *ipiv, int j0, int nj, int c0, int c1,
             row[r] = j0 + r;
             src[r] = r;
         }
-        int pos_of_slot[64];
         for (int q = 0; q < nj; q++) {
             if (slot[q] == q) {
                 pos_of_slot[q] = np;
@@ -245,7 +245,8 @@ k_laswp_rows(plasma_desc_t D, const int *ipiv, int j0, int nj, int c0, int c1,
     __syncthreads();
     const int np = npos;
     for (int q = 0; q < LW_COLS_PER_WARP; q++) {
-        const int c = c0 + blockIdx.x * LW_COLS + warp * LW_COLS_PER_WARP + q;
+        int c = c0 + blockIdx.x * LW_COLS + warp * LW_COLS_PER_WARP + q;
+        if (c >= skip0) c += skip1 - skip0;           // columns [skip0, skip1) are left out
         if (c >= c1) break;
         const int tn = c / D.nb, cc = c - tn * D.nb;
         auto at = [&](int r) -> T * {
@@ -301,6 +302,50 @@ k_laswp_vec(plasma_desc_t D, int col, const int *ipiv, int n, const plasma_devst
     }
     __syncthreads();
     for (int r = threadIdx.x; r < n; r += blockDim.x) *at(r) = v[r];
+}
+
+// The interchanges ipiv[0 .. n) composed into one permutation, once per
+// factorization: perm[i] = the row whose entry ends at row i (one thread
+// walks the swaps in shared memory).
+__global__ void __launch_bounds__(256)
+k_ipiv_perm(const int *ipiv, int n, int *perm, const plasma_devstat_t *st)
+{
+    extern __shared__ int ip_raw[];
+    int *idx = ip_raw, *pv = ip_raw + n;
+    if (plasma_failed(st)) return;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+        idx[r] = r;
+        pv[r] = ipiv[r] - 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int j = 0; j < n; j++) {
+            const int p = pv[j], x = idx[j];
+            idx[j] = idx[p];
+            idx[p] = x;
+        }
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < n; r += blockDim.x) perm[r] = idx[r];
+}
+
+// column col of D (n rows) <- its rows in the order perm
+template <typename T>
+__global__ void __launch_bounds__(1024)
+k_permute_vec(plasma_desc_t D, int col, const int *perm, int n, const plasma_devstat_t *st)
+{
+    extern __shared__ __align__(16) unsigned char pm_raw[];
+    T *v = reinterpret_cast<T *>(pm_raw);
+    if (plasma_failed(st)) return;
+    const int tn = col / D.nb, cc = col - tn * D.nb;
+    auto at = [&](int r) -> T * {
+        const int tm = r / D.mb;
+        return (T *)plasma_tile_addr(D, tm, tn) + (size_t)cc * plasma_tile_mmain(D, tm) +
+               (r - tm * D.mb);
+    };
+    for (int r = threadIdx.x; r < n; r += blockDim.x) v[r] = *at(r);
+    __syncthreads();
+    for (int r = threadIdx.x; r < n; r += blockDim.x) *at(r) = v[perm[r]];
 }
 
 // 64-wide tiles: CTA 2q inverts the unit-lower part of diagonal tile
@@ -373,6 +418,169 @@ k_trtri_lu(plasma_desc_t A, int k0, T *WL, T *WU, const plasma_devstat_t *st)
             for (int l = i + 1; l <= j; l++) s += a[(size_t)l * lda + i] * xu[l];
             xu[i] = -s / a[(size_t)i * lda + i];
         }
+    }
+}
+
+// The trailing update of step k for 64 x 64 FP32 tiles,
+//     A(m, n) -= A(m, k) A(k, n),   m, n > k,
+// on the tensor cores (mma.sync, the three-product TF32 split, FP32
+// accuracy).  A CTA owns a 128 x 128 block of C (two tile rows, two tile
+// columns) and the whole K = 64: L's two tiles and U's two tiles are copied
+// in by 16-byte cp.async (the tiles are contiguous, column-major), L as
+// As[k][i] and U as Bs[j][k] (both padded for conflict-free fragment
+// loads); eight warps of 64 x 32, then C -= the product in place.
+constexpr int LG_THREADS = 256;
+constexpr int LG_LDA = 128 + 8, LG_LDB = 64 + 4;
+constexpr int LG_SMEM = (64 * LG_LDA + 128 * LG_LDB) * 4;
+
+// acc (a warp's 64 x 32 block at rows wm, columns wn) = As^T-view x Bs over
+// K = 64: As[k][i] (rows i), Bs[j][k] (columns j)
+__device__ __forceinline__ void lg_product(const float *As, const float *Bs, int wm, int wn,
+                                           int g, int t, float (&acc)[4][4][4])
+{
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) acc[a][b][c] = 0.f;
+#pragma unroll 2
+    for (int k8 = 0; k8 < 64; k8 += 8) {
+        float bf[4][2];
+#pragma unroll
+        for (int ni = 0; ni < 4; ni++) {
+            bf[ni][0] = Bs[(wn + ni * 8 + g) * LG_LDB + k8 + t];
+            bf[ni][1] = Bs[(wn + ni * 8 + g) * LG_LDB + k8 + t + 4];
+        }
+#pragma unroll
+        for (int mi = 0; mi < 4; mi++) {
+            float af[4];
+            af[0] = As[(k8 + t) * LG_LDA + wm + mi * 16 + g];
+            af[1] = As[(k8 + t) * LG_LDA + wm + mi * 16 + g + 8];
+            af[2] = As[(k8 + t + 4) * LG_LDA + wm + mi * 16 + g];
+            af[3] = As[(k8 + t + 4) * LG_LDA + wm + mi * 16 + g + 8];
+#pragma unroll
+            for (int ni = 0; ni < 4; ni++) mma8<3>(acc[mi][ni], af, bf[ni]);
+        }
+    }
+}
+
+// 64 x 64 column-major tile (ld, rows x cols valid, zero elsewhere) into
+// shared memory: as rows (dst[c*ldd + i]) or, transposed, as columns
+// (dst[j*ldd + k] = t(k, j), k the row)
+__device__ __forceinline__ void lg_stage(float *dst, int ldd, const float *src, int ld,
+                                         int rows, int cols, int tid, int nthreads)
+{
+    for (int e = tid; e < 64 * 16; e += nthreads) {
+        const int c = e / 16, q = e % 16;              // column c, rows 4q .. 4q+3
+        float *d = &dst[c * ldd + 4 * q];
+        if (src != nullptr && c < cols && 4 * q + 3 < rows && (ld & 3) == 0) {
+            cp_async_16(d, src + (size_t)c * ld + 4 * q, true);
+        } else {
+            for (int r = 0; r < 4; r++)
+                d[r] = (src != nullptr && c < cols && 4 * q + r < rows)
+                           ? src[(size_t)c * ld + 4 * q + r] : 0.f;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(LG_THREADS, 2)
+k_lu_gemm(plasma_desc_t A, int k, const plasma_devstat_t *st)
+{
+    extern __shared__ __align__(16) float lg_raw[];
+    float *As = lg_raw;                        // [64][LG_LDA]  L(m..m+1, k)
+    float *Bs = lg_raw + 64 * LG_LDA;          // [128][LG_LDB] U(k, n..n+1), [j][k]
+    if (plasma_failed(st)) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int m0 = k + 1 + 2 * blockIdx.y, n0 = k + 1 + 2 * blockIdx.x;
+    const int kb = plasma_tile_nview(A, k);
+    // operand tiles (a missing second tile, or a ragged one, reads as zero)
+    for (int h = 0; h < 2; h++) {
+        const int m = m0 + h;
+        const bool mv = m < A.mt;
+        lg_stage(As + 64 * h, LG_LDA, mv ? (const float *)plasma_tile_addr(A, m, k) : nullptr,
+                 mv ? plasma_tile_mmain(A, m) : 0, mv ? plasma_tile_mview(A, m) : 0, kb, tid,
+                 LG_THREADS);
+        const int n = n0 + h;
+        const bool nv = n < A.nt;
+        lg_stage(Bs + 64 * h * LG_LDB, LG_LDB,
+                 nv ? (const float *)plasma_tile_addr(A, k, n) : nullptr,
+                 plasma_tile_mmain(A, k), kb, nv ? plasma_tile_nview(A, n) : 0, tid, LG_THREADS);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+
+    const int wm = (warp >> 2) * 64, wn = (warp & 3) * 32;
+    float acc[4][4][4];
+    lg_product(As, Bs, wm, wn, g, t, acc);
+    // C -= acc, tile by tile (rows of a fragment are 8 apart, columns 2t, 2t+1)
+#pragma unroll
+    for (int mi = 0; mi < 4; mi++) {
+        const int rr = wm + mi * 16;                   // 16 rows of one C tile
+        const int m = m0 + rr / 64;
+        if (m >= A.mt) continue;
+        const int rows = plasma_tile_mview(A, m), ld = plasma_tile_mmain(A, m);
+#pragma unroll
+        for (int ni = 0; ni < 4; ni++) {
+            const int cc = wn + ni * 8;
+            const int n = n0 + cc / 64;
+            if (n >= A.nt) continue;
+            const int cols = plasma_tile_nview(A, n);
+            float *c = (float *)plasma_tile_addr(A, m, n);
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const int i = rr % 64 + g + 8 * (e >> 1), j = cc % 64 + 2 * t + (e & 1);
+                if (i < rows && j < cols) c[(size_t)j * ld + i] -= acc[mi][ni][e];
+            }
+        }
+    }
+}
+
+// The block row of LU step k: A(k, n) <- W A(k, n), n > k, with W the
+// inverse of the unit-lower diagonal tile (64 x 64 FP32 tiles): two tile
+// columns per CTA of four warps, the tiles copied into shared memory before
+// they are overwritten.
+__global__ void __launch_bounds__(128)
+k_lu_rowsolve(plasma_desc_t A, int k, const float *W, const plasma_devstat_t *st)
+{
+    extern __shared__ __align__(16) float lg_raw[];
+    float *As = lg_raw;                        // [64][LG_LDA]  W
+    float *Bs = lg_raw + 64 * LG_LDA;          // [128][LG_LDB] A(k, n..n+1), [j][k]
+    if (plasma_failed(st)) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int n0 = k + 1 + 2 * blockIdx.x;
+    const int kb = plasma_tile_mview(A, k);
+    lg_stage(As, LG_LDA, W + (size_t)k * 64 * 64, 64, kb, kb, tid, 128);
+    for (int h = 0; h < 2; h++) {
+        const int n = n0 + h;
+        const bool nv = n < A.nt;
+        lg_stage(Bs + 64 * h * LG_LDB, LG_LDB,
+                 nv ? (const float *)plasma_tile_addr(A, k, n) : nullptr,
+                 plasma_tile_mmain(A, k), kb, nv ? plasma_tile_nview(A, n) : 0, tid, 128);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    float acc[4][4][4];
+    lg_product(As, Bs, 0, warp * 32, g, t, acc);
+    const int ld = plasma_tile_mmain(A, k);
+#pragma unroll
+    for (int ni = 0; ni < 4; ni++) {
+        const int cc = warp * 32 + ni * 8;
+        const int n = n0 + cc / 64;
+        if (n >= A.nt) continue;
+        const int cols = plasma_tile_nview(A, n);
+        float *c = (float *)plasma_tile_addr(A, k, n);
+#pragma unroll
+        for (int mi = 0; mi < 4; mi++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const int i = mi * 16 + g + 8 * (e >> 1), j = cc % 64 + 2 * t + (e & 1);
+                if (i < kb && j < cols) c[(size_t)j * ld + i] = acc[mi][ni][e];
+            }
     }
 }
 
@@ -572,14 +780,16 @@ k_lu_panel_cl(plasma_desc_t A, int k, int kb, int R, int *ipiv, plasma_devstat_t
 
     for (int s0 = 0; s0 < kb; s0 += CL_IB) {
         const int ce = min(kb, s0 + CL_IB);
+        // this thread's candidate for the next column: found by a scan at the
+        // start of a sub-block, then by each column's rank-1 update
+        T bv = T(-1);
+        int bi = INT_MAX;
+        for (int r = tid; r < nown; r += CL_THREADS)
+            if (row0 + r >= s0) max_pick(bv, bi, (T)fabs(P[(size_t)s0 * R + r]), row0 + r);
         for (int j = s0; j < ce; j++) {
             const int par = j & 1;
             T *slot = pub_row + par * 2 * CL_KB;
             // 1. this CTA's candidate for column j and its row
-            T bv = T(-1);
-            int bi = INT_MAX;
-            for (int r = tid; r < nown; r += CL_THREADS)
-                if (row0 + r >= j) max_pick(bv, bi, (T)fabs(P[(size_t)j * R + r]), row0 + r);
             block_best(bv, bi, red_v, red_i);
             if (tid == 0) {
                 pub_val[par] = bv;
@@ -630,33 +840,40 @@ k_lu_panel_cl(plasma_desc_t A, int k, int kb, int R, int *ipiv, plasma_devstat_t
                 prow[tid] = x;
             }
             __syncthreads();
-            if (p != j) {
-                for (int c = tid; c < kb; c += CL_THREADS) {
-                    if (cj == (int)me) P[(size_t)c * R + (j - row0)] = prow[c];
-                    if (cp == (int)me) P[(size_t)c * R + (p - row0)] = rowj[c];
-                }
-            }
             const T piv = prow[j];
             if (me == 0 && tid == 0) {
                 ipiv[d0 + j] = d0 + p + 1;
                 if (piv == T(0)) plasma_fail(st, d0 + j + 1, call);
             }
-            __syncthreads();
-            // 4. scale the rows below j, rank-1 update inside the sub-block
-            if (piv != T(0)) {
-                // LAPACK's dgetf2: a reciprocal unless the pivot is tiny
-                const bool rcp = (T)fabs(piv) >= tiny<T>();
-                const T rp = T(1) / piv;
-                for (int r = tid; r < nown; r += CL_THREADS) {
-                    if (row0 + r <= j) continue;
+            // 4. the swap (a thread per column), then the rows below j:
+            // scaled, rank-1 update inside the sub-block, and the candidate
+            // for column j+1 on the way
+            if (p != j) {
+                for (int c = tid; c < kb; c += CL_THREADS) {
+                    if (cj == (int)me) P[(size_t)c * R + (j - row0)] = prow[c];
+                    if (cp == (int)me) P[(size_t)c * R + (p - row0)] = rowj[c];
+                }
+                __syncthreads();
+            }
+            const bool rcp = (T)fabs(piv) >= tiny<T>();
+            const T rp = piv != T(0) ? T(1) / piv : T(0);
+            bv = T(-1);
+            bi = INT_MAX;
+            for (int r = tid; r < nown; r += CL_THREADS) {
+                const int pr = row0 + r;
+                if (pr <= j) continue;
+                if (piv != T(0)) {
+                    // LAPACK's dgetf2: a reciprocal unless the pivot is tiny
                     T *lr = &P[(size_t)j * R + r];
                     const T l = rcp ? *lr * rp : *lr / piv;
                     *lr = l;
                     for (int c = j + 1; c < ce; c++) P[(size_t)c * R + r] -= l * prow[c];
                 }
+                if (j + 1 < ce)
+                    max_pick(bv, bi, (T)fabs(P[(size_t)(j + 1) * R + r]), pr);
             }
-            __syncthreads();
         }
+        __syncthreads();
         if (ce >= kb) break;
         // 5. the sub-block's rows to every CTA, U12 = L11^-1 A12, A22 -= L21 U12
         const int nsb = ce - s0;
@@ -829,6 +1046,82 @@ extern "C" void plasma_cuda_getrf_panel(cudaStream_t s, plasma_devstat_t *st, in
                     2.0 * (double)M * kb * es);
 }
 
+// The trailing update of LU step k on the tensor cores for 64 x 64 FP32
+// tiles; returns 0 (nothing launched) for other tilings.
+extern "C" int plasma_cuda_lu_update(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t A,
+                                     int k)
+{
+    if (A.precision != PlasmaRealFloat || A.mb != 64 || A.nb != 64) return 0;
+    const int rt = A.mt - k - 1, ct = A.nt - k - 1;
+    if (rt <= 0 || ct <= 0) return 1;
+    static unsigned long long attr = 0;
+    if (plasma_first_on_device(&attr))
+        cudaFuncSetAttribute(k_lu_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, LG_SMEM);
+    PLASMA_COUNT_LAUNCH();
+    const double M = A.m - (k + 1) * 64.0, N = A.n - (k + 1) * 64.0;
+    int prof = plasma_prof_begin(s);
+    dim3 grid((unsigned)((ct + 1) / 2), (unsigned)((rt + 1) / 2));
+    k_lu_gemm<<<grid, LG_THREADS, LG_SMEM, s>>>(A, k, st);
+    plasma_prof_end(prof, s, PLASMA_KCLASS_UPDATE, 2.0 * M * N * 64.0, 4.0 * (2.0 * M * N));
+    return 1;
+}
+
+// The block row of LU step k, A(k, n) <- WL_k A(k, n) for n > k (WL: the
+// inverses of the unit-lower diagonal tiles, 64 x 64 each); 0 (nothing
+// launched) for other tilings.
+extern "C" int plasma_cuda_lu_rowsolve(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t A,
+                                       int k, const void *WL)
+{
+    if (A.precision != PlasmaRealFloat || A.mb != 64 || A.nb != 64) return 0;
+    const int ct = A.nt - k - 1;
+    if (ct <= 0) return 1;
+    static unsigned long long attr = 0;
+    if (plasma_first_on_device(&attr))
+        cudaFuncSetAttribute(k_lu_rowsolve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             LG_SMEM);
+    PLASMA_COUNT_LAUNCH();
+    k_lu_rowsolve<<<(unsigned)((ct + 1) / 2), 128, LG_SMEM, s>>>(A, k, (const float *)WL, st);
+    return 1;
+}
+
+// perm (device, n ints) <- the composition of the interchanges ipiv[0 .. n);
+// 0 (nothing launched) when n is too large for one CTA's shared memory.
+extern "C" int plasma_cuda_lu_perm(cudaStream_t s, plasma_devstat_t *st, const int *ipiv,
+                                   int n, int *perm)
+{
+    const size_t bytes = 2 * sizeof(int) * (size_t)n;
+    if (n <= 0 || bytes > 200 * 1024) return 0;
+    static unsigned long long attr = 0;
+    if (plasma_first_on_device(&attr))
+        cudaFuncSetAttribute(k_ipiv_perm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             200 * 1024);
+    PLASMA_COUNT_LAUNCH();
+    k_ipiv_perm<<<1, 256, bytes, s>>>(ipiv, n, perm, st);
+    return 1;
+}
+
+// The rows of column col of D reordered by perm (plasma_cuda_lu_perm): the
+// interchanges applied to a right-hand side.  0 when n is too large.
+extern "C" int plasma_cuda_permute_vec(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t D,
+                                       int col, const int *perm, int n)
+{
+    const size_t bytes = plasma_element_size(D.precision) * (size_t)n;
+    if (n <= 0 || bytes > 200 * 1024) return 0;
+    static unsigned long long attr = 0;
+    if (plasma_first_on_device(&attr)) {
+        cudaFuncSetAttribute(k_permute_vec<double>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(k_permute_vec<float>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    }
+    PLASMA_COUNT_LAUNCH();
+    if (D.precision == PlasmaRealDouble)
+        k_permute_vec<double><<<1, 1024, bytes, s>>>(D, col, perm, n, st);
+    else
+        k_permute_vec<float><<<1, 1024, bytes, s>>>(D, col, perm, n, st);
+    return 1;
+}
+
 // Largest panel height of the cluster panel kernel for 64-wide tiles.
 extern "C" int plasma_cuda_getrf_cluster_rows(int precision)
 {
@@ -866,14 +1159,30 @@ extern "C" void plasma_cuda_laswp(cudaStream_t s, plasma_devstat_t *st, plasma_d
         return;
     }
     // up to 64 rows at a time: the block kernel
-    const unsigned grid = (unsigned)((c1 - c0 + LW_COLS - 1) / LW_COLS);
+    plasma_cuda_laswp_skip(s, st, D, ipiv, j0, j1, c0, c1, c1, c1);
+}
+
+// As plasma_cuda_laswp on the columns [c0, c1) except [skip0, skip1), in
+// one launch per 64 rows.
+extern "C" void plasma_cuda_laswp_skip(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t D,
+                                       const int *ipiv, int j0, int j1, int c0, int c1,
+                                       int skip0, int skip1)
+{
+    skip0 = max(skip0, c0);
+    skip1 = max(skip0, min(skip1, c1));
+    const int ncols = c1 - c0 - (skip1 - skip0);
+    if (j1 <= j0 || ncols <= 0) return;
+    const bool dp = D.precision == PlasmaRealDouble;
+    const unsigned grid = (unsigned)((ncols + LW_COLS - 1) / LW_COLS);
     for (int b = j0; b < j1; b += 64) {
         const int nj = min(64, j1 - b);
         PLASMA_COUNT_LAUNCH();
         if (dp)
-            k_laswp_rows<double><<<grid, 32 * LW_WARPS, 0, s>>>(D, ipiv, b, nj, c0, c1, st);
+            k_laswp_rows<double><<<grid, 32 * LW_WARPS, 0, s>>>(D, ipiv, b, nj, c0, c1, skip0,
+                                                               skip1, st);
         else
-            k_laswp_rows<float><<<grid, 32 * LW_WARPS, 0, s>>>(D, ipiv, b, nj, c0, c1, st);
+            k_laswp_rows<float><<<grid, 32 * LW_WARPS, 0, s>>>(D, ipiv, b, nj, c0, c1, skip0,
+                                                              skip1, st);
     }
 }
 

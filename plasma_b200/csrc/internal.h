@@ -417,11 +417,26 @@ void plasma_cuda_getrf_panel(cudaStream_t s, plasma_devstat_t *st, int call,
 size_t plasma_cuda_getrf_parts_bytes(plasma_desc_t A);
 void plasma_cuda_laswp(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t D,
                        const int *ipiv, int j0, int j1, int c0, int c1);
+void plasma_cuda_laswp_skip(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t D,
+                            const int *ipiv, int j0, int j1, int c0, int c1, int skip0,
+                            int skip1);
 void plasma_cuda_trtri_lu(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t A,
                           int k0, int k1, void *WL, void *WU);
 /* ||A||_inf and y -= A x (one right-hand side) of a general tile matrix;
  * part: scratch of plasma_cuda_gemv_part_bytes(A) bytes. */
 size_t plasma_cuda_gemv_part_bytes(plasma_desc_t A);
+/* LU trailing update A(m,n) -= A(m,k) A(k,n), m, n > k, for 64 x 64 FP32
+ * tiles on the tensor cores; 0 (nothing launched) for other tilings. */
+int plasma_cuda_lu_update(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t A, int k);
+/* LU block row A(k,n) <- WL_k A(k,n), n > k, for 64 x 64 FP32 tiles. */
+int plasma_cuda_lu_rowsolve(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t A, int k,
+                            const void *WL);
+/* The LU's interchanges composed into one permutation, and applied to one
+ * column; 0 (nothing launched) when n is too large for one CTA. */
+int plasma_cuda_lu_perm(cudaStream_t s, plasma_devstat_t *st, const int *ipiv, int n,
+                        int *perm);
+int plasma_cuda_permute_vec(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t D, int col,
+                            const int *perm, int n);
 /* Largest panel height that the one-launch LU panel takes (64-wide tiles). */
 int plasma_cuda_getrf_cluster_rows(int precision);
 void plasma_cuda_lange_inf(cudaStream_t s, plasma_devstat_t *st, plasma_desc_t A,
