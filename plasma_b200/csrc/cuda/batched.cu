@@ -18,8 +18,11 @@
 //   (b) every thread solves one row of the panel below, x D^T = a, with D
 //       in shared memory; the panel is kept in shared memory;
 //   (c) the trailing lower triangle is updated, A22 -= P P^T, by warps on
-//       32 x 32 blocks with DMMA (FP64) or the three-product TF32 split
-//       (FP32, FP32-accurate), C read and written in global memory (L2).
+//       16 x 32 blocks with DMMA (FP64) or the three-product TF32 split
+//       (FP32, FP32-accurate), C read (before the products, so the read
+//       overlaps them) and written in global memory (L2); the first 32
+//       columns first, then warp 0 factors the next diagonal block while
+//       the other warps update the rest.
 // The solve follows in the same CTA while the factor is in L2: forward by
 // block (diagonal block by one warp, the rows below by all threads),
 // backward by block (column dot products by warps, then the diagonal block).
@@ -62,57 +65,73 @@ struct BatchArgs {
 };
 
 // ------------------------------------------------------------------ factor
+// The diagonal block at j0 (jb x jb, lower), factored by one warp, lane r
+// holding row r, pivots broadcast by shuffles; writes it to A and Ds, the
+// reciprocal pivots to rdiag and the first bad pivot (LAPACK's info within
+// the block, 0 if none) to *flag.
+template <typename T, int NB>
+__device__ __forceinline__ void diag_block(T *A, int n, int j0, int jb, T *Ds, T *rdiag,
+                                           int *flag, int lane)
+{
+    T v[NB];
+#pragma unroll
+    for (int c = 0; c < NB; c++)
+        v[c] = (lane < jb && c < jb && lane >= c) ? A[(size_t)(j0 + c) * n + j0 + lane] : T(0);
+    int bad = 0;
+    T myrd = T(1);
+#pragma unroll
+    for (int c = 0; c < NB; c++) {
+        if (c < jb) {
+            T d = __shfl_sync(0xffffffffu, v[c], c);
+            bool ok = d > T(0);
+            if (!ok && bad == 0) bad = c + 1;
+            // one reciprocal square root per pivot: 1/sqrt(d), sqrt(d) = d/sqrt(d)
+            T rd = ok ? rsqrt(d) : T(1);
+            T sd = ok ? d * rd : T(1);
+            if (lane == c) myrd = rd;
+            if (lane >= c) v[c] = (lane == c) ? sd : v[c] * rd;
+            // a fixed trip count keeps v[] in registers (full unroll)
+#pragma unroll
+            for (int c2 = 0; c2 < NB; c2++) {
+                if (c2 > c) {
+                    T l = __shfl_sync(0xffffffffu, v[c], c2);
+                    if (c2 < jb && lane >= c2) v[c2] -= v[c] * l;
+                }
+            }
+        }
+    }
+    if (lane < jb) {
+#pragma unroll
+        for (int c = 0; c < NB; c++)
+            if (c < jb && lane >= c) {
+                A[(size_t)(j0 + c) * n + j0 + lane] = v[c];
+                Ds[c * (NBMAXB + 1) + lane] = v[c];
+            }
+        rdiag[lane] = myrd;
+    }
+    if (lane == 0) *flag = bad;
+}
+
+// Per block column j0: (b) the panel below the diagonal block, a thread per
+// row, x D^T = a (kept in shared memory); (c1) the trailing update of the
+// first 32 columns of A22 (they hold the next diagonal block and the next
+// panel); then warp 0 factors the next diagonal block (a) while the other
+// warps finish the trailing update (c2), so the single-warp chain of (a)
+// overlaps the tensor work.  The trailing update runs on 16 x 32 blocks of
+// the lower triangle with DMMA (FP64) or the three-product TF32 split
+// (FP32); a warp's block of C is read into registers before its products,
+// so the L2 latency of the read overlaps them.
 template <typename T, int SPLIT, int NB>
 __device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag)
 {
     constexpr int PLD = ps_ld<T>();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, t = lane & 3;
+    if (warp == 0) diag_block<T, NB>(A, n, 0, min(NB, n), Ds, rdiag, flag, lane);
+    __syncthreads();
     for (int j0 = 0; j0 < n; j0 += NB) {
         const int jb = min(NB, n - j0);
         const int m2 = n - j0 - jb;
-        // (a) diagonal block
-        if (warp == 0) {
-            T v[NB];
-#pragma unroll
-            for (int c = 0; c < NB; c++)
-                v[c] = (lane < jb && c < jb && lane >= c) ? A[(size_t)(j0 + c) * n + j0 + lane]
-                                                          : T(0);
-            int bad = 0;
-            T myrd = T(1);
-#pragma unroll
-            for (int c = 0; c < NB; c++) {
-                if (c < jb) {
-                    T d = __shfl_sync(0xffffffffu, v[c], c);
-                    bool ok = d > T(0);
-                    if (!ok && bad == 0) bad = c + 1;
-                    // one reciprocal square root per pivot: 1/sqrt(d), sqrt(d) = d/sqrt(d)
-                    T rd = ok ? rsqrt(d) : T(1);
-                    T sd = ok ? d * rd : T(1);
-                    if (lane == c) myrd = rd;
-                    if (lane >= c) v[c] = (lane == c) ? sd : v[c] * rd;
-                    // a fixed trip count keeps v[] in registers (full unroll)
-#pragma unroll
-                    for (int c2 = 0; c2 < NB; c2++) {
-                        if (c2 > c) {
-                            T l = __shfl_sync(0xffffffffu, v[c], c2);
-                            if (c2 < jb && lane >= c2) v[c2] -= v[c] * l;
-                        }
-                    }
-                }
-            }
-            if (lane < jb) {
-#pragma unroll
-                for (int c = 0; c < NB; c++)
-                    if (c < jb && lane >= c) {
-                        A[(size_t)(j0 + c) * n + j0 + lane] = v[c];
-                        Ds[c * (NBMAXB + 1) + lane] = v[c];
-                    }
-                rdiag[lane] = myrd;
-            }
-            if (lane == 0) *flag = bad;
-        }
-        __syncthreads();
         const int bad = *flag;
         if (bad) return j0 + bad;
         // (b) panel rows below: x D^T = a, one thread per row
@@ -137,57 +156,74 @@ __device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag)
             }
         }
         __syncthreads();
-        // (c) trailing lower triangle, 32 x 32 blocks, K = NB (zero padded)
-        const int nbk = (m2 + 31) / 32;
-        const int npairs = nbk * (nbk + 1) / 2;
-        for (int p = warp; p < npairs; p += BT / 32) {
-            int bj = 0, q = p;
-            while (q >= nbk - bj) { q -= nbk - bj; bj++; }
-            const int bi = bj + q;
-            const int r0 = bi * 32, c0 = bj * 32;
-            T acc[2][4][4];
-#pragma unroll
-            for (int a = 0; a < 2; a++)
-#pragma unroll
-                for (int b = 0; b < 4; b++)
-#pragma unroll
-                    for (int c = 0; c < 4; c++) acc[a][b][c] = T(0);
-#pragma unroll
-            for (int k8 = 0; k8 < NB; k8 += 8) {
-                T bf[4][2];
-#pragma unroll
-                for (int ni = 0; ni < 4; ni++) {
-                    const int cr = c0 + ni * 8 + g;
-                    bf[ni][0] = cr < m2 ? Ps[cr * PLD + k8 + t] : T(0);
-                    bf[ni][1] = cr < m2 ? Ps[cr * PLD + k8 + t + 4] : T(0);
-                }
-#pragma unroll
-                for (int mi = 0; mi < 2; mi++) {
-                    const int ra = r0 + mi * 16 + g;
-                    T af[4];
-                    af[0] = ra < m2 ? Ps[ra * PLD + k8 + t] : T(0);
-                    af[1] = ra + 8 < m2 ? Ps[(ra + 8) * PLD + k8 + t] : T(0);
-                    af[2] = ra < m2 ? Ps[ra * PLD + k8 + t + 4] : T(0);
-                    af[3] = ra + 8 < m2 ? Ps[(ra + 8) * PLD + k8 + t + 4] : T(0);
-#pragma unroll
-                    for (int ni = 0; ni < 4; ni++) mma8<SPLIT>(acc[mi][ni], af, bf[ni]);
-                }
+        if (m2 == 0) break;
+        const int nrb = (m2 + 15) / 16, ncb = (m2 + 31) / 32;
+        T *C = A + (size_t)(j0 + jb) * n + (j0 + jb);   // A22(0,0)
+        // blocks (bi, bj) of the lower triangle, bi >= 2 bj, numbered column
+        // by column; the warps in [w0, w0 + nw) take the blocks of the block
+        // columns [bj0, bj1)
+        auto trail = [&](int bj0, int bj1, int w0, int nw) {
+            if (warp < w0 || warp >= w0 + nw) return;
+            int first = 0, count = 0;
+            for (int bj = 0; bj < bj1 && bj < ncb; bj++) {
+                const int nb_j = max(0, nrb - 2 * bj);
+                if (bj < bj0) first += nb_j;
+                else count += nb_j;
             }
-            T *C = A + (size_t)(j0 + jb) * n + (j0 + jb);   // A22(0,0)
-#pragma unroll
-            for (int mi = 0; mi < 2; mi++)
+            for (int pp = warp - w0; pp < count; pp += nw) {
+                int bj = 0, q = first + pp;
+                while (q >= nrb - 2 * bj) { q -= nrb - 2 * bj; bj++; }
+                const int r0 = (2 * bj + q) * 16, c0 = bj * 32;
+                T cv[4][4], acc[4][4];
 #pragma unroll
                 for (int ni = 0; ni < 4; ni++)
 #pragma unroll
                     for (int h = 0; h < 2; h++)
 #pragma unroll
                         for (int e = 0; e < 2; e++) {
-                            const int r = r0 + mi * 16 + g + 8 * h;
-                            const int c = c0 + ni * 8 + 2 * t + e;
-                            if (r < m2 && c < m2 && r >= c)
-                                C[(size_t)c * n + r] -= acc[mi][ni][2 * h + e];
+                            const int r = r0 + g + 8 * h, c = c0 + ni * 8 + 2 * t + e;
+                            cv[ni][2 * h + e] = (r < m2 && c < m2 && r >= c)
+                                                    ? C[(size_t)c * n + r] : T(0);
+                            acc[ni][2 * h + e] = T(0);
                         }
-        }
+#pragma unroll
+                for (int k8 = 0; k8 < NB; k8 += 8) {
+                    T bf[4][2];
+#pragma unroll
+                    for (int ni = 0; ni < 4; ni++) {
+                        const int cr = c0 + ni * 8 + g;
+                        bf[ni][0] = cr < m2 ? Ps[cr * PLD + k8 + t] : T(0);
+                        bf[ni][1] = cr < m2 ? Ps[cr * PLD + k8 + t + 4] : T(0);
+                    }
+                    const int ra = r0 + g;
+                    T af[4];
+                    af[0] = ra < m2 ? Ps[ra * PLD + k8 + t] : T(0);
+                    af[1] = ra + 8 < m2 ? Ps[(ra + 8) * PLD + k8 + t] : T(0);
+                    af[2] = ra < m2 ? Ps[ra * PLD + k8 + t + 4] : T(0);
+                    af[3] = ra + 8 < m2 ? Ps[(ra + 8) * PLD + k8 + t + 4] : T(0);
+#pragma unroll
+                    for (int ni = 0; ni < 4; ni++) mma8<SPLIT>(acc[ni], af, bf[ni]);
+                }
+#pragma unroll
+                for (int ni = 0; ni < 4; ni++)
+#pragma unroll
+                    for (int h = 0; h < 2; h++)
+#pragma unroll
+                        for (int e = 0; e < 2; e++) {
+                            const int r = r0 + g + 8 * h, c = c0 + ni * 8 + 2 * t + e;
+                            if (r < m2 && c < m2 && r >= c)
+                                C[(size_t)c * n + r] = cv[ni][2 * h + e] - acc[ni][2 * h + e];
+                        }
+            }
+        };
+        // (c1) the first 32 columns of A22, all warps
+        trail(0, 1, 0, BT / 32);
+        __syncthreads();
+        // (a) the next diagonal block by warp 0, (c2) the rest by the others
+        if (warp == 0)
+            diag_block<T, NB>(A, n, j0 + jb, min(NB, m2), Ds, rdiag, flag, lane);
+        else
+            trail(1, ncb, 1, BT / 32 - 1);
         __syncthreads();
     }
     return 0;
