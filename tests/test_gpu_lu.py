@@ -163,3 +163,34 @@ def test_omp_dsgesv_tile_interface(L):
     assert solve_residual(a, x, b) < TOL * EPS
     for k in D:
         L.plasma_desc_destroy(ctypes.byref(D[k]))
+
+
+def test_dsgesv_tuned_tiles_cluster_panel(L):
+    """Tuning on: dsgesv picks 64-wide tiles and the one-launch cluster panel
+    (panels of up to 3000 rows); the solution against the oracle's."""
+    assert L.plasma_set(pb.PlasmaTuning, pb.PlasmaEnabled) == 0
+    n = 3000
+    a, b = gen.general(n, 1, seed=9300)
+    info, it, x, piv = dsgesv(L, a, b)
+    assert info == 0 and it >= 0
+    assert valid_pivots(piv, n)
+    assert solve_residual(a, x, b) < TOL * EPS
+    xo = np.zeros((n, 1), order="F")
+    oinfo, oit, _ = oracle.dsgesv(np.asfortranarray(a), np.asfortranarray(b), xo, 64)
+    assert oinfo == 0 and oit >= 0
+    np.testing.assert_allclose(x, xo, rtol=1e-8, atol=1e-12 * np.abs(xo).max())
+
+
+def test_dsgesv_fp64_lu_mixed_panels(L):
+    """An FP32 overflow in A sends dsgesv straight to the FP64 LU; with
+    64-wide tiles at n = 3500 its first panels are taller than a cluster
+    holds in FP64 (the per-column kernels), the later ones take the cluster
+    panel: the solution meets the tester's residual bound."""
+    set_nb(L, 64)
+    n = 3500
+    a, b = gen.general(n, 1, seed=9400)
+    a = np.asfortranarray(a * 1e39)
+    info, it, x, piv = dsgesv(L, a, b)
+    assert info == 0 and it == -31
+    assert valid_pivots(piv, n)
+    assert solve_residual(a, x, b) < TOL * EPS
