@@ -560,7 +560,32 @@ extern "C" int plasma_cuda_trsm_tc(cudaStream_t s, plasma_devstat_t *st, int mod
     k_trsm_prep<<<nblk + nblk * (nblk - 1) / 2, 256, TS_PREP_SMEM, s>>>(A, k, (float *)wimg, split, st);
     PLASMA_COUNT_LAUNCH();
     dim3 grid((unsigned)(mhi - mlo), (unsigned)(nb / TS_M));
-    k_trsm_tc<<<grid, TS_THREADS, TS_SMEM, s>>>(wmap, amap, pmap, g, st);
+    static int paired = -1;
+    if (paired < 0) {
+        const char *e = getenv("PLASMA_TRSM_PAIRED");
+        paired = e ? atoi(e) != 0 : 1;
+    }
+    if (paired && grid.y == 2) {
+        // the two halves of a tile as a cluster of two CTAs: they are
+        // scheduled on a pair of SMs at once, like the trailing update's
+        // CTA pairs, so the solve and the update hand SMs to each other in
+        // pairs (the CTAs share nothing)
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = grid;
+        cfg.blockDim = dim3(TS_THREADS);
+        cfg.dynamicSmemBytes = TS_SMEM;
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = 1;
+        at[0].val.clusterDim.y = 2;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, k_trsm_tc, wmap, amap, pmap, g, st);
+    } else {
+        k_trsm_tc<<<grid, TS_THREADS, TS_SMEM, s>>>(wmap, amap, pmap, g, st);
+    }
     plasma_prof_end(prof, s, PLASMA_KCLASS_TRSM, rows * nb * nb, 2.0 * rows * nb * 4.0);
     return write_panel ? 2 : 1;
 }
