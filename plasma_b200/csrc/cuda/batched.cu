@@ -120,9 +120,13 @@ __device__ __forceinline__ void diag_block(T *A, int n, int j0, int jb, T *Ds, T
 // overlaps the tensor work.  The trailing update runs on 16 x 32 blocks of
 // the lower triangle with DMMA (FP64) or the three-product TF32 split
 // (FP32); a warp's block of C is read into registers before its products,
-// so the L2 latency of the read overlaps them.
+// so the L2 latency of the read overlaps them.  With ys (posv: the
+// right-hand side in shared memory) the forward sweep L y = b runs along:
+// y_j by warp 0 from the diagonal block while it is in shared memory, the
+// rows below from the panel, so the solve afterwards is the backward sweep
+// alone.
 template <typename T, int SPLIT, int NB>
-__device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag)
+__device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag, T *ys)
 {
     constexpr int PLD = ps_ld<T>();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -143,10 +147,14 @@ __device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag)
 #pragma unroll
             for (int c = 0; c < NB; c++) {
                 if (c < jb) {
-                    T s = x[c];
+                    // two partial sums halve the dependent chain
+                    T s0 = x[c], s1 = T(0);
 #pragma unroll
-                    for (int c2 = 0; c2 < c; c2++) s -= x[c2] * Ds[c2 * (NBMAXB + 1) + c];
-                    x[c] = s * rdiag[c];
+                    for (int c2 = 0; c2 < c; c2++) {
+                        if (c2 & 1) s1 -= x[c2] * Ds[c2 * (NBMAXB + 1) + c];
+                        else s0 -= x[c2] * Ds[c2 * (NBMAXB + 1) + c];
+                    }
+                    x[c] = (s0 + s1) * rdiag[c];
                 }
             }
 #pragma unroll
@@ -156,7 +164,20 @@ __device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag)
             }
         }
         __syncthreads();
-        if (m2 == 0) break;
+        // forward sweep, diagonal block: y_j = L_jj^-1 y_j (warp 0)
+        if (ys != nullptr && warp == 0) {
+            T y = lane < jb ? ys[j0 + lane] : T(0);
+            for (int c = 0; c < jb; c++) {
+                if (lane == c) y = y * rdiag[c];
+                const T yc = __shfl_sync(0xffffffffu, y, c);
+                if (lane > c && lane < jb) y -= Ds[c * (NBMAXB + 1) + lane] * yc;
+            }
+            if (lane < jb) ys[j0 + lane] = y;
+        }
+        if (m2 == 0) {
+            __syncthreads();
+            break;
+        }
         const int nrb = (m2 + 15) / 16, ncb = (m2 + 31) / 32;
         T *C = A + (size_t)(j0 + jb) * n + (j0 + jb);   // A22(0,0)
         // blocks (bi, bj) of the lower triangle, bi >= 2 bj, numbered column
@@ -220,10 +241,23 @@ __device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag)
         trail(0, 1, 0, BT / 32);
         __syncthreads();
         // (a) the next diagonal block by warp 0, (c2) the rest by the others
-        if (warp == 0)
+        // (after the forward sweep's rows below: y_below -= P y_j)
+        if (warp == 0) {
             diag_block<T, NB>(A, n, j0 + jb, min(NB, m2), Ds, rdiag, flag, lane);
-        else
+        } else {
+            if (ys != nullptr) {
+                for (int r = tid - 32; r < m2; r += BT - 32) {
+                    T s0 = T(0), s1 = T(0);
+#pragma unroll
+                    for (int c = 0; c < NB; c += 2) {
+                        s0 += Ps[r * PLD + c] * ys[j0 + c];
+                        s1 += Ps[r * PLD + c + 1] * ys[j0 + c + 1];
+                    }
+                    ys[j0 + jb + r] -= s0 + s1;
+                }
+            }
             trail(1, ncb, 1, BT / 32 - 1);
+        }
         __syncthreads();
     }
     return 0;
@@ -234,13 +268,14 @@ __device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag)
 // Each 32 x 32 diagonal block is first staged in shared memory (one parallel
 // load), so the warp's substitution reads shared memory only.
 template <typename T>
-__device__ void solve_one(const T *A, int n, T *b, T *Ys, T *Db, T *Dr)
+__device__ void solve_one(const T *A, int n, T *b, T *Ys, T *Db, T *Dr, bool forward_done = false)
 {
     constexpr int NB = 32, DLD = NB + 1;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int i = tid; i < n; i += BT) Ys[i] = b[i];
-    // forward: L y = b
-    for (int j0 = 0; j0 < n; j0 += NB) {
+    if (!forward_done)
+        for (int i = tid; i < n; i += BT) Ys[i] = b[i];
+    // forward: L y = b (unless the factorization ran it: Ys holds y)
+    for (int j0 = 0; j0 < n && !forward_done; j0 += NB) {
         const int jb = min(NB, n - j0);
         for (int e = tid; e < NB * NB; e += BT) {
             const int r = e % NB, c = e / NB;
@@ -467,11 +502,19 @@ k_batched(BatchArgs a)
         const int n = a.n[m];
         T *A = (T *)a.A + a.off_a[m];
         if (a.op == OP_POSV || a.op == OP_POTRF) {
-            const int info = a.nbsel[m] == 16 ? factor_one<T, SPLIT, 16>(A, n, Ps, Ds, rdiag, &flag_s)
-                                              : factor_one<T, SPLIT, 32>(A, n, Ps, Ds, rdiag, &flag_s);
+            T *b = (T *)a.B + a.off_b[m];
+            T *ys = nullptr;
+            if (a.op == OP_POSV) {
+                for (int i = tid; i < n; i += BT) Ys[i] = b[i];
+                __syncthreads();
+                ys = Ys;
+            }
+            const int info = a.nbsel[m] == 16
+                                 ? factor_one<T, SPLIT, 16>(A, n, Ps, Ds, rdiag, &flag_s, ys)
+                                 : factor_one<T, SPLIT, 32>(A, n, Ps, Ds, rdiag, &flag_s, ys);
             if (tid == 0) a.info[m] = info;
             __syncthreads();
-            if (info == 0 && a.op == OP_POSV) solve_one<T>(A, n, (T *)a.B + a.off_b[m], Ys, D2, rdiag);
+            if (info == 0 && a.op == OP_POSV) solve_one<T>(A, n, b, Ys, D2, rdiag, true);
         } else if (a.op == OP_POTRS) {
             solve_one<T>(A, n, (T *)a.B + a.off_b[m], Ys, D2, rdiag);
         } else if (a.op == OP_POTRS_ADJ) {
