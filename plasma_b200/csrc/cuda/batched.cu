@@ -65,12 +65,54 @@ struct BatchArgs {
 };
 
 // ------------------------------------------------------------------ factor
-// The diagonal block at j0 (jb x jb, lower), factored by one warp, lane r
-// holding row r, pivots broadcast by shuffles; writes it to A and Ds, the
-// reciprocal pivots to rdiag and the first bad pivot (LAPACK's info within
-// the block, 0 if none) to *flag.
+// The diagonal block at j0 (jb x jb, lower), factored by one warp in shared
+// memory (Ds), right-looking, lane r holding row r and updating its own
+// entries; writes it to A and Ds, the reciprocal pivots to rdiag and the
+// first bad pivot (LAPACK's info within the block, 0 if none) to *flag.
 template <typename T, int NB>
 __device__ __forceinline__ void diag_block(T *A, int n, int j0, int jb, T *Ds, T *rdiag,
+                                           int *flag, int lane)
+{
+    constexpr int DL = NBMAXB + 1;
+#pragma unroll 4
+    for (int c = 0; c < NB; c++)
+        Ds[c * DL + lane] = (lane < jb && c < jb && lane >= c)
+                                ? A[(size_t)(j0 + c) * n + j0 + lane] : T(0);
+    __syncwarp();
+    int bad = 0;
+    T myrd = T(1);
+    for (int c = 0; c < jb; c++) {
+        const T d = Ds[c * DL + c];
+        const bool ok = d > T(0);
+        if (!ok && bad == 0) bad = c + 1;
+        // one reciprocal square root per pivot: 1/sqrt(d), sqrt(d) = d/sqrt(d)
+        const T rd = ok ? rsqrt(d) : T(1);
+        const T sd = ok ? d * rd : T(1);
+        T l = T(0);
+        if (lane == c) myrd = rd;
+        if (lane > c && lane < jb) {
+            l = Ds[c * DL + lane] * rd;
+            Ds[c * DL + lane] = l;
+        }
+        __syncwarp();
+        if (lane > c && lane < jb)
+            for (int c2 = c + 1; c2 <= lane; c2++) Ds[c2 * DL + lane] -= l * Ds[c * DL + c2];
+        if (lane == c) Ds[c * DL + c] = sd;
+        __syncwarp();
+    }
+    if (lane < jb) {
+        for (int c = 0; c <= lane; c++) A[(size_t)(j0 + c) * n + j0 + lane] = Ds[c * DL + lane];
+        rdiag[lane] = myrd;
+    }
+    if (lane == 0) *flag = bad;
+}
+
+// The same with the block held in registers, lane r holding row r, pivots
+// broadcast by shuffles: faster for FP32 (8.0 against 8.8 ms for the 4096
+// systems of the benchmark), slower for FP64, where the unrolled chain took
+// a warp about 150 us per 32 x 32 block (13.1 against 11.3 ms).
+template <typename T, int NB>
+__device__ __forceinline__ void diag_block_regs(T *A, int n, int j0, int jb, T *Ds, T *rdiag,
                                            int *flag, int lane)
 {
     T v[NB];
@@ -112,6 +154,16 @@ __device__ __forceinline__ void diag_block(T *A, int n, int j0, int jb, T *Ds, T
     if (lane == 0) *flag = bad;
 }
 
+template <typename T, int NB>
+__device__ __forceinline__ void diag_any(T *A, int n, int j0, int jb, T *Ds, T *rdiag,
+                                         int *flag, int lane)
+{
+    if constexpr (sizeof(T) == 8)
+        diag_block<T, NB>(A, n, j0, jb, Ds, rdiag, flag, lane);
+    else
+        diag_block_regs<T, NB>(A, n, j0, jb, Ds, rdiag, flag, lane);
+}
+
 // Per block column j0: (b) the panel below the diagonal block, a thread per
 // row, x D^T = a (kept in shared memory); (c1) the trailing update of the
 // first 32 columns of A22 (they hold the next diagonal block and the next
@@ -131,7 +183,7 @@ __device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag, T *ys)
     constexpr int PLD = ps_ld<T>();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, t = lane & 3;
-    if (warp == 0) diag_block<T, NB>(A, n, 0, min(NB, n), Ds, rdiag, flag, lane);
+    if (warp == 0) diag_any<T, NB>(A, n, 0, min(NB, n), Ds, rdiag, flag, lane);
     __syncthreads();
     for (int j0 = 0; j0 < n; j0 += NB) {
         const int jb = min(NB, n - j0);
@@ -243,7 +295,7 @@ __device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag, T *ys)
         // (a) the next diagonal block by warp 0, (c2) the rest by the others
         // (after the forward sweep's rows below: y_below -= P y_j)
         if (warp == 0) {
-            diag_block<T, NB>(A, n, j0 + jb, min(NB, m2), Ds, rdiag, flag, lane);
+            diag_any<T, NB>(A, n, j0 + jb, min(NB, m2), Ds, rdiag, flag, lane);
         } else {
             if (ys != nullptr) {
                 for (int r = tid - 32; r < m2; r += BT - 32) {
