@@ -65,103 +65,53 @@ struct BatchArgs {
 };
 
 // ------------------------------------------------------------------ factor
-// The diagonal block at j0 (jb x jb, lower), factored by one warp in shared
-// memory (Ds), right-looking, lane r holding row r and updating its own
-// entries; writes it to A and Ds, the reciprocal pivots to rdiag and the
-// first bad pivot (LAPACK's info within the block, 0 if none) to *flag.
+// The diagonal block at j0 (jb x jb, lower), factored by one warp,
+// right-looking: lane r holds row r in registers (every loop unrolled, so the
+// row stays in registers), the block padded to NB x NB with the identity so
+// that no step depends on jb.  Per column c: the pivot comes from lane c by
+// one shuffle, every lane scales its entry and publishes it in Ds (column c
+// at Ds[c * (NBMAXB + 1)]), and the rank-1 update reads the column back as
+// broadcast loads, independent of one another.  (Entries above the diagonal
+// are updated too, from entries above the diagonal only, and never written
+// out.)  Writes L to A and Ds, the reciprocal pivots to rdiag and the first
+// bad pivot (LAPACK's info within the block, 0 if none) to *flag.
 template <typename T, int NB>
 __device__ __forceinline__ void diag_block(T *A, int n, int j0, int jb, T *Ds, T *rdiag,
                                            int *flag, int lane)
 {
     constexpr int DL = NBMAXB + 1;
-#pragma unroll 4
-    for (int c = 0; c < NB; c++)
-        Ds[c * DL + lane] = (lane < jb && c < jb && lane >= c)
-                                ? A[(size_t)(j0 + c) * n + j0 + lane] : T(0);
-    __syncwarp();
-    int bad = 0;
-    T myrd = T(1);
-    for (int c = 0; c < jb; c++) {
-        const T d = Ds[c * DL + c];
-        const bool ok = d > T(0);
-        if (!ok && bad == 0) bad = c + 1;
-        // one reciprocal square root per pivot: 1/sqrt(d), sqrt(d) = d/sqrt(d)
-        const T rd = ok ? rsqrt(d) : T(1);
-        const T sd = ok ? d * rd : T(1);
-        T l = T(0);
-        if (lane == c) myrd = rd;
-        if (lane > c && lane < jb) {
-            l = Ds[c * DL + lane] * rd;
-            Ds[c * DL + lane] = l;
-        }
-        __syncwarp();
-        if (lane > c && lane < jb)
-            for (int c2 = c + 1; c2 <= lane; c2++) Ds[c2 * DL + lane] -= l * Ds[c * DL + c2];
-        if (lane == c) Ds[c * DL + c] = sd;
-        __syncwarp();
-    }
-    if (lane < jb) {
-        for (int c = 0; c <= lane; c++) A[(size_t)(j0 + c) * n + j0 + lane] = Ds[c * DL + lane];
-        rdiag[lane] = myrd;
-    }
-    if (lane == 0) *flag = bad;
-}
-
-// The same with the block held in registers, lane r holding row r, pivots
-// broadcast by shuffles: faster for FP32 (8.0 against 8.8 ms for the 4096
-// systems of the benchmark), slower for FP64, where the unrolled chain took
-// a warp about 150 us per 32 x 32 block (13.1 against 11.3 ms).
-template <typename T, int NB>
-__device__ __forceinline__ void diag_block_regs(T *A, int n, int j0, int jb, T *Ds, T *rdiag,
-                                           int *flag, int lane)
-{
     T v[NB];
 #pragma unroll
     for (int c = 0; c < NB; c++)
-        v[c] = (lane < jb && c < jb && lane >= c) ? A[(size_t)(j0 + c) * n + j0 + lane] : T(0);
+        v[c] = (lane < jb && c < jb) ? (lane >= c ? A[(size_t)(j0 + c) * n + j0 + lane] : T(0))
+                                     : (lane == c ? T(1) : T(0));
     int bad = 0;
     T myrd = T(1);
 #pragma unroll
     for (int c = 0; c < NB; c++) {
-        if (c < jb) {
-            T d = __shfl_sync(0xffffffffu, v[c], c);
-            bool ok = d > T(0);
-            if (!ok && bad == 0) bad = c + 1;
-            // one reciprocal square root per pivot: 1/sqrt(d), sqrt(d) = d/sqrt(d)
-            T rd = ok ? rsqrt(d) : T(1);
-            T sd = ok ? d * rd : T(1);
-            if (lane == c) myrd = rd;
-            if (lane >= c) v[c] = (lane == c) ? sd : v[c] * rd;
-            // a fixed trip count keeps v[] in registers (full unroll)
-#pragma unroll
-            for (int c2 = 0; c2 < NB; c2++) {
-                if (c2 > c) {
-                    T l = __shfl_sync(0xffffffffu, v[c], c2);
-                    if (c2 < jb && lane >= c2) v[c2] -= v[c] * l;
-                }
-            }
+        const T d = __shfl_sync(0xffffffffu, v[c], c);
+        const bool ok = d > T(0);
+        if (!ok && bad == 0 && c < jb) bad = c + 1;
+        // one reciprocal square root per pivot: 1/sqrt(d), sqrt(d) = d/sqrt(d)
+        const T rd = ok ? rsqrt(d) : T(1);
+        if (lane == c) {
+            myrd = rd;
+            v[c] = ok ? d * rd : T(1);
+        } else {
+            v[c] *= rd;
         }
+        Ds[c * DL + lane] = v[c];
+        __syncwarp();
+#pragma unroll
+        for (int c2 = c + 1; c2 < NB; c2++) v[c2] -= v[c] * Ds[c * DL + c2];
     }
     if (lane < jb) {
 #pragma unroll
         for (int c = 0; c < NB; c++)
-            if (c < jb && lane >= c) {
-                A[(size_t)(j0 + c) * n + j0 + lane] = v[c];
-                Ds[c * (NBMAXB + 1) + lane] = v[c];
-            }
+            if (c < jb && lane >= c) A[(size_t)(j0 + c) * n + j0 + lane] = v[c];
         rdiag[lane] = myrd;
     }
     if (lane == 0) *flag = bad;
-}
-
-template <typename T, int NB>
-__device__ __forceinline__ void diag_any(T *A, int n, int j0, int jb, T *Ds, T *rdiag,
-                                         int *flag, int lane)
-{
-    if constexpr (sizeof(T) == 8)
-        diag_block<T, NB>(A, n, j0, jb, Ds, rdiag, flag, lane);
-    else
-        diag_block_regs<T, NB>(A, n, j0, jb, Ds, rdiag, flag, lane);
 }
 
 // Per block column j0: (b) the panel below the diagonal block, a thread per
@@ -183,7 +133,7 @@ __device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag, T *ys)
     constexpr int PLD = ps_ld<T>();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, t = lane & 3;
-    if (warp == 0) diag_any<T, NB>(A, n, 0, min(NB, n), Ds, rdiag, flag, lane);
+    if (warp == 0) diag_block<T, NB>(A, n, 0, min(NB, n), Ds, rdiag, flag, lane);
     __syncthreads();
     for (int j0 = 0; j0 < n; j0 += NB) {
         const int jb = min(NB, n - j0);
@@ -295,7 +245,7 @@ __device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag, T *ys)
         // (a) the next diagonal block by warp 0, (c2) the rest by the others
         // (after the forward sweep's rows below: y_below -= P y_j)
         if (warp == 0) {
-            diag_any<T, NB>(A, n, j0 + jb, min(NB, m2), Ds, rdiag, flag, lane);
+            diag_block<T, NB>(A, n, j0 + jb, min(NB, m2), Ds, rdiag, flag, lane);
         } else {
             if (ys != nullptr) {
                 for (int r = tid - 32; r < m2; r += BT - 32) {
