@@ -40,10 +40,11 @@ constexpr int NBMAXB = 32;            // largest block width
 
 template <typename T> constexpr int ps_ld() { return NBMAXB + Pad<T>::v; }
 // shared memory: panel [NMAX][ps_ld], two 32 x 33 blocks, a vector of NMAX,
-// 32 reciprocal pivots
+// 32 reciprocal pivots, the inverse of the diagonal block [32][ps_ld]
 template <typename T> constexpr int batched_smem()
 {
-    return (NMAX * ps_ld<T>() + 2 * NBMAXB * (NBMAXB + 1) + NMAX + NBMAXB) * (int)sizeof(T);
+    return (NMAX * ps_ld<T>() + 2 * NBMAXB * (NBMAXB + 1) + NMAX + NBMAXB +
+            NBMAXB * ps_ld<T>()) * (int)sizeof(T);
 }
 
 enum { OP_POSV = 0, OP_POTRF = 1, OP_POTRS = 2, OP_POTRF_ADJ = 3, OP_POTRS_ADJ = 4 };
@@ -114,12 +115,36 @@ __device__ __forceinline__ void diag_block(T *A, int n, int j0, int jb, T *Ds, T
     if (lane == 0) *flag = bad;
 }
 
-// Per block column j0: (b) the panel below the diagonal block, a thread per
-// row, x D^T = a (kept in shared memory); (c1) the trailing update of the
-// first 32 columns of A22 (they hold the next diagonal block and the next
-// panel); then warp 0 factors the next diagonal block (a) while the other
-// warps finish the trailing update (c2), so the single-warp chain of (a)
-// overlaps the tensor work.  The trailing update runs on 16 x 32 blocks of
+// The inverse of the factored diagonal block, Li = L^-1 (row i at
+// Li[i * ps_ld]), by one warp: lane j solves L y = e_j column by column
+// (y_k scaled by its reciprocal pivot, then y_i -= L_ik y_k below it, the
+// column of L read from Ds as broadcast loads); every loop unrolled, y kept
+// in registers until the end.  Lanes at or beyond NB form zero columns,
+// never read.
+template <typename T, int NB>
+__device__ __forceinline__ void diag_inverse(const T *Ds, const T *rdiag, T *Li, int lane)
+{
+    constexpr int DL = NBMAXB + 1, LLD = ps_ld<T>();
+    T y[NB];
+#pragma unroll
+    for (int i = 0; i < NB; i++) y[i] = (i == lane) ? T(1) : T(0);
+#pragma unroll
+    for (int k = 0; k < NB; k++) {
+        y[k] *= rdiag[k];
+#pragma unroll
+        for (int i = k + 1; i < NB; i++) y[i] -= Ds[k * DL + i] * y[k];
+    }
+#pragma unroll
+    for (int i = 0; i < NB; i++) Li[i * LLD + lane] = y[i];
+}
+
+// Per block column j0: (b) the panel below the diagonal block, X D^T = A21,
+// as the tensor-core product X = A21 D^-T with the inverse formed right
+// after the diagonal block was factored (kept in shared memory); (c1) the
+// trailing update of the first 32 columns of A22 (they hold the next
+// diagonal block and the next panel); then warp 0 factors the next diagonal
+// block and inverts it (a) while the other warps finish the trailing update
+// (c2), so the single-warp chains of (a) overlap the tensor work.  The trailing update runs on 16 x 32 blocks of
 // the lower triangle with DMMA (FP64) or the three-product TF32 split
 // (FP32); a warp's block of C is read into registers before its products,
 // so the L2 latency of the read overlaps them.  With ys (posv: the
@@ -128,41 +153,65 @@ __device__ __forceinline__ void diag_block(T *A, int n, int j0, int jb, T *Ds, T
 // rows below from the panel, so the solve afterwards is the backward sweep
 // alone.
 template <typename T, int SPLIT, int NB>
-__device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag, T *ys)
+__device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag, T *ys, T *Li)
 {
     constexpr int PLD = ps_ld<T>();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, t = lane & 3;
-    if (warp == 0) diag_block<T, NB>(A, n, 0, min(NB, n), Ds, rdiag, flag, lane);
+    if (warp == 0) {
+        diag_block<T, NB>(A, n, 0, min(NB, n), Ds, rdiag, flag, lane);
+        __syncwarp();
+        diag_inverse<T, NB>(Ds, rdiag, Li, lane);
+    }
     __syncthreads();
     for (int j0 = 0; j0 < n; j0 += NB) {
         const int jb = min(NB, n - j0);
         const int m2 = n - j0 - jb;
         const int bad = *flag;
         if (bad) return j0 + bad;
-        // (b) panel rows below: x D^T = a, one thread per row
-        for (int r = tid; r < m2; r += BT) {
-            const int row = j0 + jb + r;
-            T x[NB];
+        // (b) the panel below, X = A21 L_jj^-T: a tensor-core product with
+        // the inverse, 16-row blocks taken by the warps in turn (a panel
+        // exists only below a full diagonal block, jb = NB), X written to A
+        // and to Ps
+        {
+            T *A21 = A + (size_t)j0 * n + (j0 + jb);
+            for (int r0 = warp * 16; r0 < m2; r0 += BT / 2) {
+                const int ra = r0 + g;
+                T af[NB / 8][4];
 #pragma unroll
-            for (int c = 0; c < NB; c++) x[c] = c < jb ? A[(size_t)(j0 + c) * n + row] : T(0);
-#pragma unroll
-            for (int c = 0; c < NB; c++) {
-                if (c < jb) {
-                    // two partial sums halve the dependent chain
-                    T s0 = x[c], s1 = T(0);
-#pragma unroll
-                    for (int c2 = 0; c2 < c; c2++) {
-                        if (c2 & 1) s1 -= x[c2] * Ds[c2 * (NBMAXB + 1) + c];
-                        else s0 -= x[c2] * Ds[c2 * (NBMAXB + 1) + c];
-                    }
-                    x[c] = (s0 + s1) * rdiag[c];
+                for (int k8 = 0; k8 < NB; k8 += 8) {
+                    const T *c0 = A21 + (size_t)(k8 + t) * n, *c4 = c0 + (size_t)4 * n;
+                    af[k8 / 8][0] = ra < m2 ? c0[ra] : T(0);
+                    af[k8 / 8][1] = ra + 8 < m2 ? c0[ra + 8] : T(0);
+                    af[k8 / 8][2] = ra < m2 ? c4[ra] : T(0);
+                    af[k8 / 8][3] = ra + 8 < m2 ? c4[ra + 8] : T(0);
                 }
-            }
+                T acc[NB / 8][4];
 #pragma unroll
-            for (int c = 0; c < NB; c++) {
-                if (c < jb) A[(size_t)(j0 + c) * n + row] = x[c];
-                Ps[r * PLD + c] = x[c];            // zero beyond jb
+                for (int ni = 0; ni < NB / 8; ni++)
+#pragma unroll
+                    for (int e = 0; e < 4; e++) acc[ni][e] = T(0);
+#pragma unroll
+                for (int k8 = 0; k8 < NB; k8 += 8)
+#pragma unroll
+                    for (int ni = 0; ni < NB / 8; ni++) {
+                        T bf[2];
+                        bf[0] = Li[(ni * 8 + g) * PLD + k8 + t];
+                        bf[1] = Li[(ni * 8 + g) * PLD + k8 + t + 4];
+                        mma8<SPLIT>(acc[ni], af[k8 / 8], bf);
+                    }
+#pragma unroll
+                for (int ni = 0; ni < NB / 8; ni++)
+#pragma unroll
+                    for (int h = 0; h < 2; h++)
+#pragma unroll
+                        for (int e = 0; e < 2; e++) {
+                            const int r = ra + 8 * h, c = ni * 8 + 2 * t + e;
+                            if (r < m2) {
+                                A21[(size_t)c * n + r] = acc[ni][2 * h + e];
+                                Ps[r * PLD + c] = acc[ni][2 * h + e];
+                            }
+                        }
             }
         }
         __syncthreads();
@@ -246,6 +295,8 @@ __device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag, T *ys)
         // (after the forward sweep's rows below: y_below -= P y_j)
         if (warp == 0) {
             diag_block<T, NB>(A, n, j0 + jb, min(NB, m2), Ds, rdiag, flag, lane);
+            __syncwarp();
+            diag_inverse<T, NB>(Ds, rdiag, Li, lane);
         } else {
             if (ys != nullptr) {
                 for (int r = tid - 32; r < m2; r += BT - 32) {
@@ -492,6 +543,7 @@ k_batched(BatchArgs a)
     T *D2 = Ds + NBMAXB * (NBMAXB + 1);             // [32][33]
     T *Ys = D2 + NBMAXB * (NBMAXB + 1);             // [NMAX]
     T *rdiag = Ys + NMAX;                           // [32]
+    T *Li = rdiag + NBMAXB;                         // [32][ps_ld] diagonal block inverse
     __shared__ int idx_s, flag_s;
     const int tid = threadIdx.x;
     for (;;) {
@@ -512,8 +564,8 @@ k_batched(BatchArgs a)
                 ys = Ys;
             }
             const int info = a.nbsel[m] == 16
-                                 ? factor_one<T, SPLIT, 16>(A, n, Ps, Ds, rdiag, &flag_s, ys)
-                                 : factor_one<T, SPLIT, 32>(A, n, Ps, Ds, rdiag, &flag_s, ys);
+                                 ? factor_one<T, SPLIT, 16>(A, n, Ps, Ds, rdiag, &flag_s, ys, Li)
+                                 : factor_one<T, SPLIT, 32>(A, n, Ps, Ds, rdiag, &flag_s, ys, Li);
             if (tid == 0) a.info[m] = info;
             __syncthreads();
             if (info == 0 && a.op == OP_POSV) solve_one<T>(A, n, b, Ys, D2, rdiag, true);
