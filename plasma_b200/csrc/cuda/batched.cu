@@ -74,18 +74,23 @@ struct BatchArgs {
 // at Ds[c * (NBMAXB + 1)]), and the rank-1 update reads the column back as
 // broadcast loads, independent of one another.  (Entries above the diagonal
 // are updated too, from entries above the diagonal only, and never written
-// out.)  Writes L to A and Ds, the reciprocal pivots to rdiag and the first
-// bad pivot (LAPACK's info within the block, 0 if none) to *flag.
+// out.)  The block is read from A, or from Dn (column c at Dn[c * (NBMAXB
+// + 1)], its lower triangle) where the update that produced it left a copy.
+// Writes L to A and Ds, the reciprocal pivots to rdiag and the first bad
+// pivot (LAPACK's info within the block, 0 if none) to *flag.
 template <typename T, int NB>
 __device__ __forceinline__ void diag_block(T *A, int n, int j0, int jb, T *Ds, T *rdiag,
-                                           int *flag, int lane)
+                                           int *flag, int lane, const T *Dn = nullptr)
 {
     constexpr int DL = NBMAXB + 1;
     T v[NB];
 #pragma unroll
     for (int c = 0; c < NB; c++)
-        v[c] = (lane < jb && c < jb) ? (lane >= c ? A[(size_t)(j0 + c) * n + j0 + lane] : T(0))
-                                     : (lane == c ? T(1) : T(0));
+        v[c] = (lane < jb && c < jb)
+                   ? (lane >= c ? (Dn != nullptr ? Dn[c * DL + lane]
+                                                 : A[(size_t)(j0 + c) * n + j0 + lane])
+                                : T(0))
+                   : (lane == c ? T(1) : T(0));
     int bad = 0;
     T myrd = T(1);
 #pragma unroll
@@ -153,7 +158,8 @@ __device__ __forceinline__ void diag_inverse(const T *Ds, const T *rdiag, T *Li,
 // rows below from the panel, so the solve afterwards is the backward sweep
 // alone.
 template <typename T, int SPLIT, int NB>
-__device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag, T *ys, T *Li)
+__device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag, T *ys, T *Li,
+                          T *Dn)
 {
     constexpr int PLD = ps_ld<T>();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -283,8 +289,12 @@ __device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag, T *ys,
 #pragma unroll
                         for (int e = 0; e < 2; e++) {
                             const int r = r0 + g + 8 * h, c = c0 + ni * 8 + 2 * t + e;
-                            if (r < m2 && c < m2 && r >= c)
-                                C[(size_t)c * n + r] = cv[ni][2 * h + e] - acc[ni][2 * h + e];
+                            if (r < m2 && c < m2 && r >= c) {
+                                const T val = cv[ni][2 * h + e] - acc[ni][2 * h + e];
+                                C[(size_t)c * n + r] = val;
+                                // the next diagonal block, for (a) to read
+                                if (r < NBMAXB) Dn[c * (NBMAXB + 1) + r] = val;
+                            }
                         }
             }
         };
@@ -294,7 +304,7 @@ __device__ int factor_one(T *A, int n, T *Ps, T *Ds, T *rdiag, int *flag, T *ys,
         // (a) the next diagonal block by warp 0, (c2) the rest by the others
         // (after the forward sweep's rows below: y_below -= P y_j)
         if (warp == 0) {
-            diag_block<T, NB>(A, n, j0 + jb, min(NB, m2), Ds, rdiag, flag, lane);
+            diag_block<T, NB>(A, n, j0 + jb, min(NB, m2), Ds, rdiag, flag, lane, Dn);
             __syncwarp();
             diag_inverse<T, NB>(Ds, rdiag, Li, lane);
         } else {
@@ -564,8 +574,8 @@ k_batched(BatchArgs a)
                 ys = Ys;
             }
             const int info = a.nbsel[m] == 16
-                                 ? factor_one<T, SPLIT, 16>(A, n, Ps, Ds, rdiag, &flag_s, ys, Li)
-                                 : factor_one<T, SPLIT, 32>(A, n, Ps, Ds, rdiag, &flag_s, ys, Li);
+                                 ? factor_one<T, SPLIT, 16>(A, n, Ps, Ds, rdiag, &flag_s, ys, Li, D2)
+                                 : factor_one<T, SPLIT, 32>(A, n, Ps, Ds, rdiag, &flag_s, ys, Li, D2);
             if (tid == 0) a.info[m] = info;
             __syncthreads();
             if (info == 0 && a.op == OP_POSV) solve_one<T>(A, n, b, Ys, D2, rdiag, true);
