@@ -230,6 +230,29 @@ def test_autotune_argument_codes(hostonly):
     assert L.plasma_autotune_potrf(pb.PlasmaRealDouble, 100, None) == pb.PlasmaErrorEnvironment
 
 
+def test_batched_plan_argument_codes(hostonly):
+    """Batched plans: the argument checks run before any device work, so a
+    host-only context reports them; a valid plan needs the device."""
+    L = hostonly
+    plan = ctypes.c_void_p()
+    n = (ctypes.c_int * 3)(16, 512, 0)
+    assert L.plasma_batch_create(0, 3, n, ctypes.byref(plan)) == -1
+    assert L.plasma_batch_create(pb.PlasmaRealDouble, -1, n, ctypes.byref(plan)) == -2
+    assert L.plasma_batch_create(pb.PlasmaRealDouble, 3, None, ctypes.byref(plan)) == -3
+    big = (ctypes.c_int * 2)(16, 513)
+    assert L.plasma_batch_create(pb.PlasmaRealFloat, 2, big, ctypes.byref(plan)) == -3
+    neg = (ctypes.c_int * 1)(-1,)
+    assert L.plasma_batch_create(pb.PlasmaRealFloat, 1, neg, ctypes.byref(plan)) == -3
+    assert L.plasma_batch_create(pb.PlasmaRealDouble, 3, n, None) == -4
+    assert L.plasma_batch_create(pb.PlasmaRealDouble, 3, n,
+                                 ctypes.byref(plan)) == pb.PlasmaErrorEnvironment
+    assert L.plasma_dposv_batched(None, None, None, None) == -1
+    assert L.plasma_batch_offsets(None, None, None) == -1
+    assert L.plasma_batch_set_graph(None, 1) == -1
+    assert L.plasma_batch_matrix_elems(None) == 0
+    assert L.plasma_batch_vector_elems(None) == 0
+
+
 def test_dsposv_descriptor_triangles(hostonly):
     """plasma_omp_dsposv checks that packed triangles hold what the solve
     reads: A the uplo triangle, As lower (for either uplo) or upper (for
