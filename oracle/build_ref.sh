@@ -1,8 +1,10 @@
 #!/usr/bin/env bash
 # Build the reference PLASMA's SPD path (dpotrf, dpotrs, dposv, dsposv and
-# what they call) as a shared library, oracle/_ref/libplasma_ref.so, for the
-# parity tests and for the CPU reference arm of bench.py.  Test
-# infrastructure: the product never loads it.
+# what they call), its LU-based mixed-precision solver (dsgesv with dgetrf,
+# dgetrs) and its band Cholesky (dpbtrf, dpbtrs, dpbsv) as a shared library,
+# oracle/_ref/libplasma_ref.so, for the parity tests and for the CPU
+# reference arm of bench.py.  Test infrastructure: the product never loads
+# it.
 #
 # What it does:
 #   1. copies the reference sources to a scratch directory (the source tree
@@ -48,10 +50,12 @@ cd "$SCRATCH/src"
 
 COMPUTE_Z="zpotrf zpotrs zposv zcposv pzpotrf pztrsm pzsymm pzlansy pzlacpy
            pzgeadd pzlag2c pclag2z zge2desc zdesc2ge ztr2desc zdesc2tr pzge2desc
-           pzdesc2ge pztr2desc pzdesc2tr pdzamax"
+           pzdesc2ge pztr2desc pzdesc2tr pdzamax
+           zgetrf zgetrs zgesv zcgesv pzgetrf pzgeswp pzgemm pzlange
+           zpbtrf zpbtrs zpbsv pzpbtrf pztbsm zpb2desc zdesc2pb pzpb2desc pzdesc2pb"
 CORE_Z="core_zpotrf core_ztrsm core_zsyrk core_zgemm core_zsymm core_zlacpy
         core_zgeadd core_zlansy core_zlange core_zsyssq core_zgessq core_zlag2c
-        core_clag2z core_dzamax"
+        core_clag2z core_dzamax core_zgetrf core_zgeswp core_zlacpy_band"
 HDR_Z="plasma_z plasma_zc plasma_internal_z plasma_internal_zc plasma_core_blas_z
        plasma_core_blas_zc core_lapack_z plasma_zlaebz2_work"
 
@@ -66,13 +70,16 @@ for f in dpotrf dpotrs dposv dsposv spotrf spotrs sposv pdpotrf pspotrf pdtrsm \
          pstrsm pdlacpy pslacpy pdgeadd psgeadd pdsymm pdlansy pdamax pdlag2s \
          pslag2d dge2desc ddesc2ge dtr2desc ddesc2tr sge2desc sdesc2ge str2desc \
          sdesc2tr pdge2desc pddesc2ge pdtr2desc pddesc2tr psge2desc psdesc2ge \
-         pstr2desc psdesc2tr; do
+         pstr2desc psdesc2tr \
+         dgetrf dgetrs dgesv dsgesv pdgetrf psgetrf pdgeswp psgeswp pdgemm pdlange \
+         dpbtrf dpbtrs dpbsv pdpbtrf pdtbsm dpb2desc ddesc2pb pdpb2desc pddesc2pb; do
     SRC="$SRC compute/$f.c"
 done
 for f in core_dpotrf core_spotrf core_dtrsm core_strsm core_dsyrk core_ssyrk \
          core_dgemm core_sgemm core_dlacpy core_slacpy core_dsymm core_dgeadd \
          core_dlag2s core_slag2d core_dlansy core_dlange core_dsyssq core_dgessq core_sgeadd \
-         core_dcabs1 core_damax; do
+         core_dcabs1 core_damax core_dgetrf core_sgetrf core_dgeswp core_sgeswp \
+         core_dlacpy_band; do
     SRC="$SRC core_blas/$f.c"
 done
 

@@ -1,7 +1,8 @@
 """ctypes binding of the reference PLASMA itself (test infrastructure only).
 
-oracle/_ref/libplasma_ref.so is the reference's own SPD path, built from its
-sources by oracle/build_ref.sh against the image's OpenBLAS 0.3.15.  Tests
+oracle/_ref/libplasma_ref.so is the reference's own SPD path, LU-based
+mixed-precision solver and band Cholesky, built from its sources by
+oracle/build_ref.sh against the image's OpenBLAS 0.3.15.  Tests
 use it to pin the oracle and this library to the reference's outputs on the
 same bytes, and bench.py's CPU legs time it on the host cores.  The product
 library never loads it.
@@ -20,6 +21,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_ref", "libplasma_ref.so")
 REFERENCE_DIR = os.environ.get("PLASMA_REFERENCE_DIR", "/root/reference")
 UPPER, LOWER = 121, 122
+NOTRANS = 111
 # include/plasma_types.h of the reference
 PlasmaTuning, PlasmaNb = 0, 1
 PlasmaDisabled, PlasmaEnabled = 0, 1
@@ -56,8 +58,16 @@ def lib():
     L.plasma_dposv.argtypes = [ci, ci, ci, vp, ci, vp, ci]
     L.plasma_spotrf.argtypes = [ci, ci, vp, ci]
     L.plasma_dsposv.argtypes = [ci, ci, ci, vp, ci, vp, ci, vp, ci, ctypes.POINTER(ci)]
+    L.plasma_dgetrf.argtypes = [ci, ci, vp, ci, vp]
+    L.plasma_dgetrs.argtypes = [ci, ci, ci, vp, ci, vp, vp, ci]
+    L.plasma_dgesv.argtypes = [ci, ci, vp, ci, vp, vp, ci]
+    L.plasma_dsgesv.argtypes = [ci, ci, vp, ci, vp, vp, ci, vp, ci, ctypes.POINTER(ci)]
+    L.plasma_dpbtrf.argtypes = [ci, ci, ci, vp, ci]
+    L.plasma_dpbtrs.argtypes = [ci, ci, ci, ci, vp, ci, vp, ci]
+    L.plasma_dpbsv.argtypes = [ci, ci, ci, ci, vp, ci, vp, ci]
     for f in ("plasma_dpotrf", "plasma_dpotrs", "plasma_dposv", "plasma_spotrf",
-              "plasma_dsposv"):
+              "plasma_dsposv", "plasma_dgetrf", "plasma_dgetrs", "plasma_dgesv",
+              "plasma_dsgesv", "plasma_dpbtrf", "plasma_dpbtrs", "plasma_dpbsv"):
         getattr(L, f).restype = ci
     # the OpenBLAS the library links: one thread, whatever the environment said
     for name in ("openblas_set_num_threads",):
@@ -138,3 +148,56 @@ def dsposv(uplo, a, b, x, nb=256):
     info = lib().plasma_dsposv(uplo, n, nrhs, _p(a), a.shape[0], _p(b), b.shape[0], _p(x),
                                x.shape[0], ctypes.byref(it))
     return info, it.value
+
+
+def dgetrf(a, nb=256):
+    """In-place LU with partial pivoting of the Fortran-ordered square a;
+    returns (info, ipiv) with 1-based pivots."""
+    import numpy as np
+    set_nb(nb)
+    n = a.shape[0]
+    ipiv = np.zeros(max(n, 1), dtype=np.int32)
+    info = lib().plasma_dgetrf(n, n, _p(a), a.shape[0], _p(ipiv))
+    return info, ipiv[:n]
+
+
+def dgetrs(a, ipiv, b, nb=256):
+    """b <- A^-1 b with the factor and pivots of dgetrf."""
+    import numpy as np
+    set_nb(nb)
+    n, nrhs = b.shape
+    ipiv = np.ascontiguousarray(ipiv, dtype=np.int32)
+    return lib().plasma_dgetrs(NOTRANS, n, nrhs, _p(a), a.shape[0], _p(ipiv), _p(b),
+                               b.shape[0])
+
+
+def dsgesv(a, b, x, nb=256):
+    """The reference's LU-based mixed-precision solve; returns (info, iter,
+    ipiv).  a and b are left as they were, x receives the solution."""
+    import numpy as np
+    set_nb(nb)
+    n, nrhs = b.shape
+    it = ctypes.c_int(0)
+    ipiv = np.zeros(max(n, 1), dtype=np.int32)
+    info = lib().plasma_dsgesv(n, nrhs, _p(a), a.shape[0], _p(ipiv), _p(b), b.shape[0],
+                               _p(x), x.shape[0], ctypes.byref(it))
+    return info, it.value, ipiv[:n]
+
+
+def dpbtrf(uplo, ab, kd, nb=256):
+    """In-place band Cholesky of the LAPACK band array ab ((kd+1) x n)."""
+    set_nb(nb)
+    return lib().plasma_dpbtrf(uplo, ab.shape[1], kd, _p(ab), ab.shape[0])
+
+
+def dpbtrs(uplo, ab, kd, b, nb=256):
+    set_nb(nb)
+    n, nrhs = b.shape
+    return lib().plasma_dpbtrs(uplo, n, kd, nrhs, _p(ab), ab.shape[0], _p(b), b.shape[0])
+
+
+def dpbsv(uplo, ab, kd, b, nb=256):
+    """ab is overwritten by the band factor, b by the solution; returns info."""
+    set_nb(nb)
+    n, nrhs = b.shape
+    return lib().plasma_dpbsv(uplo, n, kd, nrhs, _p(ab), ab.shape[0], _p(b), b.shape[0])

@@ -1,7 +1,7 @@
 /* Minimal CBLAS declarations for building the reference PLASMA's SPD path
  * against the OpenBLAS shipped in the image.  Written from the public CBLAS
- * interface (enum values and the prototypes of the seven routines the path
- * calls); test infrastructure only. */
+ * interface (enum values and the prototypes of the routines the SPD, LU and
+ * band paths call); test infrastructure only. */
 #ifndef ORACLE_REF_SHIM_CBLAS_H
 #define ORACLE_REF_SHIM_CBLAS_H
 #ifdef __cplusplus
@@ -36,6 +36,14 @@ void cblas_strsm(CBLAS_ORDER order, CBLAS_SIDE side, CBLAS_UPLO uplo,
 void cblas_dsymm(CBLAS_ORDER order, CBLAS_SIDE side, CBLAS_UPLO uplo,
                  int m, int n, double alpha, const double *a, int lda,
                  const double *b, int ldb, double beta, double *c, int ldc);
+void cblas_dswap(int n, double *x, int incx, double *y, int incy);
+void cblas_sswap(int n, float *x, int incx, float *y, int incy);
+void cblas_dscal(int n, double alpha, double *x, int incx);
+void cblas_sscal(int n, float alpha, float *x, int incx);
+void cblas_dger(CBLAS_ORDER order, int m, int n, double alpha, const double *x, int incx,
+                const double *y, int incy, double *a, int lda);
+void cblas_sger(CBLAS_ORDER order, int m, int n, float alpha, const float *x, int incx,
+                const float *y, int incy, float *a, int lda);
 
 #ifdef __cplusplus
 }
