@@ -232,10 +232,15 @@ static void residual(plasma_context_t *plasma, plasma_desc_t A, plasma_desc_t B,
     plasma_cuda_colmax(S, st, R, rn);
 }
 
+/* zcgesv.c conv() (Rnorm <= Xnorm * cte for every column), except that a
+ * non-finite norm never counts as converged: the reference's form (fail
+ * only if Rnorm > Xnorm * cte) passes a NaN residual, and an overflowed
+ * iterate makes the bound infinite; such an iteration falls back to the
+ * FP64 LU after its last step instead. */
 static int converged(const double *rn, const double *xn, int nrhs, double cte)
 {
     for (int j = 0; j < nrhs; j++)
-        if (!(rn[j] <= xn[j] * cte))
+        if (!isfinite(xn[j]) || !isfinite(rn[j]) || !(rn[j] <= xn[j] * cte))
             return 0;
     return 1;
 }

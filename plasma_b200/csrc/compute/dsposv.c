@@ -231,8 +231,11 @@ static int refine_column(refine_t *R, int scheme, double cte, int give_up,
         *rn_out = rn;
         if ((*status = take_status(R->plasma)) != 0)
             return -1;                     /* FP32 overflow in a conversion */
-        /* stopping rule of the reference's conv(), zcposv.c:275-287 */
-        if (rn <= xn * cte)
+        /* stopping rule of the reference's conv(), zcposv.c:275-287, except
+         * that a non-finite norm never counts as converged (the reference's
+         * form passes a NaN residual, and an overflowed iterate makes the
+         * bound infinite) */
+        if (isfinite(xn) && isfinite(rn) && rn <= xn * cte)
             return it;
         if (it == ITERMAX)
             break;
