@@ -17,7 +17,24 @@ the reference's own answers where the reference itself cannot travel:
 Factors are stored as checksums (diag(L), L v with gen.probe_vector) rather
 than whole, to keep the file small.
 
-Run: python tests/golden/make_ref_golden.py   (builds oracle/_ref if needed)
+reference_lu_band_fixtures.npz holds the same for the LU-based
+mixed-precision solver and the band Cholesky:
+  lu_n{n}_nb{nb}_*   dgetrf of gen.general (seed 9500 + n): the pivots, diag(U),
+                     L v and U v (L unit lower); getrs_X with 3 right-hand
+                     sides on that factor (n = 300);
+  luinfo_{col}       dgetrf's info for a zeroed column (n = 400, nb = 64);
+  gesv_n{n}_k{e}_*   dsgesv on gen.general_spectrum (kappa 1e2, 1e5): info,
+                     iter, X.  Only kappa <= 1e5: above about 1e10 the
+                     reference's dsgesv is not reproducible (its iteration
+                     count and whether X holds NaN change with the thread
+                     count and from run to run, since its convergence test
+                     passes a NaN residual);
+  pb_n{n}_kd{kd}_{L,U}_*  dpbsv of gen.band: the factor's diagonal, its
+                     L v (or U^T v) and the solution; pbinfo_* dpbtrf's info
+                     for a zeroed row and column.
+
+Run: python tests/golden/make_ref_golden.py [spd|lu_band]  (default both;
+builds oracle/_ref if needed)
 """
 import os
 import sys
@@ -134,5 +151,73 @@ def main():
             print(f"  {k} = {int(out[k])}")
 
 
+def lu_band():
+    ref.set_threads(min(8, os.cpu_count() or 1))
+    out = {}
+    for n, nb in ((300, 64), (1000, 128)):
+        a, b = gen.general(n, 3, seed=9500 + n)
+        f = F(a)
+        info, ipiv = ref.dgetrf(f, nb)
+        assert info == 0
+        v = gen.probe_vector(n)
+        key = f"lu_n{n}_nb{nb}"
+        out[f"{key}_ipiv"] = ipiv.astype(np.int32)
+        out[f"{key}_diagU"] = np.diag(f).copy()
+        out[f"{key}_Lv"] = (np.tril(f, -1) + np.eye(n)) @ v
+        out[f"{key}_Uv"] = np.triu(f) @ v
+        if n == 300:
+            x = F(b)
+            assert ref.dgetrs(f, ipiv, x, nb) == 0
+            out[f"{key}_getrs_X"] = x
+    a, _ = gen.general(400, 1, seed=9600)
+    for col in (0, 150, 399):
+        f = F(a)
+        f[:, col] = 0.0
+        out[f"luinfo_{col}"] = np.int64(ref.dgetrf(f, 64)[0])
+    for n, nb in ((400, 64), (1000, 128)):
+        for kexp in (2, 5):
+            if n == 1000 and kexp == 2:
+                continue
+            a = gen.general_spectrum(n, 10.0 ** kexp)
+            b = F(np.cos(np.arange(2.0 * n)).reshape(n, 2))
+            x = F(np.zeros((n, 2)))
+            info, it, _ = ref.dsgesv(F(a), F(b), x, nb)
+            assert info == 0 and it >= 0, (n, kexp, info, it)
+            key = f"gesv_n{n}_k{kexp}"
+            out[f"{key}_info"] = np.int64(info)
+            out[f"{key}_iter"] = np.int64(it)
+            out[f"{key}_X"] = x
+    for n, kd, nb in ((500, 40, 64), (1000, 100, 128)):
+        a, abl, abu, b = gen.band(n, kd, 2, seed=7000 + n)
+        v = gen.probe_vector(n)
+        for uplo, ab, tag in ((LO, abl, "L"), (UP, abu, "U")):
+            f = F(ab)
+            x = F(b)
+            assert ref.dpbsv(uplo, f, kd, x, nb) == 0
+            t = gen.from_band(f, kd, lower=uplo == LO)
+            t = t if uplo == LO else t.T
+            key = f"pb_n{n}_kd{kd}_{tag}"
+            out[f"{key}_diag"] = np.diag(t).copy()
+            out[f"{key}_Lv"] = t @ v
+            out[f"{key}_X"] = x
+    a, _, _, _ = gen.band(300, 20, 1, seed=7300)
+    for col, tag, uplo in ((0, "L", LO), (137, "L", LO), (137, "U", UP)):
+        z = a.copy()
+        z[col, :] = 0.0
+        z[:, col] = 0.0
+        ab = gen.to_band(z, 20, lower=uplo == LO)
+        out[f"pbinfo_{col}_{tag}"] = np.int64(ref.dpbtrf(uplo, F(ab), 20, 64))
+    path = os.path.join(HERE, "reference_lu_band_fixtures.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}: {len(out)} arrays")
+    for k in sorted(out):
+        if k.endswith("_info") or k.endswith("_iter") or "info_" in k:
+            print(f"  {k} = {int(out[k])}")
+
+
 if __name__ == "__main__":
-    main()
+    which = sys.argv[1] if len(sys.argv) > 1 else "all"
+    if which in ("spd", "all"):
+        main()
+    if which in ("lu_band", "all"):
+        lu_band()

@@ -3,7 +3,9 @@
 reference_fixtures.npz holds what the reference itself (built from its
 sources by oracle/build_ref.sh, run by tests/golden/make_ref_golden.py)
 returns on seeded inputs: factor checksums, solutions, dsposv's iter and
-info, and its failure semantics.  The oracle must agree before it is trusted
+info, and its failure semantics; reference_lu_band_fixtures.npz the same
+for its LU-based mixed-precision solver (dgetrf, dgetrs, dsgesv) and band
+Cholesky (dpbtrf, dpbsv).  The oracle must agree before it is trusted
 as the checker of the GPU library.  Where the reference library is present
 (oracle/_ref), a few cases are also run live against it, and the library's
 argument codes are compared with the reference's.
@@ -211,3 +213,130 @@ def test_library_argument_codes_match_reference(monkeypatch):
             assert got == want, (uplo, n, lda, got, want)
     finally:
         L.plasma_finalize()
+
+
+@pytest.fixture(scope="session")
+def rlb():
+    return np.load(os.path.join(os.path.dirname(__file__), "golden",
+                                "reference_lu_band_fixtures.npz"))
+
+
+def normwise(y, yr, t):
+    """||y - yr|| / (||T||_F ||v||) for checksums y = T v of a factor T."""
+    return np.linalg.norm(y - yr) / (np.linalg.norm(t) * np.linalg.norm(gen.probe_vector(len(y))))
+
+
+@pytest.mark.parametrize("n,nb", [(300, 64), (1000, 128)])
+def test_oracle_getrf_matches_reference(rlb, n, nb):
+    """Tile LU with partial pivoting (compute/pzgetrf.c with the panel of
+    core_blas/core_zgetrf.c): the reference's pivots exactly, and its factor
+    through L v and U v to within the getrf tester's 50 eps
+    (test/test_zgetrf.c:116-138); the solve of compute/zgetrs.c."""
+    a, b = gen.general(n, 3, seed=9500 + n)
+    f = F(a)
+    info, ipiv = oracle.getrf(f, nb)
+    assert info == 0
+    key = f"lu_n{n}_nb{nb}"
+    np.testing.assert_array_equal(ipiv, rlb[f"{key}_ipiv"])
+    v = gen.probe_vector(n)
+    lo, up = np.tril(f, -1) + np.eye(n), np.triu(f)
+    assert normwise(lo @ v, rlb[f"{key}_Lv"], lo) < TOL * EPS
+    assert normwise(up @ v, rlb[f"{key}_Uv"], up) < TOL * EPS
+    d, dr = np.diag(up), rlb[f"{key}_diagU"]
+    assert np.abs(d - dr).max() / np.abs(dr).max() < TOL * n * EPS
+    if n == 300:
+        x = F(b)
+        assert oracle.getrs(f, ipiv, x) == 0
+        close(x, rlb[f"{key}_getrs_X"], tol=1e-11)
+
+
+@pytest.mark.parametrize("col", [0, 150, 399])
+def test_oracle_getrf_zero_column_matches_reference(rlb, col):
+    """A zeroed column: the first zero pivot.  The reference's LAPACK-layout
+    plasma_dgetrf returns it offset by min(m, n) (compute/zgetrf.c:101 adds
+    imin(m, n) to the tile routine's status, which is LAPACK's index); the
+    oracle reports the tile routine's (and LAPACK's) value."""
+    a, _ = gen.general(400, 1, seed=9600)
+    f = F(a)
+    f[:, col] = 0.0
+    info, _ = oracle.getrf(f, 64)
+    assert info == col + 1 == int(rlb[f"luinfo_{col}"]) - 400
+
+
+@pytest.mark.parametrize("n,nb,kexp", [(400, 64, 2), (400, 64, 5), (1000, 128, 5)])
+def test_oracle_dsgesv_matches_reference(rlb, n, nb, kexp):
+    """FP32 LU + FP64 refinement (compute/zcgesv.c:363-532) on
+    A = U diag(sigma) V^T, kappa 1e2 and 1e5: the reference's info and
+    iteration count, and its solution to within kappa n eps.  (The
+    reference's iteration count can move by one with its thread count; the
+    fixture ran 8 threads.)"""
+    a = gen.general_spectrum(n, 10.0 ** kexp)
+    b = F(np.cos(np.arange(2.0 * n)).reshape(n, 2))
+    x = F(np.zeros((n, 2)))
+    info, it, _ = oracle.dsgesv(F(a), b, x, nb)
+    key = f"gesv_n{n}_k{kexp}"
+    assert info == int(rlb[f"{key}_info"]) == 0
+    assert abs(it - int(rlb[f"{key}_iter"])) <= 1
+    xr = rlb[f"{key}_X"]
+    assert np.abs(x - xr).max() / np.abs(xr).max() < 10.0 ** kexp * n * EPS
+
+
+@pytest.mark.parametrize("n,kd,nb", [(500, 40, 64), (1000, 100, 128)])
+@pytest.mark.parametrize("tag", ["L", "U"])
+def test_oracle_band_matches_reference(rlb, n, kd, nb, tag):
+    """Band tile Cholesky and band solves (compute/pzpbtrf.c, pztbsm.c,
+    zpbsv.c): the reference's band factor through its diagonal and L v, and
+    its dpbsv solution."""
+    a, abl, abu, b = gen.band(n, kd, 2, seed=7000 + n)
+    uplo, ab = (LO, abl) if tag == "L" else (UP, abu)
+    f = F(ab)
+    assert oracle.pbtrf(uplo, f, kd, nb) == 0
+    x = F(b)
+    assert oracle.pbtrs(uplo, f, kd, x, nb) == 0
+    t = gen.from_band(f, kd, lower=uplo == LO)
+    t = t if uplo == LO else t.T
+    key = f"pb_n{n}_kd{kd}_{tag}"
+    assert np.abs(np.diag(t) - rlb[f"{key}_diag"]).max() / np.abs(np.diag(t)).max() < TOL * EPS
+    assert normwise(t @ gen.probe_vector(n), rlb[f"{key}_Lv"], t) < TOL * EPS
+    close(x, rlb[f"{key}_X"])
+
+
+@pytest.mark.parametrize("col,tag", [(0, "L"), (137, "L"), (137, "U")])
+def test_oracle_band_info_matches_reference(rlb, col, tag):
+    """A zeroed row and column of a band matrix: dpbtrf's info."""
+    a, _, _, _ = gen.band(300, 20, 1, seed=7300)
+    a[col, :] = 0.0
+    a[:, col] = 0.0
+    uplo = LO if tag == "L" else UP
+    ab = gen.to_band(a, 20, lower=uplo == LO)
+    assert oracle.pbtrf(uplo, F(ab), 20, 64) == int(rlb[f"pbinfo_{col}_{tag}"]) == col + 1
+
+
+@needs_ref
+def test_oracle_lu_band_against_live_reference():
+    """Fresh seeds on the reference library and the oracle: LU pivots and
+    solve, dsgesv at kappa 1e3, band solve."""
+    n, nb = 700, 96
+    a, b = gen.general(n, 2, seed=31)
+    fr, fo = F(a), F(a)
+    ir, pr = ref.dgetrf(fr, nb)
+    io, po = oracle.getrf(fo, nb)
+    assert ir == io == 0
+    np.testing.assert_array_equal(pr, po)
+    xr, xo = F(b), F(b)
+    assert ref.dgetrs(fr, pr, xr, nb) == 0
+    assert oracle.getrs(fo, po, xo) == 0
+    close(xo, xr, tol=1e-11)
+    s = gen.general_spectrum(n, 1e3, seed=32)
+    xr, xo = F(np.zeros((n, 2))), F(np.zeros((n, 2)))
+    ir, itr, _ = ref.dsgesv(F(s), F(b), xr, nb)
+    io, ito, _ = oracle.dsgesv(F(s), F(b), xo, nb)
+    assert ir == io == 0 and abs(itr - ito) <= 1
+    assert np.abs(xo - xr).max() / np.abs(xr).max() < 1e3 * n * EPS
+    _, abl, _, bb = gen.band(n, 60, 1, seed=33)
+    fr, fo = F(abl), F(abl)
+    xr, xo = F(bb), F(bb)
+    assert ref.dpbsv(LO, fr, 60, xr, nb) == 0
+    assert oracle.pbtrf(LO, fo, 60, nb) == 0
+    assert oracle.pbtrs(LO, fo, 60, xo, nb) == 0
+    close(xo, xr)
