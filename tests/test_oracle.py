@@ -285,6 +285,22 @@ def test_dsgesv_against_lapack(golden, kappa, iters):
     assert np.abs(x - xr).max() / np.abs(xr).max() < 10 * kappa * n * EPS
 
 
+@pytest.mark.parametrize("kappa", [1e10, 1e12])
+def test_dsgesv_diverging_refinement_falls_back(kappa):
+    """kappa = 1e10 and 1e12 at n = 400: the FP32-preconditioned iteration
+    diverges.  A NaN or infinite iterate must not pass the stopping rule
+    (the reference's form, zcgesv.c:265-276, accepts a NaN residual), so the
+    oracle ends in the FP64 fallback with a finite solution."""
+    n = 400
+    a = gen.general_spectrum(n, kappa)
+    b = np.asfortranarray(np.cos(np.arange(2.0 * n)).reshape(n, 2))
+    x = np.zeros((n, 2), order="F")
+    info, it, _ = oracle.dsgesv(np.asfortranarray(a.copy()), b.copy(order="F"), x, 64)
+    assert info == 0 and it == -31
+    assert np.isfinite(x).all()
+    assert solve_residual(a, x, b) < TOL * EPS
+
+
 def test_dsgesv_fp32_overflow_falls_back():
     n = 50
     a, b = gen.general(n, 1, seed=77)
