@@ -253,6 +253,46 @@ def cpu_baseline(a, b, nb=256):
             "seconds": dt}
 
 
+def reference_built():
+    from oracle import ref
+    return os.path.exists(ref.LIB_PATH)
+
+
+def reference_sample(routine, n, extra, nb, threads, dt, info, it=None):
+    return {"value": dt * 1e3, "unit": "ms", "cores": threads, "kind": "reference",
+            "sample": f"reference PLASMA plasma_{routine} (oracle/_ref, OpenBLAS 0.3.15 "
+                      f"single-threaded, {threads} OpenMP threads on {cpu_model()}), one "
+                      f"solve of the same n={n}{extra} system, nb={nb}: {dt:.2f} s, "
+                      f"info {info}" + ("" if it is None else f", iter {it}")}
+
+
+def reference_dsgesv_cpu(a, b, nb=256):
+    """The reference's own plasma_dsgesv on the host cores (one solve of the
+    workload's system, host copies a, b in Fortran order): the cpu_baseline
+    entry of the LU workload."""
+    from oracle import ref
+    threads = os.cpu_count() or 1
+    ref.set_threads(threads)
+    x = np.zeros(b.shape, order="F")
+    t0 = time.perf_counter()
+    info, it, _ = ref.dsgesv(a, b, x, nb)
+    dt = time.perf_counter() - t0
+    return reference_sample("dsgesv", a.shape[0], "", nb, threads, dt, info, it)
+
+
+def reference_dpbsv_cpu(ab, kd, b, nb=256):
+    """The reference's own plasma_dpbsv (lower band storage ab, (kd+1) x n,
+    Fortran order) on the host cores: the band workload's cpu_baseline."""
+    from oracle import ref
+    threads = os.cpu_count() or 1
+    ref.set_threads(threads)
+    ab, x = np.asfortranarray(ab.copy()), np.asfortranarray(b.copy())
+    t0 = time.perf_counter()
+    info = ref.dpbsv(ref.LOWER, ab, kd, x, nb)
+    dt = time.perf_counter() - t0
+    return reference_sample("dpbsv", ab.shape[1], f" kd={kd}", nb, threads, dt, info)
+
+
 def max_over_ranks(ms, world, device):
     """The job's step time: the slowest replica's (MAX over the ranks of the
     initialised process group; every rank gets it)."""
@@ -439,7 +479,7 @@ def run_band(args):
     import plasma_b200 as pb
     L = pb.lib()
     assert L.plasma_init() == 0
-    n, rows = 32768, []
+    n, rows, ref_done = 32768, [], set()
     for kd in [int(v) for v in args.band_kd.split(",")]:
         g = torch.Generator(device="cuda").manual_seed(9)
         # column-major (kd+1) x n storage = row-major n x (kd+1)
@@ -493,9 +533,17 @@ def run_band(args):
             res = ((b0 - ax).abs().max() / (n * anorm * xd.abs().max())).item()
             ms = min(times)
             flops = n * (kd * kd + 3.0 * kd) + 4.0 * n * kd
-            rows.append({"routine": f"{fn}pbsv", "n": n, "kd": kd, "nb": nb_used.value,
-                         "ms": ms, "pbtrf_ms": min(trf), "gflops": flops / ms / 1e6,
-                         "tester_residual": res})
+            row = {"routine": f"{fn}pbsv", "n": n, "kd": kd, "nb": nb_used.value,
+                   "ms": ms, "pbtrf_ms": min(trf), "gflops": flops / ms / 1e6,
+                   "tester_residual": res, "cpu_baseline": None}
+            if fn == "d" and reference_built() and kd not in ref_done:
+                # column-major (kd+1) x n band storage = AB0 (row-major n x (kd+1))
+                ab_host = np.asfortranarray(AB0.cpu().numpy().T)
+                b_host = np.asfortranarray(b0.cpu().numpy().reshape(n, 1))
+                row["cpu_baseline"] = reference_dpbsv_cpu(ab_host, kd, b_host)
+                ref_done.add(kd)
+                del ab_host
+            rows.append(row)
             del AB, AB1, x
     print(json.dumps({"workload": "band", "metric": "time of the SPD band solve "
                       "(pbsv = pbtrf + pbtrs), device-resident AB, uplo = L, nrhs = 1",
@@ -543,9 +591,15 @@ def run_lu(args):
         r = b - A.T @ x
         res = (r.abs().max() / (n * A.abs().sum(dim=0).max() * x.abs().max())).item()
         ms = min(times)
-        rows.append({"routine": "dsgesv", "n": n, "ms": ms, "iter": it.value,
-                     "gflops": (2 * n ** 3 / 3 + 2 * n ** 2) / ms / 1e6,
-                     "tester_residual": res})
+        row = {"routine": "dsgesv", "n": n, "ms": ms, "iter": it.value,
+               "gflops": (2 * n ** 3 / 3 + 2 * n ** 2) / ms / 1e6,
+               "tester_residual": res, "cpu_baseline": None}
+        if reference_built():
+            # the column-major matrix the library read is A.T
+            a_host = np.asfortranarray(A.T.cpu().numpy())
+            b_host = np.asfortranarray(b.cpu().numpy().reshape(n, 1))
+            row["cpu_baseline"] = reference_dsgesv_cpu(a_host, b_host)
+        rows.append(row)
     print(json.dumps({"workload": "lu", "metric": "time of the LU-based mixed-precision "
                       "solve (dsgesv), device-resident A, nrhs = 1",
                       "unit": "ms", "steps": args.steps, "warmup": args.warmup,
