@@ -7,7 +7,9 @@ The library (through its C ABI) against
     and the failure semantics (--zerocol info, FP32 overflow, kappa = 1e12);
   * the reference library itself (oracle/_ref/libplasma_ref.so, built by
     oracle/build_ref.sh), when present: the whole config-1 factor with the
-    potrf tester's check (test/test_zpotrf.c:124-141).
+    potrf tester's check (test/test_zpotrf.c:124-141);
+  * reference_lu_band_fixtures.npz: the reference's dsgesv (kappa 1e2, 1e5)
+    and dpbsv outputs and dpbtrf's info.
 The iteration count may differ by one: the FP32 factor here comes from
 tensor-core tiles (three TF32 products per FP32 product) and a different
 summation order than OpenBLAS's sgemm.
@@ -210,3 +212,67 @@ def test_dsposv_against_reference_library(L, n, nb, kappa):
     assert info == info_r == 0
     assert abs(it - it_r) <= 1, (it, it_r)
     close(x, xr, kappa * 1e-13)
+
+
+@pytest.fixture(scope="module")
+def rlb():
+    return np.load(os.path.join(os.path.dirname(__file__), "golden",
+                                "reference_lu_band_fixtures.npz"))
+
+
+@pytest.mark.parametrize("n,nb,kexp", [(400, 64, 2), (400, 64, 5), (1000, 128, 5)])
+def test_dsgesv_matches_reference(L, rlb, n, nb, kexp):
+    """dsgesv (compute/zcgesv.c:363-532) on the reference's fixture: its
+    info, refinement without the FP64 fallback in about as many steps (the
+    FP32 LU here is tensor-core tiles in another summation order than
+    OpenBLAS's), the solution within kappa n eps of the reference's, and
+    the tester's residual (test/test_zcgesv.c:150-170)."""
+    set_nb(L, nb)
+    a = gen.general_spectrum(n, 10.0 ** kexp)
+    b = F(np.cos(np.arange(2.0 * n)).reshape(n, 2))
+    af, bf = F(a), F(b)
+    x = F(np.zeros((n, 2)))
+    piv = np.zeros(n, dtype=np.int32)
+    it = ctypes.c_int(-99)
+    info = L.plasma_dsgesv(n, 2, af.ctypes.data, n, piv.ctypes.data, bf.ctypes.data, n,
+                           x.ctypes.data, n, ctypes.byref(it))
+    key = f"gesv_n{n}_k{kexp}"
+    assert info == int(rlb[f"{key}_info"]) == 0
+    assert it.value >= 0 and abs(it.value - int(rlb[f"{key}_iter"])) <= 2, it.value
+    close(x, rlb[f"{key}_X"], 10.0 ** kexp * n * EPS)
+    assert solve_residual(a, x, b) < TOL * EPS
+
+
+@pytest.mark.parametrize("n,kd,nb", [(500, 40, 64), (1000, 100, 128)])
+@pytest.mark.parametrize("tag", ["L", "U"])
+def test_dpbsv_matches_reference(L, rlb, n, kd, nb, tag):
+    """Band factor and solve (compute/zpbsv.c) against the reference's
+    dpbsv on the same bytes: the factor's diagonal and L v, the solution,
+    and the tester's residual."""
+    set_nb(L, nb)
+    a, abl, abu, b = gen.band(n, kd, 2, seed=7000 + n)
+    lower = tag == "L"
+    ab, x = F(abl if lower else abu), F(b)
+    assert L.plasma_dpbsv(LO if lower else UP, n, kd, 2, ab.ctypes.data, kd + 1,
+                          x.ctypes.data, n) == 0
+    t = gen.from_band(ab, kd, lower=lower)
+    t = t if lower else t.T
+    key = f"pb_n{n}_kd{kd}_{tag}"
+    close(np.diag(t), rlb[f"{key}_diag"], 1e-12)
+    v = gen.probe_vector(n)
+    assert np.linalg.norm(t @ v - rlb[f"{key}_Lv"]) / (np.linalg.norm(t) * np.linalg.norm(v)) < 1e-12
+    close(x, rlb[f"{key}_X"], 1e-11)
+    assert solve_residual(a, x, b) < TOL * EPS
+
+
+@pytest.mark.parametrize("col,tag", [(0, "L"), (137, "L"), (137, "U")])
+def test_dpbtrf_info_matches_reference(L, rlb, col, tag):
+    """A zeroed row and column of a band matrix: the reference's dpbtrf info."""
+    set_nb(L, 64)
+    a, _, _, _ = gen.band(300, 20, 1, seed=7300)
+    a[col, :] = 0.0
+    a[:, col] = 0.0
+    lower = tag == "L"
+    ab = F(gen.to_band(a, 20, lower=lower))
+    info = L.plasma_dpbtrf(LO if lower else UP, 300, 20, ab.ctypes.data, 21)
+    assert info == int(rlb[f"pbinfo_{col}_{tag}"]) == col + 1
