@@ -1,7 +1,8 @@
 #!/usr/bin/env bash
 # Build the reference PLASMA's SPD path (dpotrf, dpotrs, dposv, dsposv and
 # what they call), its LU-based mixed-precision solver (dsgesv with dgetrf,
-# dgetrs) and its band Cholesky (dpbtrf, dpbtrs, dpbsv) as a shared library,
+# dgetrs), its band Cholesky (dpbtrf, dpbtrs, dpbsv) and its SPD inverse
+# (dpotri, dpoinv) as a shared library,
 # oracle/_ref/libplasma_ref.so, for the parity tests and for the CPU
 # reference arm of bench.py.  Test infrastructure: the product never loads
 # it.
@@ -52,10 +53,12 @@ COMPUTE_Z="zpotrf zpotrs zposv zcposv pzpotrf pztrsm pzsymm pzlansy pzlacpy
            pzgeadd pzlag2c pclag2z zge2desc zdesc2ge ztr2desc zdesc2tr pzge2desc
            pzdesc2ge pztr2desc pzdesc2tr pdzamax
            zgetrf zgetrs zgesv zcgesv pzgetrf pzgeswp pzgemm pzlange
-           zpbtrf zpbtrs zpbsv pzpbtrf pztbsm zpb2desc zdesc2pb pzpb2desc pzdesc2pb"
+           zpbtrf zpbtrs zpbsv pzpbtrf pztbsm zpb2desc zdesc2pb pzpb2desc pzdesc2pb
+           zpotri zpoinv pztrtri pzlauum"
 CORE_Z="core_zpotrf core_ztrsm core_zsyrk core_zgemm core_zsymm core_zlacpy
         core_zgeadd core_zlansy core_zlange core_zsyssq core_zgessq core_zlag2c
-        core_clag2z core_dzamax core_zgetrf core_zgeswp core_zlacpy_band"
+        core_clag2z core_dzamax core_zgetrf core_zgeswp core_zlacpy_band
+        core_ztrmm core_ztrtri core_zlauum"
 HDR_Z="plasma_z plasma_zc plasma_internal_z plasma_internal_zc plasma_core_blas_z
        plasma_core_blas_zc core_lapack_z plasma_zlaebz2_work"
 
@@ -72,14 +75,15 @@ for f in dpotrf dpotrs dposv dsposv spotrf spotrs sposv pdpotrf pspotrf pdtrsm \
          sdesc2tr pdge2desc pddesc2ge pdtr2desc pddesc2tr psge2desc psdesc2ge \
          pstr2desc psdesc2tr \
          dgetrf dgetrs dgesv dsgesv pdgetrf psgetrf pdgeswp psgeswp pdgemm pdlange \
-         dpbtrf dpbtrs dpbsv pdpbtrf pdtbsm dpb2desc ddesc2pb pdpb2desc pddesc2pb; do
+         dpbtrf dpbtrs dpbsv pdpbtrf pdtbsm dpb2desc ddesc2pb pdpb2desc pddesc2pb \
+         dpotri dpoinv pdtrtri pdlauum; do
     SRC="$SRC compute/$f.c"
 done
 for f in core_dpotrf core_spotrf core_dtrsm core_strsm core_dsyrk core_ssyrk \
          core_dgemm core_sgemm core_dlacpy core_slacpy core_dsymm core_dgeadd \
          core_dlag2s core_slag2d core_dlansy core_dlange core_dsyssq core_dgessq core_sgeadd \
          core_dcabs1 core_damax core_dgetrf core_sgetrf core_dgeswp core_sgeswp \
-         core_dlacpy_band; do
+         core_dlacpy_band core_dtrmm core_dtrtri core_dlauum; do
     SRC="$SRC core_blas/$f.c"
 done
 

@@ -1,7 +1,7 @@
 """ctypes binding of the reference PLASMA itself (test infrastructure only).
 
 oracle/_ref/libplasma_ref.so is the reference's own SPD path, LU-based
-mixed-precision solver and band Cholesky, built from its sources by
+mixed-precision solver, band Cholesky and SPD inverse, built from its sources by
 oracle/build_ref.sh against the image's OpenBLAS 0.3.15.  Tests
 use it to pin the oracle and this library to the reference's outputs on the
 same bytes, and bench.py's CPU legs time it on the host cores.  The product
@@ -65,9 +65,12 @@ def lib():
     L.plasma_dpbtrf.argtypes = [ci, ci, ci, vp, ci]
     L.plasma_dpbtrs.argtypes = [ci, ci, ci, ci, vp, ci, vp, ci]
     L.plasma_dpbsv.argtypes = [ci, ci, ci, ci, vp, ci, vp, ci]
+    L.plasma_dpotri.argtypes = [ci, ci, vp, ci]
+    L.plasma_dpoinv.argtypes = [ci, ci, vp, ci]
     for f in ("plasma_dpotrf", "plasma_dpotrs", "plasma_dposv", "plasma_spotrf",
               "plasma_dsposv", "plasma_dgetrf", "plasma_dgetrs", "plasma_dgesv",
-              "plasma_dsgesv", "plasma_dpbtrf", "plasma_dpbtrs", "plasma_dpbsv"):
+              "plasma_dsgesv", "plasma_dpbtrf", "plasma_dpbtrs", "plasma_dpbsv",
+              "plasma_dpotri", "plasma_dpoinv"):
         getattr(L, f).restype = ci
     # the OpenBLAS the library links: one thread, whatever the environment said
     for name in ("openblas_set_num_threads",):
@@ -201,3 +204,16 @@ def dpbsv(uplo, ab, kd, b, nb=256):
     set_nb(nb)
     n, nrhs = b.shape
     return lib().plasma_dpbsv(uplo, n, kd, nrhs, _p(ab), ab.shape[0], _p(b), b.shape[0])
+
+
+def dpotri(uplo, a, nb=256):
+    """The inverse from the Cholesky factor in the uplo triangle of a (in
+    place, that triangle only); returns info."""
+    set_nb(nb)
+    return lib().plasma_dpotri(uplo, a.shape[0], _p(a), a.shape[0])
+
+
+def dpoinv(uplo, a, nb=256):
+    """Factor and inverse in one call (in place, the uplo triangle)."""
+    set_nb(nb)
+    return lib().plasma_dpoinv(uplo, a.shape[0], _p(a), a.shape[0])

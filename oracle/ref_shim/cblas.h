@@ -1,7 +1,7 @@
 /* Minimal CBLAS declarations for building the reference PLASMA's SPD path
  * against the OpenBLAS shipped in the image.  Written from the public CBLAS
- * interface (enum values and the prototypes of the routines the SPD, LU and
- * band paths call); test infrastructure only. */
+ * interface (enum values and the prototypes of the routines the SPD, LU,
+ * band and inverse paths call); test infrastructure only. */
 #ifndef ORACLE_REF_SHIM_CBLAS_H
 #define ORACLE_REF_SHIM_CBLAS_H
 #ifdef __cplusplus
@@ -36,6 +36,9 @@ void cblas_strsm(CBLAS_ORDER order, CBLAS_SIDE side, CBLAS_UPLO uplo,
 void cblas_dsymm(CBLAS_ORDER order, CBLAS_SIDE side, CBLAS_UPLO uplo,
                  int m, int n, double alpha, const double *a, int lda,
                  const double *b, int ldb, double beta, double *c, int ldc);
+void cblas_dtrmm(CBLAS_ORDER order, CBLAS_SIDE side, CBLAS_UPLO uplo,
+                 CBLAS_TRANSPOSE ta, CBLAS_DIAG diag, int m, int n,
+                 double alpha, const double *a, int lda, double *b, int ldb);
 void cblas_dswap(int n, double *x, int incx, double *y, int incy);
 void cblas_sswap(int n, float *x, int incx, float *y, int incy);
 void cblas_dscal(int n, double alpha, double *x, int incx);

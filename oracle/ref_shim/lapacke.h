@@ -41,6 +41,10 @@ lapack_int LAPACKE_dlag2s_work(int layout, lapack_int m, lapack_int n,
 lapack_int LAPACKE_slag2d_work(int layout, lapack_int m, lapack_int n,
                                const float *sa, lapack_int ldsa, double *a,
                                lapack_int lda);
+lapack_int LAPACKE_dtrtri_work(int layout, char uplo, char diag, lapack_int n,
+                               double *a, lapack_int lda);
+lapack_int LAPACKE_dlauum_work(int layout, char uplo, lapack_int n, double *a,
+                               lapack_int lda);
 double LAPACKE_dlamch_work(char cmach);
 float LAPACKE_slamch_work(char cmach);
 double LAPACKE_dlange_work(int layout, char norm, lapack_int m, lapack_int n,
