@@ -33,8 +33,15 @@ mixed-precision solver and the band Cholesky:
                      L v (or U^T v) and the solution; pbinfo_* dpbtrf's info
                      for a zeroed row and column.
 
-Run: python tests/golden/make_ref_golden.py [spd|lu_band]  (default both;
-builds oracle/_ref if needed)
+reference_potri_fixtures.npz holds its SPD inverse:
+  potri_n{n}_nb{nb}_{L,U}_*  dpotri on its own dpotrf factor of
+                     gen.diag_dominant (seed 8800 + n): the inverse's
+                     diagonal and sym(inv) v; poinv gives the same bytes;
+  potriinfo_{col}_{L,U}  dpotri's info for a zero on the factor's diagonal
+                     (n = 300, nb = 64).
+
+Run: python tests/golden/make_ref_golden.py [spd|lu_band|potri]  (default
+all; builds oracle/_ref if needed)
 """
 import os
 import sys
@@ -215,9 +222,42 @@ def lu_band():
             print(f"  {k} = {int(out[k])}")
 
 
+def potri():
+    ref.set_threads(min(8, os.cpu_count() or 1))
+    out = {}
+    for n, nb in ((300, 64), (1000, 128)):
+        a, _ = gen.diag_dominant(n, 1, seed=8800 + n)
+        v = gen.probe_vector(n)
+        for uplo, tag in ((LO, "L"), (UP, "U")):
+            f = F(a)
+            assert ref.dpotrf(uplo, f, nb) == 0
+            assert ref.dpotri(uplo, f, nb) == 0
+            t = np.tril(f) if uplo == LO else np.triu(f)
+            full = t + t.T - np.diag(np.diag(t))
+            g = F(a)
+            assert ref.dpoinv(uplo, g, nb) == 0
+            tg = np.tril(g) if uplo == LO else np.triu(g)
+            assert np.array_equal(tg, t)
+            key = f"potri_n{n}_nb{nb}_{tag}"
+            out[f"{key}_diag"] = np.diag(t).copy()
+            out[f"{key}_Sv"] = full @ v
+    a, _ = gen.diag_dominant(300, 1, seed=9100)
+    for col in (0, 137, 299):
+        for uplo, tag in ((LO, "L"), (UP, "U")):
+            f = F(a)
+            assert ref.dpotrf(uplo, f, 64) == 0
+            f[col, col] = 0.0
+            out[f"potriinfo_{col}_{tag}"] = np.int64(ref.dpotri(uplo, f, 64))
+    path = os.path.join(HERE, "reference_potri_fixtures.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}: {len(out)} arrays")
+
+
 if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "all"
     if which in ("spd", "all"):
         main()
     if which in ("lu_band", "all"):
         lu_band()
+    if which in ("potri", "all"):
+        potri()

@@ -9,7 +9,8 @@ The library (through its C ABI) against
     oracle/build_ref.sh), when present: the whole config-1 factor with the
     potrf tester's check (test/test_zpotrf.c:124-141);
   * reference_lu_band_fixtures.npz: the reference's dsgesv (kappa 1e2, 1e5)
-    and dpbsv outputs and dpbtrf's info.
+    and dpbsv outputs and dpbtrf's info;
+  * reference_potri_fixtures.npz: its SPD inverse and dpotri's info.
 The iteration count may differ by one: the FP32 factor here comes from
 tensor-core tiles (three TF32 products per FP32 product) and a different
 summation order than OpenBLAS's sgemm.
@@ -276,3 +277,44 @@ def test_dpbtrf_info_matches_reference(L, rlb, col, tag):
     ab = F(gen.to_band(a, 20, lower=lower))
     info = L.plasma_dpbtrf(LO if lower else UP, 300, 20, ab.ctypes.data, 21)
     assert info == int(rlb[f"pbinfo_{col}_{tag}"]) == col + 1
+
+
+@pytest.fixture(scope="module")
+def rpi():
+    return np.load(os.path.join(os.path.dirname(__file__), "golden",
+                                "reference_potri_fixtures.npz"))
+
+
+@pytest.mark.parametrize("n,nb", [(300, 64), (1000, 128)])
+@pytest.mark.parametrize("tag", ["L", "U"])
+def test_poinv_matches_reference(L, rpi, n, nb, tag):
+    """plasma_dpoinv (factor and inverse, compute/zpoinv.c) against the
+    reference's inverse of the same matrix, through the inverse's diagonal
+    and sym(inv) v."""
+    set_nb(L, nb)
+    a, _ = gen.diag_dominant(n, 1, seed=8800 + n)
+    lower = tag == "L"
+    f = F(a)
+    assert L.plasma_dpoinv(LO if lower else UP, n, f.ctypes.data, n) == 0
+    t = np.tril(f) if lower else np.triu(f)
+    full = t + t.T - np.diag(np.diag(t))
+    key = f"potri_n{n}_nb{nb}_{tag}"
+    dr = rpi[f"{key}_diag"]
+    assert np.linalg.norm(np.diag(t) - dr) / np.linalg.norm(dr) < 1e-12
+    v = gen.probe_vector(n)
+    assert (np.linalg.norm(full @ v - rpi[f"{key}_Sv"]) / (np.linalg.norm(full) * np.linalg.norm(v))
+            < 1e-12)
+
+
+@pytest.mark.parametrize("col", [0, 137, 299])
+@pytest.mark.parametrize("tag", ["L", "U"])
+def test_potri_info_matches_reference(L, rpi, col, tag):
+    """A zero on the factor's diagonal: the reference's dpotri info."""
+    set_nb(L, 64)
+    a, _ = gen.diag_dominant(300, 1, seed=9100)
+    lower = tag == "L"
+    f = F(a)
+    assert L.plasma_dpotrf(LO if lower else UP, 300, f.ctypes.data, 300) == 0
+    f[col, col] = 0.0
+    info = L.plasma_dpotri(LO if lower else UP, 300, f.ctypes.data, 300)
+    assert info == int(rpi[f"potriinfo_{col}_{tag}"]) == col + 1

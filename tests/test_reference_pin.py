@@ -340,3 +340,40 @@ def test_oracle_lu_band_against_live_reference():
     assert oracle.pbtrf(LO, fo, 60, nb) == 0
     assert oracle.pbtrs(LO, fo, 60, xo, nb) == 0
     close(xo, xr)
+
+
+@pytest.fixture(scope="session")
+def rpi():
+    return np.load(os.path.join(os.path.dirname(__file__), "golden",
+                                "reference_potri_fixtures.npz"))
+
+
+@pytest.mark.parametrize("n,nb", [(300, 64), (1000, 128)])
+@pytest.mark.parametrize("tag", ["L", "U"])
+def test_oracle_potri_matches_reference(rpi, n, nb, tag):
+    """The inverse from the factor (compute/zpotri.c: pztrtri then pzlauum):
+    the reference's inverse through its diagonal and sym(inv) v, within the
+    potri tester's 50 eps (test/test_zpotri.c:135-155) normwise."""
+    a, _ = gen.diag_dominant(n, 1, seed=8800 + n)
+    uplo = LO if tag == "L" else UP
+    f = F(a)
+    assert oracle.potrf(uplo, f, nb) == 0
+    assert oracle.potri(uplo, f) == 0
+    t = np.tril(f) if uplo == LO else np.triu(f)
+    full = t + t.T - np.diag(np.diag(t))
+    key = f"potri_n{n}_nb{nb}_{tag}"
+    d, dr = np.diag(t), rpi[f"{key}_diag"]
+    assert np.linalg.norm(d - dr) / np.linalg.norm(dr) < TOL * EPS
+    assert normwise(full @ gen.probe_vector(n), rpi[f"{key}_Sv"], full) < TOL * EPS
+
+
+@pytest.mark.parametrize("col", [0, 137, 299])
+@pytest.mark.parametrize("tag", ["L", "U"])
+def test_oracle_potri_info_matches_reference(rpi, col, tag):
+    """A zero on the factor's diagonal: dpotri's info (dtrtri's index)."""
+    a, _ = gen.diag_dominant(300, 1, seed=9100)
+    uplo = LO if tag == "L" else UP
+    f = F(a)
+    assert oracle.potrf(uplo, f, 64) == 0
+    f[col, col] = 0.0
+    assert oracle.potri(uplo, f) == int(rpi[f"potriinfo_{col}_{tag}"]) == col + 1
