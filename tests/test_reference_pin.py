@@ -215,6 +215,59 @@ def test_library_argument_codes_match_reference(monkeypatch):
         L.plasma_finalize()
 
 
+@needs_ref
+def test_library_argument_codes_match_reference_next_rows(monkeypatch):
+    """dsgesv, the band routines and the inverse: the library returns the
+    reference's code for each illegal argument and quick return (host-only
+    context, so only cases where neither side computes)."""
+    import plasma_b200 as pb
+    monkeypatch.setenv("PLASMA_ALLOW_NO_DEVICE", "1")
+    L = pb.lib()
+    R = ref.lib()
+    if L.plasma_init() != 0:
+        pytest.skip("library context unavailable")
+    vp = ctypes.c_void_p
+    try:
+        buf = np.zeros(64 * 8)
+        p = buf.ctypes.data
+        piv = np.zeros(64, dtype=np.int32)
+        it1, it2 = ctypes.c_int(5), ctypes.c_int(5)
+        for n, nrhs, lda, ldb, ldx in ((-1, 2, 8, 8, 8), (8, -1, 8, 8, 8), (8, 2, 7, 8, 8),
+                                       (8, 2, 8, 7, 8), (8, 2, 8, 8, 7), (0, 2, 1, 1, 1),
+                                       (8, 0, 8, 8, 8)):
+            got = L.plasma_dsgesv(n, nrhs, p, lda, piv.ctypes.data, p, ldb, p, ldx,
+                                  ctypes.byref(it1))
+            want = R.plasma_dsgesv(n, nrhs, vp(p), lda, vp(piv.ctypes.data), vp(p), ldb,
+                                   vp(p), ldx, ctypes.byref(it2))
+            assert got == want, ("dsgesv", n, nrhs, lda, ldb, ldx, got, want)
+        for uplo, n, kd, nrhs, ldab, ldb in ((999, 8, 2, 1, 3, 8), (LO, -1, 2, 1, 3, 8),
+                                             (LO, 8, -1, 1, 3, 8), (LO, 8, 2, -1, 3, 8),
+                                             (LO, 8, 2, 1, 2, 8), (LO, 8, 2, 1, 3, 7),
+                                             (LO, 0, 0, 1, 1, 1), (UP, 8, 2, 0, 3, 8)):
+            legal = (uplo in (LO, UP) and n >= 0 and kd >= 0 and nrhs >= 0
+                     and ldab >= kd + 1 and ldb >= max(1, n))
+            # the quick returns of compute/zpbsv.c:131-133 and zpbtrs.c:120-122;
+            # past them both sides go on to build descriptors and compute
+            for name, quick in (("plasma_dpbsv", min(n, nrhs) == 0),
+                                ("plasma_dpbtrs", max(n, nrhs) == 0)):
+                got = getattr(L, name)(uplo, n, kd, nrhs, p, ldab, p, ldb)
+                want = getattr(R, name)(uplo, n, kd, nrhs, vp(p), ldab, vp(p), ldb)
+                if not legal or quick:
+                    assert got == want, (name, uplo, n, kd, nrhs, ldab, ldb, got, want)
+        for uplo, n, kd, ldab in ((999, 8, 2, 3), (LO, -1, 2, 3), (LO, 8, -1, 3),
+                                  (LO, 8, 2, 2), (LO, 0, 0, 1)):
+            got = L.plasma_dpbtrf(uplo, n, kd, p, ldab)
+            want = R.plasma_dpbtrf(uplo, n, kd, vp(p), ldab)
+            assert got == want, ("dpbtrf", uplo, n, kd, ldab, got, want)
+        for uplo, n, lda in ((999, 8, 8), (LO, -1, 8), (LO, 8, 7), (LO, 0, 1)):
+            for name in ("plasma_dpotri", "plasma_dpoinv"):
+                got = getattr(L, name)(uplo, n, p, lda)
+                want = getattr(R, name)(uplo, n, vp(p), lda)
+                assert got == want, (name, uplo, n, lda, got, want)
+    finally:
+        L.plasma_finalize()
+
+
 @pytest.fixture(scope="session")
 def rlb():
     return np.load(os.path.join(os.path.dirname(__file__), "golden",
