@@ -474,7 +474,9 @@ def run_band(args):
     2 kd + 1 added to the diagonal (diagonally dominant), b ~ U[-1, 1]
     (seed 9).  GFLOP/s counts LAPACK's flops for dpbtrf (n (kd^2 + 3 kd))
     and dpbtrs (4 n kd nrhs); the error is the reference tester's residual
-    ||b - A x||_inf / (n ||A||_F ||x||_inf)."""
+    ||b - A x||_inf / (n ||A||_F ||x||_inf).  cpu_baseline (first FP64 row
+    per kd): the reference's own plasma_dpbsv (oracle/_ref) on the host
+    cores, one solve of the same system, when that library is built."""
     import torch
     import plasma_b200 as pb
     L = pb.lib()
@@ -558,7 +560,9 @@ def run_lu(args):
     device-resident general A = U[-0.5, 0.5] (seed 9), n = 4096, one
     right-hand side b ~ U[-1, 1].  GFLOP/s counts LAPACK's dgetrf + dgetrs
     flops (2n^3/3 + 2n^2); the error is the reference tester's residual
-    ||b - A x||_inf / (n ||A||_inf ||x||_inf)."""
+    ||b - A x||_inf / (n ||A||_inf ||x||_inf).  cpu_baseline: the
+    reference's own plasma_dsgesv (oracle/_ref) on the host cores, one solve
+    of the same system, when that library is built."""
     import torch
     import plasma_b200 as pb
     L = pb.lib()
