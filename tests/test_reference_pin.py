@@ -430,3 +430,83 @@ def test_oracle_potri_info_matches_reference(rpi, col, tag):
     assert oracle.potrf(uplo, f, 64) == 0
     f[col, col] = 0.0
     assert oracle.potri(uplo, f) == int(rpi[f"potriinfo_{col}_{tag}"]) == col + 1
+
+
+@needs_ref
+def test_descriptors_match_reference(monkeypatch):
+    """plasma_desc_t as the reference builds it (control/descriptor.c): the
+    general, triangular and band inits, views and plasma_desc_check give the
+    same struct, field for field, and the same codes, on the same arguments
+    (host-only context; no storage is allocated)."""
+    import plasma_b200 as pb
+    monkeypatch.setenv("PLASMA_ALLOW_NO_DEVICE", "1")
+    L = pb.lib()
+    R = ref.lib()
+    if L.plasma_init() != 0:
+        pytest.skip("library context unavailable")
+    D = pb.plasma_desc_t
+    ci, vp = ctypes.c_int, ctypes.c_void_p
+    R.plasma_desc_general_init.argtypes = [ci, vp] + [ci] * 8 + [ctypes.POINTER(D)]
+    R.plasma_desc_triangular_init.argtypes = [ci, ci, vp] + [ci] * 8 + [ctypes.POINTER(D)]
+    R.plasma_desc_general_band_init.argtypes = [ci, ci, vp] + [ci] * 10 + [ctypes.POINTER(D)]
+    R.plasma_desc_view.argtypes = [D, ci, ci, ci, ci]
+    R.plasma_desc_view.restype = D
+    R.plasma_desc_check.argtypes = [D]
+    for f in ("plasma_desc_general_init", "plasma_desc_triangular_init",
+              "plasma_desc_general_band_init", "plasma_desc_check"):
+        getattr(R, f).restype = ci
+    mat = vp(0x10000)
+
+    def same(d1, d2, what):
+        for name, _ in D._fields_:
+            assert getattr(d1, name) == getattr(d2, name), (what, name, getattr(d1, name),
+                                                            getattr(d2, name))
+
+    try:
+        for prec in (pb.PlasmaRealDouble, pb.PlasmaRealFloat):
+            for mb, nb, lm, ln, i, j, m, n in ((256, 256, 1000, 700, 0, 0, 1000, 700),
+                                               (64, 64, 512, 512, 64, 128, 300, 200),
+                                               (128, 96, 385, 97, 0, 0, 385, 97),
+                                               (4, 4, 8, 8, 0, 0, 8, 8)):
+                d1, d2 = D(), D()
+                r1 = L.plasma_desc_general_init(prec, mat, mb, nb, lm, ln, i, j, m, n,
+                                                ctypes.byref(d1))
+                r2 = R.plasma_desc_general_init(prec, mat, mb, nb, lm, ln, i, j, m, n,
+                                                ctypes.byref(d2))
+                assert r1 == r2
+                same(d1, d2, ("general", mb, nb, lm, ln, i, j, m, n))
+                assert L.plasma_desc_check(d1) == R.plasma_desc_check(d2)
+                if m > mb and n > nb:
+                    same(L.plasma_desc_view(d1, mb, nb, m - mb, n - nb),
+                         R.plasma_desc_view(d2, mb, nb, m - mb, n - nb), "view")
+            for uplo in (LO, UP):
+                for nb, n in ((256, 1000), (64, 512), (96, 97)):
+                    d1, d2 = D(), D()
+                    assert (L.plasma_desc_triangular_init(prec, uplo, mat, nb, nb, n, n, 0, 0,
+                                                          n, n, ctypes.byref(d1))
+                            == R.plasma_desc_triangular_init(prec, uplo, mat, nb, nb, n, n,
+                                                             0, 0, n, n, ctypes.byref(d2)))
+                    same(d1, d2, ("triangular", uplo, nb, n))
+                    assert L.plasma_desc_check(d1) == R.plasma_desc_check(d2)
+                for nb, n, kd in ((128, 1000, 100), (64, 300, 200), (256, 2049, 256)):
+                    lm = nb * (1 + (kd + nb - 1) // nb)
+                    d1, d2 = D(), D()
+                    assert (L.plasma_desc_general_band_init(prec, uplo, mat, nb, nb, lm, n, 0,
+                                                            0, n, n, kd, kd, ctypes.byref(d1))
+                            == R.plasma_desc_general_band_init(prec, uplo, mat, nb, nb, lm, n,
+                                                               0, 0, n, n, kd, kd,
+                                                               ctypes.byref(d2)))
+                    same(d1, d2, ("band", uplo, nb, n, kd))
+                    assert L.plasma_desc_check(d1) == R.plasma_desc_check(d2)
+        # descriptors plasma_desc_check rejects (mb = 0 is left out: the
+        # reference's init divides by it, control/descriptor.c:144, where the
+        # library records the descriptor for plasma_desc_check to reject)
+        for args in ((pb.PlasmaRealDouble, 4, 4, 8, 8, 2, 0, 4, 8),
+                     (pb.PlasmaRealDouble, 4, 4, 8, 8, 4, 0, 8, 8),
+                     (99, 4, 4, 8, 8, 0, 0, 8, 8)):
+            d1, d2 = D(), D()
+            L.plasma_desc_general_init(args[0], mat, *args[1:], ctypes.byref(d1))
+            R.plasma_desc_general_init(args[0], mat, *args[1:], ctypes.byref(d2))
+            assert L.plasma_desc_check(d1) == R.plasma_desc_check(d2) != 0, args
+    finally:
+        L.plasma_finalize()
