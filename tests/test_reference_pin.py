@@ -510,3 +510,45 @@ def test_descriptors_match_reference(monkeypatch):
             assert L.plasma_desc_check(d1) == R.plasma_desc_check(d2) != 0, args
     finally:
         L.plasma_finalize()
+
+
+@needs_ref
+def test_settings_match_reference(monkeypatch):
+    """plasma_set / plasma_get (control/context.c:78-159) on the reference's
+    parameters: the same code for every legal and illegal value and for an
+    unknown parameter, and plasma_get returning what was set."""
+    import plasma_b200 as pb
+    monkeypatch.setenv("PLASMA_ALLOW_NO_DEVICE", "1")
+    L = pb.lib()
+    R = ref.lib()
+    if L.plasma_init() != 0:
+        pytest.skip("library context unavailable")
+    R.plasma_get.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    R.plasma_get.restype = ctypes.c_int
+    tuning, nb, ib, inout, threads, householder = range(6)
+    cases = [(tuning, v) for v in (0, 1, 2, -1)] + \
+            [(nb, v) for v in (1, 96, 256, 0, -5)] + \
+            [(ib, v) for v in (1, 32, 0, -1)] + \
+            [(inout, v) for v in (0, 1, 5)] + \
+            [(threads, v) for v in (1, 4, 0)] + \
+            [(householder, v) for v in (0, 1, 2)] + \
+            [(77, 1), (-3, 1)]
+    saved = {}
+    for param in (tuning, nb, ib, threads, householder):
+        v = ctypes.c_int()
+        assert R.plasma_get(param, ctypes.byref(v)) == 0
+        saved[param] = v.value
+    try:
+        for param, value in cases:
+            got, want = L.plasma_set(param, value), R.plasma_set(param, value)
+            assert got == want, (param, value, got, want)
+            if want == 0:
+                g1, g2 = ctypes.c_int(-7), ctypes.c_int(-7)
+                assert L.plasma_get(param, ctypes.byref(g1)) == R.plasma_get(
+                    param, ctypes.byref(g2)) == 0
+                assert g1.value == g2.value == value, (param, value, g1.value, g2.value)
+    finally:
+        L.plasma_finalize()
+        # the reference context is shared by the other tests
+        for param, v in saved.items():
+            R.plasma_set(param, v)
