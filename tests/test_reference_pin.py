@@ -552,3 +552,21 @@ def test_settings_match_reference(monkeypatch):
         # the reference context is shared by the other tests
         for param, v in saved.items():
             R.plasma_set(param, v)
+
+
+@needs_ref
+def test_lapack_constants_match_reference():
+    """plasma_{uplo,trans,side,diag,norm}_const (control/constants.c): the
+    reference's enum for every LAPACK character, either case, and for
+    characters it does not know."""
+    import plasma_b200 as pb
+    L = pb.lib()
+    R = ref.lib()
+    for name in ("plasma_uplo_const", "plasma_trans_const", "plasma_side_const",
+                 "plasma_diag_const", "plasma_norm_const"):
+        f = getattr(R, name)
+        f.argtypes = [ctypes.c_char]
+        f.restype = ctypes.c_int
+        for ch in b"ABCDEFGHIJKLMNOPQRSTUVWXYZabcdefghijklmnopqrstuvwxyz0123456789":
+            c = bytes([ch])
+            assert getattr(L, name)(c) == f(c), (name, c)
